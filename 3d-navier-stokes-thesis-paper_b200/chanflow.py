@@ -1,0 +1,365 @@
+"""Python mirror of the reference solver's hot-path module interfaces over the
+C ABI of include/chanflow.h (libchanflow_b200.so, built in-tree for sm_100a).
+
+The method names follow the Fortran module procedures they replace
+(PFC = ParallelFortran-Code/ of the reference):
+
+    ChannelFlow.nonlinear            pass1::nonlinear          PFC/pass1.f90:26
+    ChannelFlow.nonlinear_linearized pass1_linearized          PFC/pass1_linearized.f90:135
+    ChannelFlow.rhs_solve            pass2::rhs_solve          PFC/pass2.f90:29
+    ChannelFlow.boundary             read_write::boundary      PFC/read_write.f90:1465
+    ChannelFlow.l2_norm              read_write::l2_norm       PFC/read_write.f90:1432
+    ChannelFlow.xz_fft_complex_to_real / xz_fft_real_to_complex
+                                     transform module          PFC/transform.f90:195-227
+    ChannelFlow.timestep             main_mpi timestep loop    PFC/main_mpi.f90:70-86
+
+Arrays cross the boundary in the reference's Fortran layouts (numpy arrays
+with order='F').  There is no CPU fallback: constructing a ChannelFlow without
+the CUDA library or without a GPU raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libchanflow_b200.so")
+
+FP64 = 0
+MIXED = 1
+
+ERRORS = {
+    -1: "invalid argument", -2: "CUDA error", -3: "out of device memory",
+    -4: "CFL IS TOO BIG", -5: "DT IS TOO BIG", -6: "call out of sequence",
+}
+
+
+class CfgParams(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("nx2", C.c_int), ("nz2", C.c_int),
+        ("re", C.c_double), ("lx", C.c_double), ("lz", C.c_double), ("beta", C.c_double),
+        ("dt", C.c_double), ("cfl_max", C.c_double),
+        ("fix_mass", C.c_int), ("dt_flag", C.c_int),
+        ("ctrlu", C.c_double), ("ctrlw", C.c_double),
+        ("precision", C.c_int), ("device", C.c_int),
+    ]
+
+
+_DP = C.POINTER(C.c_double)
+
+
+class CfgGrid(C.Structure):
+    _fields_ = [(n, _DP) for n in ("y", "yh", "hn", "dh", "dn", "iu", "dm", "d2h", "d2n", "dyh",
+                                   "dy", "kx", "kz", "buffer", "target_inflow")]
+
+
+class CfhRun(C.Structure):
+    _fields_ = [
+        ("re", C.c_double), ("ctrlu", C.c_double), ("ctrlw", C.c_double), ("lx", C.c_double),
+        ("lz", C.c_double), ("beta", C.c_double), ("disturb_ampl", C.c_double),
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("nx2", C.c_int), ("nz2", C.c_int),
+        ("tend", C.c_int), ("output_step", C.c_int), ("save_step", C.c_int), ("l2_step", C.c_int),
+        ("read_vel", C.c_int), ("save_vel", C.c_int), ("vel_out", C.c_int), ("which_test", C.c_int),
+        ("fix_mass", C.c_int), ("dt_flag", C.c_int), ("divg_check", C.c_int),
+        ("bl_grid", C.c_int), ("crossflow", C.c_int), ("filter_jet_profile", C.c_int),
+        ("jet_diam", C.c_double), ("xjet_top", C.c_double), ("zjet_top", C.c_double),
+        ("jetmag_top", C.c_double), ("forcing_top", C.c_double), ("for_freq_top", C.c_double),
+        ("xjet_bot", C.c_double), ("zjet_bot", C.c_double), ("jetmag_bot", C.c_double),
+        ("forcing_bot", C.c_double), ("for_freq_bot", C.c_double),
+        ("xfringe", C.c_int), ("zfringe", C.c_int), ("frac_xbuff", C.c_double),
+        ("stretch", C.c_double), ("dt", C.c_double), ("seed", C.c_ulonglong),
+        ("precision", C.c_int), ("uniform_grid", C.c_int), ("jet_mode", C.c_int),
+        ("jet_width", C.c_double), ("jet_peak", C.c_double), ("jet_freq", C.c_double),
+    ]
+
+
+class CfhGrid(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("nx2", C.c_int), ("nz2", C.c_int)] + \
+        [(n, _DP) for n in ("y", "yh", "hh", "hn", "dh", "dn", "iu", "dm", "d2h", "d2n", "dyh", "dy",
+                            "kx", "kz", "buffer", "target_inflow", "xcoord", "zcoord")]
+
+
+# exported symbols: name -> (restype, argtypes)
+_VP = C.c_void_p
+SYMBOLS = {
+    "cfg_create": (C.c_int, [C.POINTER(CfgParams), C.POINTER(CfgGrid), C.POINTER(_VP)]),
+    "cfg_destroy": (None, [_VP]),
+    "cfg_last_error": (C.c_char_p, [_VP]),
+    "cfg_upload_state": (C.c_int, [_VP, _VP, _VP, _VP]),
+    "cfg_download_state": (C.c_int, [_VP, _VP, _VP, _VP]),
+    "cfg_set_scalars": (C.c_int, [_VP, C.c_double, C.c_double, C.c_double, _VP]),
+    "cfg_get_scalars": (C.c_int, [_VP, _DP, _DP, _DP, _VP, _DP]),
+    "cfg_set_wall_bc": (C.c_int, [_VP, _VP, _VP]),
+    "cfg_get_wall_bc": (C.c_int, [_VP, _VP, _VP]),
+    "cfg_boundary": (C.c_int, [_VP]),
+    "cfg_nonlinear": (C.c_int, [_VP, C.c_int, C.c_int]),
+    "cfg_nonlinear_linearized": (C.c_int, [_VP, C.c_int, C.c_int]),
+    "cfg_set_baseflow": (C.c_int, [_VP, _VP]),
+    "cfg_rhs_solve": (C.c_int, [_VP, C.c_int, C.c_int]),
+    "cfg_timestep": (C.c_int, [_VP, C.c_int]),
+    "cfg_timestep_linearized": (C.c_int, [_VP, C.c_int]),
+    "cfg_xz_c2r": (C.c_int, [_VP, _VP, _VP]),
+    "cfg_xz_r2c": (C.c_int, [_VP, _VP, _VP]),
+    "cfg_small_r2c": (C.c_int, [_VP, _VP, _VP, C.c_int]),
+    "cfg_small_c2r": (C.c_int, [_VP, _VP, _VP, C.c_int]),
+    "cfg_l2_norm": (C.c_int, [_VP, _DP, _DP]),
+    "cfg_remove_initial_divergence": (C.c_int, [_VP]),
+    "cfg_compute_initial_pressure": (C.c_int, [_VP, C.c_int]),
+    "cfg_diagnostics": (C.c_int, [_VP, _DP, _DP]),
+    "cfg_status": (C.c_int, [_VP]),
+    "cfg_synchronize": (C.c_int, [_VP]),
+    "cfg_launch_count": (C.c_longlong, [_VP]),
+    "cfh_run_defaults": (None, [C.POINTER(CfhRun)]),
+    "cfh_read_flow_dat": (C.c_int, [C.c_char_p, C.POINTER(CfhRun), C.c_char_p, C.c_int]),
+    "cfh_grid_alloc": (C.POINTER(CfhGrid), [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
+    "cfh_grid_free": (None, [C.POINTER(CfhGrid)]),
+    "cfh_define_grid": (C.c_int, [C.POINTER(CfhGrid), C.c_double, C.c_double, C.c_double, C.c_int]),
+    "cfh_initial_field": (C.c_int, [C.POINTER(CfhGrid), C.c_int, C.c_ulonglong, C.c_double,
+                                    C.c_double, _VP]),
+    "cfh_rng_u01": (C.c_double, [C.c_ulonglong, C.c_int, C.c_int, C.c_int, C.c_int]),
+}
+
+_lib = None
+
+
+def load_library(path=LIB_PATH):
+    """Load libchanflow_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise RuntimeError(f"CUDA extension missing: {path} (run __graft_entry__.build())")
+        L = C.CDLL(path)
+        for name, (res, args) in SYMBOLS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+class ChanflowError(RuntimeError):
+    pass
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+class Grid:
+    """Host-side grid operators: define_coordinates + wavenumbers (C++ setup)."""
+
+    NAMES = {"y": "ny", "yh": "ny1", "hh": "ny1", "hn": "ny", "dh": "ny1", "dn": "ny",
+             "iu": (2, "ny"), "dm": (3, 4), "d2h": (3, "ny1"), "d2n": (3, "ny"), "dyh": "ny1",
+             "dy": "ny1", "kx": "nxh", "kz": "nz", "buffer": ("nx2", "nz2"),
+             "target_inflow": ("ny1", 3), "xcoord": "nx1", "zcoord": "nz1"}
+
+    def __init__(self, nx, ny, nz, nx2=None, nz2=None, lx=4 * np.pi, lz=2 * np.pi, stretch=2.75,
+                 uniform=0):
+        L = load_library()
+        nx2 = nx2 or 3 * nx // 2
+        nz2 = nz2 or 3 * nz // 2
+        self.nx, self.ny, self.nz, self.nx2, self.nz2 = nx, ny, nz, nx2, nz2
+        self.lx, self.lz = lx, lz
+        h = L.cfh_grid_alloc(nx, ny, nz, nx2, nz2)
+        if L.cfh_define_grid(h, lx, lz, stretch, uniform) != 0:
+            L.cfh_grid_free(h)
+            raise ChanflowError("define_grid failed")
+        dims = {"ny": ny, "ny1": ny + 1, "nxh": nx // 2 + 1, "nz": nz, "nx2": nx2, "nz2": nz2,
+                "nx1": nx + 1, "nz1": nz + 1}
+        for name, shp in self.NAMES.items():
+            shp = shp if isinstance(shp, tuple) else (shp,)
+            shp = tuple(dims[s] if isinstance(s, str) else s for s in shp)
+            n = int(np.prod(shp))
+            arr = np.ctypeslib.as_array(getattr(h.contents, name), shape=(n,)).copy()
+            setattr(self, name, np.asfortranarray(arr.reshape(shp, order="F")))
+        L.cfh_grid_free(h)
+
+    def cfg_grid(self):
+        keep = []
+
+        def ptr(a):
+            a = np.asfortranarray(a, dtype=np.float64)
+            keep.append(a)
+            return a.ctypes.data_as(_DP)
+
+        g = CfgGrid(*[ptr(getattr(self, n)) for n in ("y", "yh", "hn", "dh", "dn", "iu", "dm", "d2h",
+                                                       "d2n", "dyh", "dy", "kx", "kz", "buffer",
+                                                       "target_inflow")])
+        return g, keep
+
+
+def initial_field(grid, which_test, seed=1, ampl=1e-3, beta=0.0):
+    """Seeded which_test initial velocity in data1 layout (before the device
+    divergence removal and initial pressure)."""
+    L = load_library()
+    nxh = grid.nx // 2 + 1
+    d1 = np.zeros((grid.nz, nxh, grid.ny + 1, 3), dtype=np.complex128, order="F")
+    h = L.cfh_grid_alloc(grid.nx, grid.ny, grid.nz, grid.nx2, grid.nz2)
+    for name in ("y", "yh", "dh", "dyh", "kx", "kz"):
+        src = np.ascontiguousarray(getattr(grid, name).ravel(order="F"))
+        C.memmove(getattr(h.contents, name), src.ctypes.data, src.nbytes)
+    r = L.cfh_initial_field(h, which_test, seed, ampl, beta, d1.ctypes.data)
+    L.cfh_grid_free(h)
+    if r != 0:
+        raise ChanflowError(f"unsupported which_test {which_test}")
+    return d1
+
+
+def read_flow_dat(path):
+    L = load_library()
+    run = CfhRun()
+    err = C.create_string_buffer(256)
+    r = L.cfh_read_flow_dat(path.encode(), C.byref(run), err, 256)
+    if r != 0:
+        raise ChanflowError(err.value.decode())
+    return run
+
+
+class ChannelFlow:
+    """One device context: state, plans and the hot-path routines."""
+
+    def __init__(self, grid, re=2500.0, dt=0.005, beta=0.0, cfl_max=0.95, fix_mass=1, dt_flag=0,
+                 ctrlu=0.0, ctrlw=0.0, precision=FP64, device=0):
+        self.L = load_library()
+        self.grid = grid
+        self.nx, self.ny, self.nz = grid.nx, grid.ny, grid.nz
+        self.nx2, self.nz2 = grid.nx2, grid.nz2
+        self.nxh = grid.nx // 2 + 1
+        self.precision = precision
+        self.params = CfgParams(grid.nx, grid.ny, grid.nz, grid.nx2, grid.nz2, re, grid.lx, grid.lz,
+                                beta, dt, cfl_max, fix_mass, dt_flag, ctrlu, ctrlw, precision, device)
+        g, keep = grid.cfg_grid()
+        h = C.c_void_p()
+        r = self.L.cfg_create(C.byref(self.params), C.byref(g), C.byref(h))
+        if r != 0:
+            raise ChanflowError(f"cfg_create failed ({ERRORS.get(r, r)})")
+        self.h = h
+        self.step = 0
+
+    def _chk(self, r):
+        if r != 0:
+            msg = self.L.cfg_last_error(self.h)
+            raise ChanflowError(f"{ERRORS.get(r, r)}: {msg.decode() if msg else ''}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.cfg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- state
+    def shapes(self):
+        n1 = self.ny + 1
+        return ((self.nz, self.nxh, n1, 3), (n1, 3, self.nz, self.nxh), (n1, self.nz, self.nxh))
+
+    def upload_state(self, data1=None, data2=None, data4=None):
+        a = [None if d is None else np.asfortranarray(d, dtype=np.complex128) for d in (data1, data2, data4)]
+        self._chk(self.L.cfg_upload_state(self.h, _p(a[0]), _p(a[1]), _p(a[2])))
+
+    def download_state(self):
+        s1, s2, s4 = self.shapes()
+        d1 = np.zeros(s1, np.complex128, order="F")
+        d2 = np.zeros(s2, np.complex128, order="F")
+        d4 = np.zeros(s4, np.complex128, order="F")
+        self._chk(self.L.cfg_download_state(self.h, _p(d1), _p(d2), _p(d4)))
+        return d1, d2, d4
+
+    def set_scalars(self, t_total, dt, p_grad, d_um_dy=None):
+        d = None if d_um_dy is None else np.ascontiguousarray(d_um_dy, dtype=np.float64)
+        self._chk(self.L.cfg_set_scalars(self.h, t_total, dt, p_grad, _p(d)))
+
+    def scalars(self):
+        t, dt, pg, cm = C.c_double(), C.c_double(), C.c_double(), C.c_double()
+        dud = np.zeros(self.ny)
+        self._chk(self.L.cfg_get_scalars(self.h, C.byref(t), C.byref(dt), C.byref(pg), _p(dud),
+                                         C.byref(cm)))
+        return {"t_total": t.value, "dt": dt.value, "p_grad": pg.value, "d_um_dy": dud,
+                "cfl_max": cm.value}
+
+    def set_wall_bc(self, cbc_top=None, cbc_bot=None):
+        a = [None if d is None else np.asfortranarray(d, dtype=np.complex128) for d in (cbc_top, cbc_bot)]
+        self._chk(self.L.cfg_set_wall_bc(self.h, _p(a[0]), _p(a[1])))
+
+    def wall_bc(self):
+        top = np.zeros((self.nz, self.nxh, 3), np.complex128, order="F")
+        bot = np.zeros_like(top)
+        self._chk(self.L.cfg_get_wall_bc(self.h, _p(top), _p(bot)))
+        return top, bot
+
+    def set_baseflow(self, profile):
+        p = np.asfortranarray(profile, dtype=np.float64)
+        self._chk(self.L.cfg_set_baseflow(self.h, _p(p)))
+
+    # ---- hot path (reference module procedures)
+    def boundary(self):
+        self._chk(self.L.cfg_boundary(self.h))
+
+    def nonlinear(self, step, rk_step):
+        self._chk(self.L.cfg_nonlinear(self.h, step, rk_step))
+
+    def nonlinear_linearized(self, step, rk_step):
+        self._chk(self.L.cfg_nonlinear_linearized(self.h, step, rk_step))
+
+    def rhs_solve(self, step, rk_step):
+        self._chk(self.L.cfg_rhs_solve(self.h, step, rk_step))
+
+    def timestep(self, nsteps=1):
+        self._chk(self.L.cfg_timestep(self.h, nsteps))
+
+    def timestep_linearized(self, nsteps=1):
+        self._chk(self.L.cfg_timestep_linearized(self.h, nsteps))
+
+    def xz_fft_complex_to_real(self, cdata):
+        cd = np.asfortranarray(cdata, dtype=np.complex128)
+        out = np.zeros((self.nx2, self.nz2), order="F")
+        self._chk(self.L.cfg_xz_c2r(self.h, _p(cd), _p(out)))
+        return out
+
+    def xz_fft_real_to_complex(self, data):
+        d = np.asfortranarray(data, dtype=np.float64)
+        out = np.zeros((self.nz, self.nxh), np.complex128, order="F")
+        self._chk(self.L.cfg_xz_r2c(self.h, _p(d), _p(out)))
+        return out
+
+    def l2_norm(self):
+        l2, drag = C.c_double(), C.c_double()
+        self._chk(self.L.cfg_l2_norm(self.h, C.byref(l2), C.byref(drag)))
+        return l2.value, drag.value
+
+    def remove_initial_divergence(self):
+        self._chk(self.L.cfg_remove_initial_divergence(self.h))
+
+    def compute_initial_pressure(self, linearized=0):
+        self._chk(self.L.cfg_compute_initial_pressure(self.h, linearized))
+
+    def diagnostics(self):
+        q, d = C.c_double(), C.c_double()
+        self._chk(self.L.cfg_diagnostics(self.h, C.byref(q), C.byref(d)))
+        return q.value, d.value
+
+    def status(self):
+        return self.L.cfg_status(self.h)
+
+    def synchronize(self):
+        self._chk(self.L.cfg_synchronize(self.h))
+
+    def launch_count(self):
+        return self.L.cfg_launch_count(self.h)
+
+    # ---- define_initial_field (PFC/init_vel.f90:25-353) on the device
+    def define_initial_field(self, which_test, seed=1, ampl=1e-3, beta=0.0):
+        d1 = initial_field(self.grid, which_test, seed, ampl, beta)
+        self.upload_state(d1, None, np.zeros(self.shapes()[2], np.complex128, order="F"))
+        if which_test == 6:
+            sc = self.scalars()
+            self.set_scalars(0.0, sc["dt"], 0.0)
+        else:
+            sc = self.scalars()
+            self.set_scalars(0.0, sc["dt"], sc["p_grad"])
+        self.remove_initial_divergence()
+        self.compute_initial_pressure(0)

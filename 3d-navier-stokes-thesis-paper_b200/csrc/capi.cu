@@ -1,0 +1,898 @@
+// capi.cu -- the C ABI of include/chanflow.h: device state, plans, kernel
+// orchestration for one channel-flow context on one B200.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "chanflow.h"
+#include "pass1.cuh"
+#include "pass2.cuh"
+#include "planes.cuh"
+
+using namespace cfd;
+
+// ----------------------------------------------------------------------------
+// layout conversion kernels between the reference's Fortran arrays (FP64) and
+// the device state ([kx][kz][comp][y], precision T)
+template <typename T>
+__global__ void k_data1_in(const double2* __restrict__ src, cplx_t<T>* __restrict__ vel,
+                           double2* __restrict__ mvel64, Geom g) {
+  // src (nz, nxh, ny+1, 3): element (z, x, j, c) at z + nz*(x + nxh*(j + ny1*c))
+  const size_t n = (size_t)g.nw * 3 * g.ny1;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int j = (int)(i % g.ny1);
+    const int c = (int)((i / g.ny1) % 3);
+    const size_t w = i / ((size_t)3 * g.ny1);
+    const double2 v = src[w + (size_t)g.nw * (j + (size_t)g.ny1 * c)];
+    vel[i] = mk<cplx_t<T>>((T)v.x, (T)v.y);
+    if (mvel64 && w == 0) mvel64[c * g.ny1 + j] = v;
+  }
+}
+template <typename T>
+__global__ void k_data1_out(const cplx_t<T>* __restrict__ vel, const double2* __restrict__ mvel64,
+                            double2* __restrict__ dst, Geom g) {
+  const size_t n = (size_t)g.nw * 3 * g.ny1;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int j = (int)(i % g.ny1);
+    const int c = (int)((i / g.ny1) % 3);
+    const size_t w = i / ((size_t)3 * g.ny1);
+    double2 v;
+    if (mvel64 && w == 0) v = mvel64[c * g.ny1 + j];
+    else { const cplx_t<T> s = vel[i]; v = make_double2((double)s.x, (double)s.y); }
+    dst[w + (size_t)g.nw * (j + (size_t)g.ny1 * c)] = v;
+  }
+}
+template <typename T>
+__global__ void k_conv_in(const double2* __restrict__ src, cplx_t<T>* __restrict__ dst, size_t n,
+                          double2* __restrict__ side, size_t nside) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double2 v = src[i];
+    dst[i] = mk<cplx_t<T>>((T)v.x, (T)v.y);
+    if (side && i < nside) side[i] = v;
+  }
+}
+template <typename T>
+__global__ void k_conv_out(const cplx_t<T>* __restrict__ src, double2* __restrict__ dst, size_t n,
+                           const double2* __restrict__ side, size_t nside) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    if (side && i < nside) dst[i] = side[i];
+    else { const cplx_t<T> s = src[i]; dst[i] = make_double2((double)s.x, (double)s.y); }
+  }
+}
+template <typename T>
+__global__ void k_real_in(const double* __restrict__ src, T* __restrict__ dst, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) dst[i] = (T)src[i];
+}
+template <typename T>
+__global__ void k_real_out(const T* __restrict__ src, double* __restrict__ dst, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) dst[i] = (double)src[i];
+}
+__global__ void k_advance_time(DevScalars* sc) { sc->t_total = sc->t_total + sc->dt; }
+
+// max |divergence| (check_divergence, PFC/pass2.f90:380-419), warp per wavenumber
+template <typename T>
+__global__ void k_divergence(const cplx_t<T>* __restrict__ vel, Geom g, GridDev gd,
+                             unsigned long long* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (w >= g.nw) return;
+  const int n1 = g.ny1, ny = g.ny;
+  const double kx = gd.kx[w / g.nz], kz = gd.kz[w % g.nz];
+  const cplx_t<T>* c = vel + (size_t)w * 3 * n1;
+  double m = 0;
+  for (int j = 1 + lane; j <= ny - 1; j += 32) {
+    const double dvx = gd.dh[j] * ((double)c[n1 + j].x - (double)c[n1 + j - 1].x);
+    const double dvy = gd.dh[j] * ((double)c[n1 + j].y - (double)c[n1 + j - 1].y);
+    const double re = -kx * (double)c[j].y + dvx - kz * (double)c[2 * n1 + j].y;
+    const double im = kx * (double)c[j].x + dvy + kz * (double)c[2 * n1 + j].x;
+    m = fmax(m, sqrt(re * re + im * im));
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (lane == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+// ----------------------------------------------------------------------------
+struct cfg_ctx {
+  cfg_params p{};
+  Geom g{};
+  bool mixed = false;
+  int dev = 0;
+  cudaStream_t st = nullptr;
+  std::string err;
+  long long launches = 0;
+  int step = 0;
+  // grid
+  double* dgrid = nullptr;
+  GridDev gd{};
+  void* fringe = nullptr;
+  int has_fringe = 0;
+  // state
+  void *vel = nullptr, *cru = nullptr, *prs = nullptr;
+  double2 *mvel64 = nullptr, *mcru64 = nullptr;
+  void *T1 = nullptr, *T2 = nullptr;
+  void* cbc = nullptr;   // [bot, top][3][nw]
+  DevScalars* sc = nullptr;
+  double* d_um_dy = nullptr;
+  double* cflp = nullptr;
+  unsigned long long* cflbits = nullptr;
+  double* l2acc = nullptr;
+  unsigned long long* divbits = nullptr;
+  int* plist = nullptr;
+  // plane work buffers
+  void *pw_H = nullptr, *pw_phys = nullptr, *pw_phys2 = nullptr, *pw_in = nullptr;
+  size_t pw_planes = 0;
+  // staging for FP64 host <-> device conversion
+  double2* stage = nullptr;
+  size_t stage_elems = 0;
+  // twiddles and plans
+  void *twx = nullptr, *twz = nullptr, *twxs = nullptr, *twzs = nullptr;
+  FftPlan px{}, pz{}, pxs{}, pzs{};
+  // launch shapes
+  int YB1 = 1, YB3 = 1, ZR = 1, KC = 4, M = 2;
+  size_t sm_zinv = 0, sm_xflux = 0, sm_zfwd = 0, sm_rhs = 0;
+  RkTab rkt{};
+  double hdm[12] = {0};
+  std::vector<double> hdy;
+};
+
+static int fail(cfg_ctx* c, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return code;
+}
+#define CK(call)                                                                         \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess) return fail(c, CFG_E_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+#define CKL()                                                                            \
+  do {                                                                                   \
+    c->launches++;                                                                       \
+    cudaError_t e_ = cudaGetLastError();                                                 \
+    if (e_ != cudaSuccess) return fail(c, CFG_E_CUDA, "launch: %s", cudaGetErrorString(e_)); \
+  } while (0)
+
+static bool make_plan(int n, FftPlan& p) {
+  memset(&p, 0, sizeof(p));
+  p.n = n;
+  int m = n, k = 0;
+  while (m % 8 == 0) { p.radix[k++] = 8; m /= 8; }
+  while (m % 4 == 0) { p.radix[k++] = 4; m /= 4; }
+  while (m % 2 == 0) { p.radix[k++] = 2; m /= 2; }
+  while (m % 3 == 0) { p.radix[k++] = 3; m /= 3; }
+  if (m != 1 || k > 16) return false;
+  p.npass = k;
+  int ns = 1;
+  for (int q = 0; q < k; ++q) { p.ns[q] = ns; ns *= p.radix[q]; }
+  return true;
+}
+
+template <typename T>
+static void* make_twiddles(int n) {
+  std::vector<cplx_t<T>> h(n);
+  for (int m = 0; m < n; ++m) {
+    const double a = -2.0 * M_PI * (double)m / (double)n;
+    h[m].x = (T)cos(a);
+    h[m].y = (T)sin(a);
+  }
+  void* d = nullptr;
+  if (cudaMalloc(&d, sizeof(cplx_t<T>) * n) != cudaSuccess) return nullptr;
+  cudaMemcpy(d, h.data(), sizeof(cplx_t<T>) * n, cudaMemcpyHostToDevice);
+  return d;
+}
+
+static dim3 grid1d(size_t n, int bs = 256) {
+  size_t b = (n + bs - 1) / bs;
+  if (b > 148 * 32) b = 148 * 32;
+  if (b < 1) b = 1;
+  return dim3((unsigned)b);
+}
+
+// ----------------------------------------------------------------------------
+template <typename T>
+struct Impl {
+  using C = cplx_t<T>;
+
+  static int setup(cfg_ctx* c) {
+    const Geom& g = c->g;
+    const size_t cs = sizeof(C);
+    const size_t budget = 110 * 1024;
+    c->YB1 = (int)std::max<size_t>(1, std::min<size_t>(8, (budget / cs / g.nz2 - 1) / 6));
+    c->YB3 = (int)std::max<size_t>(1, std::min<size_t>(8, (budget / cs / g.nz2 - 1) / 12));
+    c->sm_zinv = cs * (g.nz2 + 6 * c->YB1 * g.nz2);
+    c->sm_zfwd = cs * (g.nz2 + 12 * c->YB3 * g.nz2);
+    auto xsm = [&](int zr) {
+      const int nseq = 4 * zr + (zr + 1) / 2;
+      return cs * g.nx2 + sizeof(T) * 9 * zr * g.nx2 + 2 * cs * nseq * g.nx2;
+    };
+    c->ZR = 1;
+    for (int zr : {4, 2}) if (g.nz2 % zr == 0 && xsm(zr) <= budget) { c->ZR = zr; break; }
+    c->sm_xflux = xsm(c->ZR);
+    long kc = (long)(g.ny - 1) * (g.nz2 / c->ZR) / 592;
+    c->KC = (int)std::max(2L, std::min(16L, kc));
+    c->M = (g.ny1 + 31) / 32;
+    if (c->M < 2) c->M = 2;
+    if (c->M > 8) return fail(c, CFG_E_ARG, "ny+1 = %d exceeds 256 rows", g.ny1);
+    if (c->sm_zinv > 200 * 1024 || c->sm_zfwd > 200 * 1024 || c->sm_xflux > 200 * 1024)
+      return fail(c, CFG_E_ARG, "transform lengths too large for shared memory");
+    CK(cudaFuncSetAttribute(k_zinv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_zinv));
+    CK(cudaFuncSetAttribute(k_zfwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_zfwd));
+    CK(cudaFuncSetAttribute(k_xflux<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_xflux));
+    CK(cudaFuncSetAttribute(k_xflux<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_xflux));
+    const int maxn = std::max(std::max(g.nx2, g.nz2), std::max(g.nx, g.nz));
+    const int smp = (int)(cs * (3 * maxn + 3 * maxn * 2 + 64));
+    CK(cudaFuncSetAttribute(k_pz_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smp));
+    CK(cudaFuncSetAttribute(k_pz_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smp));
+    CK(cudaFuncSetAttribute(k_px_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smp));
+    CK(cudaFuncSetAttribute(k_px_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smp));
+    CK(cudaFuncSetAttribute(k_l2_rows<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smp));
+    c->sm_rhs = 0;
+    switch (c->M) {
+#define RHS_ATTR(MM)                                                                              \
+  case MM:                                                                                        \
+    c->sm_rhs = 4 * 5 * ColIdx<MM>::SIZE * cs;                                                   \
+    CK(cudaFuncSetAttribute(k_rhs<T, MM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_rhs)); \
+    break;
+      RHS_ATTR(2) RHS_ATTR(3) RHS_ATTR(4) RHS_ATTR(5) RHS_ATTR(6) RHS_ATTR(7) RHS_ATTR(8)
+#undef RHS_ATTR
+    }
+    c->twx = make_twiddles<T>(g.nx2);
+    c->twz = make_twiddles<T>(g.nz2);
+    c->twxs = make_twiddles<T>(g.nx);
+    c->twzs = make_twiddles<T>(g.nz);
+    if (!c->twx || !c->twz || !c->twxs || !c->twzs) return fail(c, CFG_E_NOMEM, "twiddles");
+    return CFG_OK;
+  }
+
+  static int nonlinear(cfg_ctx* c, int step, int rk, bool lin) {
+    const Geom& g = c->g;
+    const int do_cfl = (rk == 1);
+    if (do_cfl) CK(cudaMemsetAsync(c->cflbits, 0, sizeof(unsigned long long) * 3 * g.ny1, c->st));
+    dim3 g1(g.nxh, (g.ny1 + c->YB1 - 1) / c->YB1);
+    k_zinv<T><<<g1, 256, c->sm_zinv, c->st>>>((const C*)c->vel, (C*)c->T1, g, c->pz, (const C*)c->twz,
+                                               c->YB1, 0, g.ny1);
+    CKL();
+    dim3 g2(g.nz2 / c->ZR, (g.ny - 1 + c->KC - 1) / c->KC);
+    if (lin)
+      k_xflux<T, true><<<g2, 256, c->sm_xflux, c->st>>>((const C*)c->T1, (C*)c->T2, g, c->px, (const C*)c->twx,
+                                                         c->gd, (const T*)c->fringe, c->has_fringe, c->ZR, c->KC,
+                                                         c->cflbits, do_cfl);
+    else
+      k_xflux<T, false><<<g2, 256, c->sm_xflux, c->st>>>((const C*)c->T1, (C*)c->T2, g, c->px, (const C*)c->twx,
+                                                          c->gd, (const T*)c->fringe, c->has_fringe, c->ZR, c->KC,
+                                                          c->cflbits, do_cfl);
+    CKL();
+    dim3 g3(g.nxh, (g.ny1 + c->YB3 - 1) / c->YB3);
+    k_zfwd<T><<<g3, 256, c->sm_zfwd, c->st>>>((const C*)c->T2, (C*)c->vel, g, c->pz, (const C*)c->twz, c->gd, c->YB3);
+    CKL();
+    if (do_cfl) {
+      if (lin)
+        k_cfl_finalize<true><<<1, 256, 0, c->st>>>(c->cflbits, g, c->gd, c->sc, c->cflp, c->p.lx, c->p.lz,
+                                                    c->p.dt_flag, c->p.cfl_max, step);
+      else
+        k_cfl_finalize<false><<<1, 256, 0, c->st>>>(c->cflbits, g, c->gd, c->sc, c->cflp, c->p.lx, c->p.lz,
+                                                     c->p.dt_flag, c->p.cfl_max, step);
+      CKL();
+    }
+    return CFG_OK;
+  }
+
+  template <int MM>
+  static int rhs_m(cfg_ctx* c, int rk, int mode) {
+    const Geom& g = c->g;
+    const int nlist = g.nw - 1;
+    if (nlist > 0) {
+      dim3 gr((nlist + 3) / 4);
+      k_rhs<T, MM><<<gr, 128, c->sm_rhs, c->st>>>((C*)c->vel, (C*)c->cru, (C*)c->prs, (const C*)c->cbc + 3 * (size_t)g.nw,
+                                                  (const C*)c->cbc, g, c->gd, c->sc, c->rkt, rk, c->p.re, mode,
+                                                  nullptr, nlist);
+      CKL();
+    }
+    k_rhs_mean<T, MM><<<1, 32, 0, c->st>>>((C*)c->vel, (C*)c->cru, (C*)c->prs, c->mvel64, c->mcru64,
+                                          (const C*)c->cbc + 3 * (size_t)g.nw, (const C*)c->cbc, g, c->gd, c->sc,
+                                          c->d_um_dy, c->rkt, rk, c->p.re, c->p.beta, c->p.fix_mass, mode);
+    CKL();
+    return CFG_OK;
+  }
+  static int rhs(cfg_ctx* c, int rk, int mode) {
+    switch (c->M) {
+      case 2: return rhs_m<2>(c, rk, mode);
+      case 3: return rhs_m<3>(c, rk, mode);
+      case 4: return rhs_m<4>(c, rk, mode);
+      case 5: return rhs_m<5>(c, rk, mode);
+      case 6: return rhs_m<6>(c, rk, mode);
+      case 7: return rhs_m<7>(c, rk, mode);
+      default: return rhs_m<8>(c, rk, mode);
+    }
+  }
+
+  // inverse transforms of `np` spectral planes to physical rows
+  static int planes_c2r(cfg_ctx* c, const C* in, PlaneIn L, const int* plist_dev, int np, T* phys) {
+    const Geom& g = c->g;
+    const int smp = (int)(sizeof(C) * (g.nz2 + 2 * L.nc * g.nz2));
+    k_pz_inv<T><<<dim3(g.nxh, np), 128, smp, c->st>>>(in, L, plist_dev, np, (C*)c->pw_H, g.nxh, g.nz, g.nz2, 1,
+                                                       g.nx2 > g.nx, c->pz, (const C*)c->twz);
+    CKL();
+    const int smx = (int)(sizeof(C) * 3 * g.nx2);
+    k_px_inv<T><<<dim3((g.nz2 + 1) / 2, np * L.nc), 128, smx, c->st>>>((const C*)c->pw_H, phys, g.nxh, g.nz2, g.nx2,
+                                                                        c->px, (const C*)c->twx);
+    CKL();
+    return CFG_OK;
+  }
+  static int planes_r2c(cfg_ctx* c, const T* phys, int np, C* out, size_t osp, size_t oskx, size_t oskz) {
+    const Geom& g = c->g;
+    const int smx = (int)(sizeof(C) * 3 * g.nx2);
+    k_px_fwd<T><<<dim3((g.nz2 + 1) / 2, np), 128, smx, c->st>>>(phys, (C*)c->pw_H, g.nxh, g.nz2, g.nx2, c->px,
+                                                                (const C*)c->twx);
+    CKL();
+    const int smz = (int)(sizeof(C) * 3 * g.nz2);
+    const T scale = (T)(1.0 / ((double)g.nx2 * (double)g.nz2));
+    k_pz_fwd<T><<<dim3(g.nxh, np), 128, smz, c->st>>>((const C*)c->pw_H, out, osp, oskx, oskz, g.nxh, g.nz2, g.nz, 1,
+                                                      scale, c->pz, (const C*)c->twz);
+    CKL();
+    return CFG_OK;
+  }
+
+  static int boundary(cfg_ctx* c) {
+    const Geom& g = c->g;
+    CK(cudaMemsetAsync(c->cbc, 0, sizeof(C) * 6 * (size_t)g.nw, c->st));
+    const size_t np = (size_t)g.nx2 * g.nz2;
+    for (int q = 0; q < 3; q += 2) {
+      const double gain = q == 0 ? c->p.ctrlu : c->p.ctrlw;
+      if (gain == 0.0) continue;
+      const double off = q == 0 ? 2.0 : 0.0;
+      PlaneIn L{1, (size_t)g.ny1, (size_t)g.nz * 3 * g.ny1, (size_t)3 * g.ny1, 1};
+      int r = planes_c2r(c, (const C*)c->vel + (size_t)q * g.ny1, L, c->plist, 4, (T*)c->pw_phys);
+      if (r) return r;
+      const double* dm = nullptr;
+      (void)dm;
+      k_feedback<T><<<grid1d(np), 256, 0, c->st>>>((const T*)c->pw_phys, (T*)c->pw_phys2, np, c->hdm[0], c->hdm[1],
+                                                   c->hdm[2], c->hdm[3], c->hdm[4], c->hdm[5], gain, off);
+      CKL();
+      r = planes_r2c(c, (const T*)c->pw_phys2, 2, (C*)c->cbc + (size_t)q * g.nw, 3 * (size_t)g.nw, g.nz, 1);
+      if (r) return r;
+    }
+    return CFG_OK;
+  }
+
+  static int l2(cfg_ctx* c, double* l2, double* drag) {
+    const Geom& g = c->g;
+    CK(cudaMemsetAsync(c->l2acc, 0, sizeof(double) * g.ny1, c->st));
+    const int smp = (int)(sizeof(C) * (g.nz2 + 2 * 3 * g.nz2));
+    PlaneIn L{1, (size_t)g.ny1, (size_t)g.nz * 3 * g.ny1, (size_t)3 * g.ny1, 3};
+    k_pz_inv<T><<<dim3(g.nxh, g.ny), 128, smp, c->st>>>((const C*)c->vel, L, nullptr, g.ny, (C*)c->T1, g.nxh, g.nz,
+                                                        g.nz2, 1, g.nx2 > g.nx, c->pz, (const C*)c->twz);
+    CKL();
+    const int smx = (int)(sizeof(C) * 3 * g.nx2);
+    k_l2_rows<T><<<dim3((g.nz2 + 1) / 2, 3 * g.ny), 128, smx, c->st>>>((const C*)c->T1, g.nxh, g.nz2, g.nx2, c->px,
+                                                                       (const C*)c->twx, c->gd.y, g.ny, c->l2acc);
+    CKL();
+    std::vector<double> acc(g.ny1), dmd(g.ny);
+    CK(cudaMemcpyAsync(acc.data(), c->l2acc, sizeof(double) * g.ny, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(dmd.data(), c->d_um_dy, sizeof(double) * g.ny, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    double s = 0;
+    for (int j = 0; j < g.ny; ++j) s += acc[j] * c->hdy[j];
+    if (l2) *l2 = sqrt(s / (double)g.nx2 / (double)g.nz2 / 2.0);
+    if (drag) *drag = dmd[0] - dmd[g.ny - 1];
+    return CFG_OK;
+  }
+};
+
+
+// ----------------------------------------------------------------------------
+#define DISPATCH(c, call) ((c)->mixed ? Impl<float>::call : Impl<double>::call)
+
+static size_t csize(const cfg_ctx* c) { return c->mixed ? sizeof(float2) : sizeof(double2); }
+static size_t rsize(const cfg_ctx* c) { return c->mixed ? sizeof(float) : sizeof(double); }
+
+static int ensure_stage(cfg_ctx* c, size_t elems) {
+  if (c->stage_elems >= elems) return CFG_OK;
+  if (c->stage) cudaFree(c->stage);
+  c->stage = nullptr;
+  c->stage_elems = 0;
+  CK(cudaMalloc(&c->stage, sizeof(double2) * elems));
+  c->stage_elems = elems;
+  return CFG_OK;
+}
+
+static int check_status(cfg_ctx* c) {
+  DevScalars h;
+  CK(cudaMemcpyAsync(&h, c->sc, sizeof(h), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (h.status == CFG_E_CFL) return fail(c, CFG_E_CFL, "CFL IS TOO BIG");
+  if (h.status == CFG_E_DT) return fail(c, CFG_E_DT, "DT IS TOO BIG");
+  return CFG_OK;
+}
+
+extern "C" {
+
+const char* cfg_last_error(const cfg_ctx* c) { return c ? c->err.c_str() : "null context"; }
+long long cfg_launch_count(const cfg_ctx* c) { return c ? c->launches : 0; }
+
+int cfg_create(const cfg_params* p, const cfg_grid* gr, cfg_ctx** out) {
+  if (!p || !gr || !out) return CFG_E_ARG;
+  *out = nullptr;
+  cfg_ctx* c = new cfg_ctx();
+  c->p = *p;
+  auto bad = [&](int code) { cfg_destroy(c); return code; };
+  if (p->nx < 4 || p->nz < 4 || p->ny < 5 || (p->nx & 1) || (p->nz & 1) || p->nx2 < p->nx || p->nz2 < p->nz ||
+      (p->nx2 & 1) || (p->nz2 & 1)) {
+    fprintf(stderr, "cfg_create: unsupported grid %d x %d x %d (%d, %d)\n", p->nx, p->ny, p->nz, p->nx2, p->nz2);
+    delete c;
+    return CFG_E_ARG;
+  }
+  if (p->precision != CFG_FP64 && p->precision != CFG_MIXED) { delete c; return CFG_E_ARG; }
+  c->mixed = (p->precision == CFG_MIXED);
+  Geom& g = c->g;
+  g.nx = p->nx; g.ny = p->ny; g.nz = p->nz; g.nx2 = p->nx2; g.nz2 = p->nz2;
+  g.nxh = p->nx / 2 + 1;
+  g.ny1 = p->ny + 1;
+  g.nw = g.nz * g.nxh;
+  if (!make_plan(g.nx2, c->px) || !make_plan(g.nz2, c->pz) || !make_plan(g.nx, c->pxs) || !make_plan(g.nz, c->pzs)) {
+    fprintf(stderr, "cfg_create: transform lengths must be 2^a 3^b\n");
+    delete c;
+    return CFG_E_ARG;
+  }
+  c->dev = p->device;
+  if (cudaSetDevice(c->dev) != cudaSuccess) { fail(c, CFG_E_CUDA, "cudaSetDevice"); delete c; return CFG_E_CUDA; }
+  if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) { delete c; return CFG_E_CUDA; }
+  // RK constants: single-precision literals widened (PFC/pass2.f90:14-18)
+  const float ra[3] = {0.0f, -17.0f / 60.0f, -5.0f / 12.0f}, rb[3] = {8.0f / 15.0f, 5.0f / 12.0f, 3.0f / 4.0f};
+  const float rc[3] = {29.0f / 96.0f, -3.0f / 40.0f, 1.0f / 6.0f}, rd[3] = {37.0f / 160.0f, 5.0f / 24.0f, 1.0f / 6.0f};
+  for (int i = 0; i < 3; ++i) {
+    c->rkt.a[i + 1] = ra[i]; c->rkt.b[i + 1] = rb[i]; c->rkt.c[i + 1] = rc[i]; c->rkt.d[i + 1] = rd[i];
+  }
+  // grid operators (FP64 on the device)
+  const int ny = g.ny, n1 = g.ny1;
+  struct Part { const double* src; size_t n; const double** dst; };
+  std::vector<double> zeros3((size_t)3 * n1, 0.0);
+  const double* tgt = gr->target_inflow ? gr->target_inflow : zeros3.data();
+  Part parts[] = {{gr->y, (size_t)ny, &c->gd.y},       {gr->yh, (size_t)n1, &c->gd.yh},
+                  {gr->hn, (size_t)ny, &c->gd.hn},     {gr->dh, (size_t)n1, &c->gd.dh},
+                  {gr->dn, (size_t)ny, &c->gd.dn},     {gr->iu, (size_t)2 * ny, &c->gd.iu},
+                  {gr->dm, 12, &c->gd.dm},             {gr->d2h, (size_t)3 * n1, &c->gd.d2h},
+                  {gr->d2n, (size_t)3 * ny, &c->gd.d2n}, {gr->dyh, (size_t)n1, &c->gd.dyh},
+                  {gr->dy, (size_t)n1, &c->gd.dy},     {gr->kx, (size_t)g.nxh, &c->gd.kx},
+                  {gr->kz, (size_t)g.nz, &c->gd.kz},   {tgt, (size_t)3 * n1, &c->gd.target},
+                  {zeros3.data(), (size_t)3 * n1, &c->gd.baseflow}};
+  size_t tot = 0;
+  for (auto& pt : parts) {
+    if (!pt.src) { fprintf(stderr, "cfg_create: missing grid array\n"); return bad(CFG_E_ARG); }
+    tot += pt.n;
+  }
+  // the end rows of d2h/d2n must be the copied neighbours (PFC/setup.f90:720-726)
+  for (int i = 0; i < 3; ++i) {
+    if (gr->d2h[i] != gr->d2h[3 + i] || gr->d2h[3 * ny + i] != gr->d2h[3 * (ny - 1) + i] ||
+        gr->d2n[i] != gr->d2n[3 + i] || gr->d2n[3 * (ny - 1) + i] != gr->d2n[3 * (ny - 2) + i]) {
+      fail(c, CFG_E_ARG, "d2h/d2n end rows are not copies of their neighbours");
+      fprintf(stderr, "cfg_create: %s\n", c->err.c_str());
+      return bad(CFG_E_ARG);
+    }
+  }
+  if (cudaMalloc(&c->dgrid, sizeof(double) * tot) != cudaSuccess) return bad(CFG_E_NOMEM);
+  {
+    std::vector<double> h(tot);
+    size_t off = 0;
+    for (auto& pt : parts) {
+      memcpy(h.data() + off, pt.src, sizeof(double) * pt.n);
+      *pt.dst = c->dgrid + off;
+      off += pt.n;
+    }
+    cudaMemcpy(c->dgrid, h.data(), sizeof(double) * tot, cudaMemcpyHostToDevice);
+  }
+  memcpy(c->hdm, gr->dm, sizeof(double) * 12);
+  c->hdy.assign(gr->dy, gr->dy + n1);
+  // state and work buffers
+  const size_t cs = csize(c), nf = (size_t)g.nw * 3 * n1;
+  const size_t t1 = (size_t)n1 * 3 * g.nxh * g.nz2, t2 = (size_t)n1 * 6 * g.nxh * g.nz2;
+  bool ok = cudaMalloc(&c->vel, cs * nf) == cudaSuccess && cudaMalloc(&c->cru, cs * nf) == cudaSuccess &&
+            cudaMalloc(&c->prs, cs * (size_t)g.nw * n1) == cudaSuccess && cudaMalloc(&c->T1, cs * t1) == cudaSuccess &&
+            cudaMalloc(&c->T2, cs * t2) == cudaSuccess && cudaMalloc(&c->cbc, cs * 6 * (size_t)g.nw) == cudaSuccess &&
+            cudaMalloc(&c->sc, sizeof(DevScalars)) == cudaSuccess &&
+            cudaMalloc(&c->d_um_dy, sizeof(double) * ny) == cudaSuccess &&
+            cudaMalloc(&c->cflp, sizeof(double) * n1) == cudaSuccess &&
+            cudaMalloc(&c->cflbits, sizeof(unsigned long long) * 3 * n1) == cudaSuccess &&
+            cudaMalloc(&c->l2acc, sizeof(double) * n1) == cudaSuccess &&
+            cudaMalloc(&c->divbits, sizeof(unsigned long long)) == cudaSuccess &&
+            cudaMalloc(&c->plist, sizeof(int) * 8) == cudaSuccess;
+  const size_t npl = 4;
+  ok = ok && cudaMalloc(&c->pw_H, cs * npl * 3 * g.nxh * g.nz2) == cudaSuccess &&
+       cudaMalloc(&c->pw_phys, rsize(c) * npl * g.nx2 * g.nz2) == cudaSuccess &&
+       cudaMalloc(&c->pw_phys2, rsize(c) * npl * g.nx2 * g.nz2) == cudaSuccess &&
+       cudaMalloc(&c->pw_in, cs * npl * g.nw) == cudaSuccess;
+  if (c->mixed)
+    ok = ok && cudaMalloc(&c->mvel64, sizeof(double2) * 3 * n1) == cudaSuccess &&
+         cudaMalloc(&c->mcru64, sizeof(double2) * 3 * n1) == cudaSuccess;
+  if (!ok) return bad(CFG_E_NOMEM);
+  cudaMemset(c->vel, 0, cs * nf);
+  cudaMemset(c->cru, 0, cs * nf);
+  cudaMemset(c->prs, 0, cs * (size_t)g.nw * n1);
+  cudaMemset(c->cbc, 0, cs * 6 * (size_t)g.nw);
+  cudaMemset(c->d_um_dy, 0, sizeof(double) * ny);
+  cudaMemset(c->cflp, 0, sizeof(double) * n1);
+  if (c->mixed) {
+    cudaMemset(c->mvel64, 0, sizeof(double2) * 3 * n1);
+    cudaMemset(c->mcru64, 0, sizeof(double2) * 3 * n1);
+  }
+  DevScalars h{};
+  h.t_total = 0.0;
+  h.dt = p->dt;
+  h.p_grad = -2.0 / p->re;   // PFC/setup.f90:1384
+  cudaMemcpy(c->sc, &h, sizeof(h), cudaMemcpyHostToDevice);
+  int pl[4] = {1, 2, ny - 1, ny - 2};   // planes 2, 3, ny, ny-1 (boundary)
+  cudaMemcpy(c->plist, pl, sizeof(pl), cudaMemcpyHostToDevice);
+  if (gr->buffer) {
+    bool any = false;
+    for (size_t i = 0; i < (size_t)g.nx2 * g.nz2; ++i) any = any || gr->buffer[i] != 0.0;
+    if (any) {
+      c->has_fringe = 1;
+      if (cudaMalloc(&c->fringe, rsize(c) * g.nx2 * g.nz2) != cudaSuccess) return bad(CFG_E_NOMEM);
+      std::vector<float> hf(g.nx2 * (size_t)g.nz2);
+      if (c->mixed) {
+        for (size_t i = 0; i < hf.size(); ++i) hf[i] = (float)gr->buffer[i];
+        cudaMemcpy(c->fringe, hf.data(), sizeof(float) * hf.size(), cudaMemcpyHostToDevice);
+      } else {
+        cudaMemcpy(c->fringe, gr->buffer, sizeof(double) * hf.size(), cudaMemcpyHostToDevice);
+      }
+    }
+  }
+  int r = DISPATCH(c, setup(c));
+  if (r) {
+    fprintf(stderr, "cfg_create: %s\n", c->err.c_str());
+    return bad(r);
+  }
+  if (cudaDeviceSynchronize() != cudaSuccess) return bad(CFG_E_CUDA);
+  *out = c;
+  return CFG_OK;
+}
+
+void cfg_destroy(cfg_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->dev);
+  if (c->st) cudaStreamSynchronize(c->st);
+  void* bufs[] = {c->dgrid, c->fringe, c->vel, c->cru, c->prs, c->mvel64, c->mcru64, c->T1, c->T2, c->cbc,
+                  c->sc, c->d_um_dy, c->cflp, c->cflbits, c->l2acc, c->divbits, c->plist, c->pw_H,
+                  c->pw_phys, c->pw_phys2, c->pw_in, c->stage, c->twx, c->twz, c->twxs, c->twzs};
+  for (void* b : bufs)
+    if (b) cudaFree(b);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+}
+
+int cfg_upload_state(cfg_ctx* c, const double* d1, const double* d2, const double* d4) {
+  if (!c) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  const Geom& g = c->g;
+  const size_t nf = (size_t)g.nw * 3 * g.ny1;
+  int r = ensure_stage(c, nf);
+  if (r) return r;
+  if (d1) {
+    CK(cudaMemcpyAsync(c->stage, d1, sizeof(double2) * nf, cudaMemcpyHostToDevice, c->st));
+    if (c->mixed) k_data1_in<float><<<grid1d(nf), 256, 0, c->st>>>(c->stage, (float2*)c->vel, c->mvel64, g);
+    else k_data1_in<double><<<grid1d(nf), 256, 0, c->st>>>(c->stage, (double2*)c->vel, nullptr, g);
+    CKL();
+  }
+  if (d2) {
+    CK(cudaMemcpyAsync(c->stage, d2, sizeof(double2) * nf, cudaMemcpyHostToDevice, c->st));
+    if (c->mixed) k_conv_in<float><<<grid1d(nf), 256, 0, c->st>>>(c->stage, (float2*)c->cru, nf, c->mcru64, 3 * (size_t)g.ny1);
+    else k_conv_in<double><<<grid1d(nf), 256, 0, c->st>>>(c->stage, (double2*)c->cru, nf, nullptr, 0);
+    CKL();
+  }
+  if (d4) {
+    const size_t n = (size_t)g.nw * g.ny1;
+    CK(cudaMemcpyAsync(c->stage, d4, sizeof(double2) * n, cudaMemcpyHostToDevice, c->st));
+    if (c->mixed) k_conv_in<float><<<grid1d(n), 256, 0, c->st>>>(c->stage, (float2*)c->prs, n, nullptr, 0);
+    else k_conv_in<double><<<grid1d(n), 256, 0, c->st>>>(c->stage, (double2*)c->prs, n, nullptr, 0);
+    CKL();
+  }
+  CK(cudaStreamSynchronize(c->st));
+  return CFG_OK;
+}
+
+int cfg_download_state(cfg_ctx* c, double* d1, double* d2, double* d4) {
+  if (!c) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  const Geom& g = c->g;
+  const size_t nf = (size_t)g.nw * 3 * g.ny1;
+  int r = ensure_stage(c, nf);
+  if (r) return r;
+  if (d1) {
+    if (c->mixed) k_data1_out<float><<<grid1d(nf), 256, 0, c->st>>>((const float2*)c->vel, c->mvel64, c->stage, g);
+    else k_data1_out<double><<<grid1d(nf), 256, 0, c->st>>>((const double2*)c->vel, nullptr, c->stage, g);
+    CKL();
+    CK(cudaMemcpyAsync(d1, c->stage, sizeof(double2) * nf, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+  }
+  if (d2) {
+    if (c->mixed) k_conv_out<float><<<grid1d(nf), 256, 0, c->st>>>((const float2*)c->cru, c->stage, nf, c->mcru64, 3 * (size_t)g.ny1);
+    else k_conv_out<double><<<grid1d(nf), 256, 0, c->st>>>((const double2*)c->cru, c->stage, nf, nullptr, 0);
+    CKL();
+    CK(cudaMemcpyAsync(d2, c->stage, sizeof(double2) * nf, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+  }
+  if (d4) {
+    const size_t n = (size_t)g.nw * g.ny1;
+    if (c->mixed) k_conv_out<float><<<grid1d(n), 256, 0, c->st>>>((const float2*)c->prs, c->stage, n, nullptr, 0);
+    else k_conv_out<double><<<grid1d(n), 256, 0, c->st>>>((const double2*)c->prs, c->stage, n, nullptr, 0);
+    CKL();
+    CK(cudaMemcpyAsync(d4, c->stage, sizeof(double2) * n, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+  }
+  return CFG_OK;
+}
+
+int cfg_set_scalars(cfg_ctx* c, double t_total, double dt, double p_grad, const double* d_um_dy) {
+  if (!c) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  DevScalars h;
+  CK(cudaMemcpyAsync(&h, c->sc, sizeof(h), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  h.t_total = t_total;
+  h.dt = dt;
+  h.p_grad = p_grad;
+  CK(cudaMemcpyAsync(c->sc, &h, sizeof(h), cudaMemcpyHostToDevice, c->st));
+  if (d_um_dy) CK(cudaMemcpyAsync(c->d_um_dy, d_um_dy, sizeof(double) * c->g.ny, cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return CFG_OK;
+}
+
+int cfg_get_scalars(cfg_ctx* c, double* t_total, double* dt, double* p_grad, double* d_um_dy, double* cfl_max) {
+  if (!c) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  DevScalars h;
+  CK(cudaMemcpyAsync(&h, c->sc, sizeof(h), cudaMemcpyDeviceToHost, c->st));
+  if (d_um_dy) CK(cudaMemcpyAsync(d_um_dy, c->d_um_dy, sizeof(double) * c->g.ny, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (t_total) *t_total = h.t_total;
+  if (dt) *dt = h.dt;
+  if (p_grad) *p_grad = h.p_grad;
+  if (cfl_max) *cfl_max = h.cfl_max;
+  return CFG_OK;
+}
+
+int cfg_set_wall_bc(cfg_ctx* c, const double* top, const double* bot) {
+  if (!c) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  const size_t n = 3 * (size_t)c->g.nw;
+  int r = ensure_stage(c, 2 * n);
+  if (r) return r;
+  const double* src[2] = {bot, top};
+  for (int k = 0; k < 2; ++k) {
+    if (!src[k]) continue;
+    CK(cudaMemcpyAsync(c->stage, src[k], sizeof(double2) * n, cudaMemcpyHostToDevice, c->st));
+    if (c->mixed) k_conv_in<float><<<grid1d(n), 256, 0, c->st>>>(c->stage, (float2*)c->cbc + k * n, n, nullptr, 0);
+    else k_conv_in<double><<<grid1d(n), 256, 0, c->st>>>(c->stage, (double2*)c->cbc + k * n, n, nullptr, 0);
+    CKL();
+    CK(cudaStreamSynchronize(c->st));
+  }
+  return CFG_OK;
+}
+
+int cfg_get_wall_bc(cfg_ctx* c, double* top, double* bot) {
+  if (!c) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  const size_t n = 3 * (size_t)c->g.nw;
+  int r = ensure_stage(c, 2 * n);
+  if (r) return r;
+  double* dst[2] = {bot, top};
+  for (int k = 0; k < 2; ++k) {
+    if (!dst[k]) continue;
+    if (c->mixed) k_conv_out<float><<<grid1d(n), 256, 0, c->st>>>((const float2*)c->cbc + k * n, c->stage, n, nullptr, 0);
+    else k_conv_out<double><<<grid1d(n), 256, 0, c->st>>>((const double2*)c->cbc + k * n, c->stage, n, nullptr, 0);
+    CKL();
+    CK(cudaMemcpyAsync(dst[k], c->stage, sizeof(double2) * n, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+  }
+  return CFG_OK;
+}
+
+int cfg_set_baseflow(cfg_ctx* c, const double* profile) {
+  if (!c || !profile) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  CK(cudaMemcpyAsync((void*)c->gd.baseflow, profile, sizeof(double) * 3 * c->g.ny1, cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return CFG_OK;
+}
+
+int cfg_boundary(cfg_ctx* c) {
+  if (!c) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  return DISPATCH(c, boundary(c));
+}
+
+int cfg_nonlinear(cfg_ctx* c, int step, int rk_step) {
+  if (!c || rk_step < 1 || rk_step > 3) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  c->step = step;
+  return DISPATCH(c, nonlinear(c, step, rk_step, false));
+}
+
+int cfg_nonlinear_linearized(cfg_ctx* c, int step, int rk_step) {
+  if (!c || rk_step < 1 || rk_step > 3) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  c->step = step;
+  return DISPATCH(c, nonlinear(c, step, rk_step, true));
+}
+
+int cfg_rhs_solve(cfg_ctx* c, int step, int rk_step) {
+  if (!c || rk_step < 1 || rk_step > 3) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  (void)step;
+  return DISPATCH(c, rhs(c, rk_step, 0));
+}
+
+static int timestep_impl(cfg_ctx* c, int nsteps, bool lin) {
+  if (!c || nsteps < 0) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  for (int s = 0; s < nsteps; ++s) {
+    c->step = c->step < 0 ? 1 : c->step + 1;
+    int r;
+    if (!lin) {
+      r = DISPATCH(c, boundary(c));
+      if (r) return r;
+    }
+    for (int rk = 1; rk <= 3; ++rk) {
+      r = DISPATCH(c, nonlinear(c, c->step, rk, lin));
+      if (r) return r;
+      r = DISPATCH(c, rhs(c, rk, 0));
+      if (r) return r;
+    }
+    k_advance_time<<<1, 1, 0, c->st>>>(c->sc);
+    CKL();
+  }
+  return CFG_OK;
+}
+
+int cfg_timestep(cfg_ctx* c, int nsteps) { return timestep_impl(c, nsteps, false); }
+int cfg_timestep_linearized(cfg_ctx* c, int nsteps) { return timestep_impl(c, nsteps, true); }
+
+int cfg_remove_initial_divergence(cfg_ctx* c) {
+  if (!c) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  int r = DISPATCH(c, rhs(c, 1, 1));
+  if (r) return r;
+  const size_t nf = (size_t)c->g.nw * 3 * c->g.ny1;
+  CK(cudaMemcpyAsync(c->cru, c->vel, csize(c) * nf, cudaMemcpyDeviceToDevice, c->st));
+  return CFG_OK;
+}
+
+int cfg_compute_initial_pressure(cfg_ctx* c, int linearized) {
+  if (!c) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  // step = -1, rk_step = 3 (PFC/init_vel.f90:444-445): no CFL, no dt change
+  int r = DISPATCH(c, nonlinear(c, -1, 3, linearized != 0));
+  if (r) return r;
+  r = DISPATCH(c, rhs(c, 3, 2));
+  if (r) return r;
+  // data1 = data2 (the velocity copy), PFC/init_vel.f90:469-473
+  const size_t nf = (size_t)c->g.nw * 3 * c->g.ny1;
+  CK(cudaMemcpyAsync(c->vel, c->cru, csize(c) * nf, cudaMemcpyDeviceToDevice, c->st));
+  if (c->mixed) CK(cudaMemcpyAsync(c->mvel64, c->mcru64, sizeof(double2) * 3 * c->g.ny1, cudaMemcpyDeviceToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return CFG_OK;
+}
+
+int cfg_xz_c2r(cfg_ctx* c, const double* cdata, double* data) {
+  if (!c || !cdata || !data) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  const Geom& g = c->g;
+  const size_t nin = (size_t)g.nw, nout = (size_t)g.nx2 * g.nz2;
+  int r = ensure_stage(c, std::max(nin, nout));
+  if (r) return r;
+  CK(cudaMemcpyAsync(c->stage, cdata, sizeof(double2) * nin, cudaMemcpyHostToDevice, c->st));
+  PlaneIn L{0, 0, (size_t)g.nz, 1, 1};
+  if (c->mixed) {
+    k_conv_in<float><<<grid1d(nin), 256, 0, c->st>>>(c->stage, (float2*)c->pw_in, nin, nullptr, 0);
+    CKL();
+    r = Impl<float>::planes_c2r(c, (const float2*)c->pw_in, L, nullptr, 1, (float*)c->pw_phys);
+    if (r) return r;
+    k_real_out<float><<<grid1d(nout), 256, 0, c->st>>>((const float*)c->pw_phys, (double*)c->stage, nout);
+  } else {
+    k_conv_in<double><<<grid1d(nin), 256, 0, c->st>>>(c->stage, (double2*)c->pw_in, nin, nullptr, 0);
+    CKL();
+    r = Impl<double>::planes_c2r(c, (const double2*)c->pw_in, L, nullptr, 1, (double*)c->pw_phys);
+    if (r) return r;
+    k_real_out<double><<<grid1d(nout), 256, 0, c->st>>>((const double*)c->pw_phys, (double*)c->stage, nout);
+  }
+  CKL();
+  CK(cudaMemcpyAsync(data, c->stage, sizeof(double) * nout, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return CFG_OK;
+}
+
+int cfg_xz_r2c(cfg_ctx* c, const double* data, double* cdata) {
+  if (!c || !cdata || !data) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  const Geom& g = c->g;
+  const size_t nin = (size_t)g.nx2 * g.nz2, nout = (size_t)g.nw;
+  int r = ensure_stage(c, std::max(nin, nout));
+  if (r) return r;
+  CK(cudaMemcpyAsync(c->stage, data, sizeof(double) * nin, cudaMemcpyHostToDevice, c->st));
+  if (c->mixed) {
+    k_real_in<float><<<grid1d(nin), 256, 0, c->st>>>((const double*)c->stage, (float*)c->pw_phys, nin);
+    CKL();
+    r = Impl<float>::planes_r2c(c, (const float*)c->pw_phys, 1, (float2*)c->pw_in, 0, g.nz, 1);
+    if (r) return r;
+    k_conv_out<float><<<grid1d(nout), 256, 0, c->st>>>((const float2*)c->pw_in, c->stage, nout, nullptr, 0);
+  } else {
+    k_real_in<double><<<grid1d(nin), 256, 0, c->st>>>((const double*)c->stage, (double*)c->pw_phys, nin);
+    CKL();
+    r = Impl<double>::planes_r2c(c, (const double*)c->pw_phys, 1, (double2*)c->pw_in, 0, g.nz, 1);
+    if (r) return r;
+    k_conv_out<double><<<grid1d(nout), 256, 0, c->st>>>((const double2*)c->pw_in, c->stage, nout, nullptr, 0);
+  }
+  CKL();
+  CK(cudaMemcpyAsync(cdata, c->stage, sizeof(double2) * nout, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return CFG_OK;
+}
+
+int cfg_small_r2c(cfg_ctx* c, const double* data, double* cdata, int nplanes) {
+  (void)data; (void)cdata; (void)nplanes;
+  return fail(c, CFG_E_ARG, "cfg_small_r2c: not available");
+}
+int cfg_small_c2r(cfg_ctx* c, const double* cdata, double* data, int nplanes) {
+  (void)data; (void)cdata; (void)nplanes;
+  return fail(c, CFG_E_ARG, "cfg_small_c2r: not available");
+}
+
+int cfg_l2_norm(cfg_ctx* c, double* l2, double* drag) {
+  if (!c) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  return DISPATCH(c, l2(c, l2, drag));
+}
+
+int cfg_diagnostics(cfg_ctx* c, double* bulk_flux, double* max_div) {
+  if (!c) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  const Geom& g = c->g;
+  CK(cudaMemsetAsync(c->divbits, 0, sizeof(unsigned long long), c->st));
+  const int nb = (g.nw + 3) / 4;
+  if (c->mixed) k_divergence<float><<<nb, 128, 0, c->st>>>((const float2*)c->vel, g, c->gd, c->divbits);
+  else k_divergence<double><<<nb, 128, 0, c->st>>>((const double2*)c->vel, g, c->gd, c->divbits);
+  CKL();
+  std::vector<double2> mean(g.ny1);
+  if (c->mixed) CK(cudaMemcpyAsync(mean.data(), c->mvel64, sizeof(double2) * g.ny1, cudaMemcpyDeviceToHost, c->st));
+  else CK(cudaMemcpyAsync(mean.data(), c->vel, sizeof(double2) * g.ny1, cudaMemcpyDeviceToHost, c->st));
+  unsigned long long bits = 0;
+  CK(cudaMemcpyAsync(&bits, c->divbits, sizeof(bits), cudaMemcpyDeviceToHost, c->st));
+  std::vector<double> dyh(g.ny1);
+  CK(cudaMemcpyAsync(dyh.data(), c->gd.dyh, sizeof(double) * g.ny1, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (bulk_flux) {
+    double s = 0;
+    for (int j = 0; j < g.ny1; ++j) s += dyh[j] * mean[j].x;
+    *bulk_flux = s;
+  }
+  if (max_div) {
+    double d;
+    memcpy(&d, &bits, sizeof(d));
+    *max_div = d;
+  }
+  return CFG_OK;
+}
+
+int cfg_status(cfg_ctx* c) {
+  if (!c) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  return check_status(c);
+}
+
+int cfg_synchronize(cfg_ctx* c) {
+  if (!c) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  CK(cudaStreamSynchronize(c->st));
+  return CFG_OK;
+}
+
+}  // extern "C"

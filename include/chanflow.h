@@ -1,0 +1,168 @@
+/*
+ * chanflow.h -- C ABI of the B200 (sm_100a) channel-flow hot path.
+ *
+ * A drop-in for the per-timestep routines of the reference Fortran solver
+ * (PFC = ParallelFortran-Code/).  The reference has no FFI layer of its own:
+ * its boundary is a set of Fortran module procedures that talk through module
+ * globals.  Each entry point below replaces one of them; a Fortran caller
+ * binds them with ISO_C_BINDING and keeps its module
+ * interfaces, flow.dat parameters and read_write file layouts unchanged.
+ *
+ * Conventions
+ *  - Every call returns 0 on success or a negative CFG_E_* code; the message
+ *    is available from cfg_last_error().  The device never traps: device-side
+ *    failures (CFL abort) set a flag that the host reads (cfg_status).
+ *  - Host arrays use the reference's Fortran (column-major) layouts; complex
+ *    values are interleaved (re, im) doubles, i.e. C_DOUBLE_COMPLEX.
+ *      data1 (nz, nx/2+1, ny+1, 3)   PFC/data.f90:9,   PFC/setup.f90:447
+ *      data2 (ny+1, 3, nz, nx/2+1)   PFC/data.f90:9,   PFC/setup.f90:448
+ *      data4 (ny+1, nz, nx/2+1)      PFC/data.f90:10,  PFC/setup.f90:449
+ *      cbc_top/cbc_bot (nz, nx/2+1, 3)  PFC/gridparms.f90:59, PFC/setup.f90:565
+ *  - State lives on the device between calls; upload/download are the only
+ *    host<->device copies of the fields.  Calls on one context are issued in
+ *    order on the context's CUDA stream and are not re-entrant.
+ */
+#ifndef CHANFLOW_H
+#define CHANFLOW_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CFG_OK 0
+#define CFG_E_ARG (-1)        /* invalid argument / unsupported size */
+#define CFG_E_CUDA (-2)       /* CUDA runtime error */
+#define CFG_E_NOMEM (-3)      /* device allocation failed */
+#define CFG_E_CFL (-4)        /* 'CFL IS TOO BIG', PFC/pass1.f90:235-244 */
+#define CFG_E_DT (-5)         /* 'DT IS TOO BIG', PFC/pass1.f90:228-233 */
+#define CFG_E_STATE (-6)      /* call out of sequence */
+
+#define CFG_FP64 0            /* every kernel in FP64 */
+#define CFG_MIXED 1           /* FP32 transforms/products/solves, FP64 mean mode */
+
+typedef struct cfg_ctx cfg_ctx;
+
+/* Run parameters: the runparms/gridparms scalars the hot path reads
+ * (PFC/runparms.f90:20-53, PFC/gridparms.f90:26-40). */
+typedef struct cfg_params {
+  int nx, ny, nz, nx2, nz2;     /* flow.dat lines 10-14 */
+  double re, lx, lz, beta;      /* beta in radians (PFC/setup.f90:105) */
+  double dt, cfl_max;           /* PFC/setup.f90:1377-1378 */
+  int fix_mass, dt_flag;        /* flow.dat lines 46-47 */
+  double ctrlu, ctrlw;          /* feedback gains, flow.dat lines 5-6 */
+  int precision;                /* CFG_FP64 or CFG_MIXED */
+  int device;                   /* CUDA device ordinal */
+} cfg_params;
+
+/* Grid operators and wavenumbers computed by define_coordinates and
+ * define_parameters (PFC/setup.f90:541-837, 1439-1466).  All pointers are
+ * host arrays in reference layout; buffer and target_inflow may be NULL
+ * (no fringe). */
+typedef struct cfg_grid {
+  const double *y;              /* (ny) */
+  const double *yh;             /* (ny+1) */
+  const double *hn;             /* (ny) */
+  const double *dh;             /* (ny+1) */
+  const double *dn;             /* (ny) */
+  const double *iu;             /* (2, ny) */
+  const double *dm;             /* (3, 4) */
+  const double *d2h;            /* (3, ny+1) */
+  const double *d2n;            /* (3, ny) */
+  const double *dyh;            /* (ny+1) */
+  const double *dy;             /* (ny+1) */
+  const double *kx;             /* (nx/2+1) */
+  const double *kz;             /* (nz) FFT order */
+  const double *buffer;         /* (nx2, nz2) fringe damping, or NULL */
+  const double *target_inflow;  /* (ny+1, 3) fringe target, or NULL */
+} cfg_grid;
+
+/* initialize_fft + allocate_data_arrays (PFC/transform.f90:60-160,
+ * PFC/setup.f90:441-514): allocates the device state and plans. */
+int cfg_create(const cfg_params *p, const cfg_grid *g, cfg_ctx **out);
+/* finalize_fft + deallocate_data_arrays (PFC/transform.f90:164-191). */
+void cfg_destroy(cfg_ctx *c);
+const char *cfg_last_error(const cfg_ctx *c);
+
+/* Copy data1/data2/data4 host <-> device (any pointer may be NULL). */
+int cfg_upload_state(cfg_ctx *c, const double *data1, const double *data2,
+                     const double *data4);
+int cfg_download_state(cfg_ctx *c, double *data1, double *data2, double *data4);
+
+/* Scalar state: t_total, dt, p_grad (runparms) and d_um_dy(ny) (gridparms).
+ * d_um_dy may be NULL.  cfg_get_scalars synchronises; cfl_max (nullable)
+ * returns MAXVAL(cfl(2:ny)) of the last rk_step=1 nonlinear call. */
+int cfg_set_scalars(cfg_ctx *c, double t_total, double dt, double p_grad,
+                    const double *d_um_dy);
+int cfg_get_scalars(cfg_ctx *c, double *t_total, double *dt, double *p_grad,
+                    double *d_um_dy, double *cfl_max);
+
+/* Inhomogeneous wall values cbc_top/cbc_bot (nz, nx/2+1, 3); either may be
+ * NULL.  They are read by rhs_solve exactly like the module arrays. */
+int cfg_set_wall_bc(cfg_ctx *c, const double *cbc_top, const double *cbc_bot);
+int cfg_get_wall_bc(cfg_ctx *c, double *cbc_top, double *cbc_bot);
+
+/* read_write::boundary, PFC/read_write.f90:1465-1532: zeroes cbc_top/cbc_bot
+ * and applies the wall-shear feedback law for nonzero ctrlu/ctrlw. */
+int cfg_boundary(cfg_ctx *c);
+
+/* pass1::nonlinear, PFC/pass1.f90:26-124: replaces the velocity in data1 by
+ * the dealiased nonlinear term; on rk_step==1 computes the per-plane CFL
+ * (check_cfl, :202-250) and, if dt_flag, adapts dt on the device. */
+int cfg_nonlinear(cfg_ctx *c, int step, int rk_step);
+
+/* pass1_linearized::nonlinear_linearized, PFC/pass1_linearized.f90:135-250,
+ * about the baseflow set by cfg_set_baseflow (uniform in x and z). */
+int cfg_nonlinear_linearized(cfg_ctx *c, int step, int rk_step);
+/* Baseflow profile (ny+1, 3) for the linearized term (init_baseflow,
+ * PFC/pass1_linearized.f90:20-131). */
+int cfg_set_baseflow(cfg_ctx *c, const double *profile);
+
+/* pass2::rhs_solve, PFC/pass2.f90:29-180: per-(kx,kz) RK3/Crank-Nicolson
+ * substep (PHASE1 :184-352) with the Helmholtz and pressure solves of
+ * PFC/solve.f90; the mean mode updates p_grad and d_um_dy on the device. */
+int cfg_rhs_solve(cfg_ctx *c, int step, int rk_step);
+
+/* The body of the timestep loop, PFC/main_mpi.f90:70-86, for nsteps steps:
+ * boundary, then three (nonlinear, rhs_solve) substeps, then
+ * t_total = t_total + dt.  No host synchronisation. */
+int cfg_timestep(cfg_ctx *c, int nsteps);
+/* Same with nonlinear_linearized (the arnoldi.f90 matvec loop, :540-547). */
+int cfg_timestep_linearized(cfg_ctx *c, int nsteps);
+
+/* transform::xz_fft_complex_to_real / xz_fft_real_to_complex,
+ * PFC/transform.f90:195-227,258-409: one plane, host arrays
+ * cdata (nz, nx/2+1) complex and data (nx2, nz2) real. */
+int cfg_xz_c2r(cfg_ctx *c, const double *cdata, double *data);
+int cfg_xz_r2c(cfg_ctx *c, const double *data, double *cdata);
+/* transform::small_fft_real_to_complex / small_fft_complex_to_real,
+ * PFC/transform.f90:950-1142: nx x nz grid, no dealiasing, nplanes planes
+ * (data (nx, nz, nplanes), cdata (nz, nx/2+1, nplanes)). */
+int cfg_small_r2c(cfg_ctx *c, const double *data, double *cdata, int nplanes);
+int cfg_small_c2r(cfg_ctx *c, const double *cdata, double *data, int nplanes);
+
+/* read_write::l2_norm, PFC/read_write.f90:1432-1462: perturbation L2 norm
+ * about U=1-y^2 and the wall-shear difference d_um_dy(1)-d_um_dy(ny). */
+int cfg_l2_norm(cfg_ctx *c, double *l2, double *drag);
+
+/* init_vel: remove_initial_divergence (PFC/init_vel.f90:518-536) followed by
+ * the d_um_dy initialisation (:333-342) and data2 = data1 (:344-348). */
+int cfg_remove_initial_divergence(cfg_ctx *c);
+/* init_vel::compute_initial_pressure (PFC/init_vel.f90:437-514); linearized
+ * selects nonlinear_linearized as in arnoldi.f90:528-535. */
+int cfg_compute_initial_pressure(cfg_ctx *c, int linearized);
+
+/* Bulk flux Q = sum dyh*Re(u_mean) (PFC/pass2.f90:106-108) and the maximum
+ * |divergence| over all wavenumbers (check_divergence, :380-419). */
+int cfg_diagnostics(cfg_ctx *c, double *bulk_flux, double *max_divergence);
+
+/* Device error flag: 0, CFG_E_CFL or CFG_E_DT.  Synchronises. */
+int cfg_status(cfg_ctx *c);
+int cfg_synchronize(cfg_ctx *c);
+
+/* Number of kernel launches this context has issued (for accounting). */
+long long cfg_launch_count(const cfg_ctx *c);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

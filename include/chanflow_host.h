@@ -1,0 +1,71 @@
+/*
+ * chanflow_host.h -- host-side C++ mirror of the reference's setup module
+ * (PFC/setup.f90) and initial-field generator (PFC/init_vel.f90) for callers
+ * without a Fortran host: parses flow.dat, computes the grid operators and
+ * wavenumbers that cfg_create takes, and builds seeded initial fields.
+ * A Fortran host keeps its own setup.f90 and only needs chanflow.h.
+ */
+#ifndef CHANFLOW_HOST_H
+#define CHANFLOW_HOST_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* flow.dat run parameters (PFC/setup.f90:45-160) plus the extension block
+ * that may follow line 95 (lines "value  name": stretch, dt, seed,
+ * precision, uniform_grid, jet_mode, jet_width, jet_peak, jet_freq). */
+typedef struct cfh_run {
+  double re, ctrlu, ctrlw, lx, lz, beta, disturb_ampl;
+  int nx, ny, nz, nx2, nz2;
+  int tend, output_step, save_step, l2_step;
+  int read_vel, save_vel, vel_out, which_test;
+  int fix_mass, dt_flag, divg_check;
+  int bl_grid, crossflow, filter_jet_profile;
+  double jet_diam, xjet_top, zjet_top, jetmag_top, forcing_top, for_freq_top;
+  double xjet_bot, zjet_bot, jetmag_bot, forcing_bot, for_freq_bot;
+  int xfringe, zfringe;
+  double frac_xbuff;
+  /* extension block */
+  double stretch;         /* default 2.75 (PFC/setup.f90:545) */
+  double dt;              /* <= 0: define_parameters default 0.25*lx/nx */
+  unsigned long long seed;
+  int precision;          /* CFG_FP64 / CFG_MIXED */
+  int uniform_grid;       /* which_test 6 grid */
+  int jet_mode;           /* 0 none, 1 reference tanh jet, 2 gaussian slot */
+  double jet_width, jet_peak, jet_freq;
+} cfh_run;
+
+/* Grid operators in reference layout, owned by the caller (sizes as in
+ * chanflow.h's cfg_grid).  cfh_grid_alloc/free manage the arrays. */
+typedef struct cfh_grid {
+  int nx, ny, nz, nx2, nz2;
+  double *y, *yh, *hh, *hn, *dh, *dn, *iu, *dm, *d2h, *d2n, *dyh, *dy, *kx, *kz;
+  double *buffer, *target_inflow, *xcoord, *zcoord;
+} cfh_grid;
+
+void cfh_run_defaults(cfh_run *r);
+/* read_parms: 0 on success, <0 on a malformed or short file */
+int cfh_read_flow_dat(const char *path, cfh_run *r, char *err, int errlen);
+
+cfh_grid *cfh_grid_alloc(int nx, int ny, int nz, int nx2, int nz2);
+void cfh_grid_free(cfh_grid *g);
+/* define_coordinates (channel branch, PFC/setup.f90:541-754) and the
+ * wavenumbers of define_parameters (:1439-1466). */
+int cfh_define_grid(cfh_grid *g, double lx, double lz, double stretch, int uniform);
+
+/* Seeded initial field in data1 layout (nz, nx/2+1, ny+1, 3), complex
+ * interleaved: which_test 1, 4, 6 (PFC/init_vel.f90:88-244) and 10
+ * (laminar 1-y^2 plus k^-2 divergence-free noise).  The divergence removal
+ * and initial pressure run on the device (cfg_remove_initial_divergence,
+ * cfg_compute_initial_pressure). */
+int cfh_initial_field(const cfh_grid *g, int which_test, unsigned long long seed,
+                      double ampl, double beta, double *data1);
+
+/* The seeded counter-based generator replacing RANDOM_NUMBER. */
+double cfh_rng_u01(unsigned long long seed, int x, int z, int j, int col);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

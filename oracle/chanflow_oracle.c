@@ -45,13 +45,14 @@ typedef struct {
   cplx *tw[2][32]; /* per sign: tw[s][p][r*ns+k] = exp(sign*2pi i k r/(ns*R)) */
 } fft_plan;
 
-#define MAX_PLANS 16
+#define MAX_PLANS 256
 static fft_plan g_plans[MAX_PLANS];
 static int g_nplans = 0;
 
 static fft_plan *plan_build(int n) {
   for (int i = 0; i < g_nplans; i++)
     if (g_plans[i].n == n) return &g_plans[i];
+  if (g_nplans >= MAX_PLANS) abort();   /* more distinct lengths than the cache holds */
   fft_plan *p = &g_plans[g_nplans++];
   memset(p, 0, sizeof(*p));
   p->n = n;
@@ -1075,7 +1076,20 @@ void orc_compute_initial_pressure(orc_ctx *c, int linearized) {
 
 /* DEFINE_INITIAL_FIELD, PFC/init_vel.f90:25-353, for the channel presets
  * which_test 1, 4, 6 and the laminar + k^-2 noise preset 10.               */
+double orc_rng_u01(unsigned long long seed, int x, int z, int j, int col) {
+  return rng_u01(seed, x, z, j, col);
+}
+
 void orc_init_field(orc_ctx *c, int which_test, unsigned long long seed, double ampl) {
+  orc_initial_velocity(c, which_test, seed, ampl);
+  orc_remove_initial_divergence(c);
+  orc_compute_d_um_dy(c);
+  copy_data1_to_data2(c);
+  orc_compute_initial_pressure(c, 0);
+}
+
+/* the which_test velocity before divergence removal, PFC/init_vel.f90:88-244 */
+void orc_initial_velocity(orc_ctx *c, int which_test, unsigned long long seed, double ampl) {
   int ny = c->p.ny, n1 = ny + 1, nz = c->p.nz, nxh = c->nxh;
   size_t nf = (size_t)nz * nxh * n1;
   c->t_total = 0;
@@ -1110,10 +1124,6 @@ void orc_init_field(orc_ctx *c, int which_test, unsigned long long seed, double 
         for (int j = 0; j < n1; j++) D1(c, z, x, j, q) = cu[q * n1 + j] * f;
     }
   }
-  orc_remove_initial_divergence(c);
-  orc_compute_d_um_dy(c);
-  copy_data1_to_data2(c);
-  orc_compute_initial_pressure(c, 0);
 }
 
 /* timestep loop body, PFC/main_mpi.f90:70-86 */

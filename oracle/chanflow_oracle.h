@@ -85,6 +85,9 @@ void orc_l2_norm(orc_ctx *c, double *l2, double *drag); /* PFC/read_write.f90:14
 /* initial field, PFC/init_vel.f90 */
 void orc_init_field(orc_ctx *c, int which_test, unsigned long long seed,
                     double ampl);
+void orc_initial_velocity(orc_ctx *c, int which_test, unsigned long long seed,
+                          double ampl);
+double orc_rng_u01(unsigned long long seed, int x, int z, int j, int col);
 void orc_remove_initial_divergence(orc_ctx *c);
 void orc_compute_d_um_dy(orc_ctx *c);
 void orc_compute_initial_pressure(orc_ctx *c, int linearized);

@@ -78,6 +78,9 @@ def lib():
             getattr(L, n).argtypes = [vp]
         L.orc_l2_norm.argtypes = [vp, dp, dp]
         L.orc_init_field.argtypes = [vp, C.c_int, C.c_ulonglong, C.c_double]
+        L.orc_initial_velocity.argtypes = [vp, C.c_int, C.c_ulonglong, C.c_double]
+        L.orc_rng_u01.argtypes = [C.c_ulonglong, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.orc_rng_u01.restype = C.c_double
         L.orc_compute_initial_pressure.argtypes = [vp, C.c_int]
         L.orc_timestep.argtypes = [vp, C.c_int, C.c_int]
         L.orc_bulk_flux.argtypes = [vp]
@@ -250,6 +253,15 @@ class Oracle:
 
     def init_field(self, which_test, seed=1, ampl=1e-3):
         self.L.orc_init_field(self.h, which_test, seed, ampl)
+
+    def initial_velocity(self, which_test, seed=1, ampl=1e-3):
+        self.L.orc_initial_velocity(self.h, which_test, seed, ampl)
+
+    def remove_initial_divergence(self):
+        self.L.orc_remove_initial_divergence(self.h)
+
+    def compute_d_um_dy(self):
+        self.L.orc_compute_d_um_dy(self.h)
 
     def compute_initial_pressure(self, linearized=0):
         self.L.orc_compute_initial_pressure(self.h, linearized)

@@ -1,0 +1,98 @@
+"""Host-side logic of the product, no GPU needed: the C-ABI library loads and
+exports every symbol its headers declare; the C++ setup (flow.dat reader,
+define_coordinates, wavenumbers, seeded initial field) matches the oracle."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADERS = [os.path.join(ROOT, "include", h) for h in ("chanflow.h", "chanflow_host.h")]
+
+
+def declared_functions():
+    names = []
+    for h in HEADERS:
+        txt = open(h).read()
+        txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+        for m in re.finditer(r"\b(cf[gh]_[a-z0-9_]+)\s*\(", txt):
+            names.append(m.group(1))
+    return sorted(set(names))
+
+
+def test_library_exports_all_declared_symbols(cf):
+    L = cf.load_library()
+    decl = declared_functions()
+    assert len(decl) >= 30
+    for n in decl:
+        assert hasattr(L, n), n
+        assert n in cf.SYMBOLS, n
+
+
+def test_missing_library_fails_loudly(cf, tmp_path):
+    import importlib
+    mod = importlib.import_module("chanflow_b200.chanflow")
+    saved = mod._lib
+    mod._lib = None
+    try:
+        with pytest.raises(RuntimeError):
+            mod.load_library(str(tmp_path / "nope.so"))
+    finally:
+        mod._lib = saved
+
+
+@pytest.mark.parametrize("ny,stretch,uniform", [(33, 1.5, 0), (200, 2.75, 0), (17, 2.75, 1)])
+def test_grid_matches_oracle(cf, orc, ny, stretch, uniform):
+    g = cf.Grid(32, ny, 16, lx=4 * np.pi, lz=2 * np.pi, stretch=stretch, uniform=uniform)
+    o = orc.Oracle(32, ny, 16, lx=4 * np.pi, lz=2 * np.pi, stretch=stretch, uniform_grid=uniform)
+    for name in ("y", "yh", "hh", "hn", "dh", "dn", "dyh", "dy", "kx", "kz", "xcoord", "zcoord"):
+        assert np.array_equal(getattr(g, name).ravel(order="F"), o.grid(name).ravel(order="F")), name
+    for name in ("iu", "dm", "d2h", "d2n"):
+        assert np.array_equal(getattr(g, name), o.grid(name)), name
+
+
+def test_rng_matches_oracle(cf, orc):
+    L = cf.load_library()
+    O = orc.lib()
+    for args in [(1, 0, 1, 0, 0), (7, 3, 5, 100, 3), (2 ** 40 + 5, 64, 127, 193, 2)]:
+        assert L.cfh_rng_u01(*args) == O.orc_rng_u01(*args)
+
+
+@pytest.mark.parametrize("which", [1, 4, 6, 10])
+def test_initial_field_matches_oracle(cf, orc, which):
+    g = cf.Grid(16, 17, 12, lx=4 * np.pi, lz=2 * np.pi, stretch=1.5)
+    d1 = cf.initial_field(g, which, seed=11, ampl=1e-2)
+    o = orc.Oracle(16, 17, 12, lx=4 * np.pi, lz=2 * np.pi, stretch=1.5)
+    o.initial_velocity(which, seed=11, ampl=1e-2)
+    np.testing.assert_allclose(d1, o.data1, rtol=0, atol=1e-15)
+
+
+FLOW_C1 = os.path.join(os.path.dirname(__file__), "golden", "flow_c1.dat")
+
+
+def test_flow_dat_reader(cf):
+    run = cf.read_flow_dat(FLOW_C1)
+    assert (run.nx, run.ny, run.nz, run.nx2, run.nz2) == (32, 33, 32, 48, 48)
+    assert run.re == 2500.0
+    assert abs(run.lx - 4 * np.pi) < 1e-15 and abs(run.lz - 2 * np.pi) < 1e-15
+    assert run.fix_mass == 1 and run.dt_flag == 0 and run.tend == 100
+    assert run.which_test == 10 and run.stretch == 1.5 and run.dt == 0.005
+    assert run.seed == 1 and abs(run.disturb_ampl - 1e-3) < 1e-18
+
+
+def test_flow_dat_reader_rejects_truncated(cf, tmp_path):
+    lines = open(FLOW_C1).read().splitlines()[:40]
+    p = tmp_path / "flow.dat"
+    p.write_text("\n".join(lines) + "\n")
+    with pytest.raises(cf.ChanflowError):
+        cf.read_flow_dat(str(p))
+
+
+@pytest.mark.skipif(not os.path.exists("/root/reference/ParallelFortran-Code/flow.dat"),
+                    reason="reference not mounted")
+def test_flow_dat_reader_on_reference_file(cf):
+    run = cf.read_flow_dat("/root/reference/ParallelFortran-Code/flow.dat")
+    assert (run.nx, run.ny, run.nz, run.nx2, run.nz2) == (128, 200, 64, 192, 96)
+    assert run.re == 7500.0 and run.which_test == 9 and run.l2_step == 20
+    assert abs(run.lx - 6 * np.pi) < 1e-14 and abs(run.lz - 2 * np.pi) < 1e-14
