@@ -109,6 +109,9 @@ SYMBOLS = {
     "cfg_status": (C.c_int, [_VP]),
     "cfg_synchronize": (C.c_int, [_VP]),
     "cfg_launch_count": (C.c_longlong, [_VP]),
+    "cfg_stream": (_VP, [_VP]),
+    "cfg_profile_enable": (C.c_int, [_VP, C.c_int]),
+    "cfg_profile_read": (C.c_int, [_VP, C.c_int, C.c_char_p, C.c_int, C.POINTER(C.c_int), _DP]),
     "cfh_run_defaults": (None, [C.POINTER(CfhRun)]),
     "cfh_read_flow_dat": (C.c_int, [C.c_char_p, C.POINTER(CfhRun), C.c_char_p, C.c_int]),
     "cfh_grid_alloc": (C.POINTER(CfhGrid), [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
@@ -350,6 +353,26 @@ class ChannelFlow:
 
     def launch_count(self):
         return self.L.cfg_launch_count(self.h)
+
+    def stream_ptr(self):
+        """The cudaStream_t this context issues its kernels on."""
+        return self.L.cfg_stream(self.h)
+
+    def profile_enable(self, on=True):
+        self._chk(self.L.cfg_profile_enable(self.h, 1 if on else 0))
+
+    def profile_read(self):
+        """{kernel name: (launches, total device ms)} since profile_enable."""
+        n = self.L.cfg_profile_read(self.h, -1, None, 0, None, None)
+        if n < 0:
+            self._chk(n)
+        out = {}
+        for i in range(n):
+            name = C.create_string_buffer(64)
+            cnt, ms = C.c_int(), C.c_double()
+            self._chk(self.L.cfg_profile_read(self.h, i, name, 64, C.byref(cnt), C.byref(ms)))
+            out[name.value.decode()] = (cnt.value, ms.value)
+        return out
 
     # ---- define_initial_field (PFC/init_vel.f90:25-353) on the device
     def define_initial_field(self, which_test, seed=1, ampl=1e-3, beta=0.0):

@@ -138,7 +138,46 @@ struct cfg_ctx {
   RkTab rkt{};
   double hdm[12] = {0};
   std::vector<double> hdy;
+  // mixed precision: whether mvel64 holds the current data1 mean column (it
+  // does not while data1 holds the nonlinear term)
+  bool mean64_valid = true;
+  // wavenumber lists for the rhs kernels: fast (arithmetic in the storage
+  // precision) and, in mixed precision, |k| < 4 solved in FP64
+  int* wl_fast = nullptr;
+  int* wl_prec = nullptr;
+  int n_fast = 0, n_prec = 0;
+  size_t sm_rhs64 = 0;
+  // optional per-launch CUDA-event timing on the context stream
+  bool prof_on = false;
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  struct Rec { const char* name; cudaEvent_t a, b; };
+  std::vector<Rec> recs;
+  const char* cur_name = nullptr;
+  cudaEvent_t cur_a = nullptr;
 };
+
+static cudaEvent_t prof_event(cfg_ctx* c) {
+  if (c->ev_used == c->ev_pool.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    c->ev_pool.push_back(e);
+  }
+  return c->ev_pool[c->ev_used++];
+}
+static void prof_begin(cfg_ctx* c, const char* name) {
+  if (!c->prof_on) return;
+  c->cur_name = name;
+  c->cur_a = prof_event(c);
+  cudaEventRecord(c->cur_a, c->st);
+}
+static void prof_end(cfg_ctx* c) {
+  if (!c->prof_on || !c->cur_name) return;
+  cudaEvent_t b = prof_event(c);
+  cudaEventRecord(b, c->st);
+  c->recs.push_back({c->cur_name, c->cur_a, b});
+  c->cur_name = nullptr;
+}
 
 static int fail(cfg_ctx* c, int code, const char* fmt, ...) {
   char buf[512];
@@ -157,6 +196,7 @@ static int fail(cfg_ctx* c, int code, const char* fmt, ...) {
 #define CKL()                                                                            \
   do {                                                                                   \
     c->launches++;                                                                       \
+    prof_end(c);                                                                         \
     cudaError_t e_ = cudaGetLastError();                                                 \
     if (e_ != cudaSuccess) return fail(c, CFG_E_CUDA, "launch: %s", cudaGetErrorString(e_)); \
   } while (0)
@@ -240,7 +280,9 @@ struct Impl {
 #define RHS_ATTR(MM)                                                                              \
   case MM:                                                                                        \
     c->sm_rhs = 4 * 5 * ColIdx<MM>::SIZE * cs;                                                   \
-    CK(cudaFuncSetAttribute(k_rhs<T, MM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_rhs)); \
+    c->sm_rhs64 = 4 * 5 * ColIdx<MM>::SIZE * sizeof(double2);                                    \
+    CK(cudaFuncSetAttribute(k_rhs<T, T, MM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_rhs)); \
+    CK(cudaFuncSetAttribute(k_rhs<double, T, MM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_rhs64)); \
     break;
       RHS_ATTR(2) RHS_ATTR(3) RHS_ATTR(4) RHS_ATTR(5) RHS_ATTR(6) RHS_ATTR(7) RHS_ATTR(8)
 #undef RHS_ATTR
@@ -255,13 +297,16 @@ struct Impl {
 
   static int nonlinear(cfg_ctx* c, int step, int rk, bool lin) {
     const Geom& g = c->g;
+    c->mean64_valid = false;
     const int do_cfl = (rk == 1);
     if (do_cfl) CK(cudaMemsetAsync(c->cflbits, 0, sizeof(unsigned long long) * 3 * g.ny1, c->st));
     dim3 g1(g.nxh, (g.ny1 + c->YB1 - 1) / c->YB1);
+    prof_begin(c, "k_zinv");
     k_zinv<T><<<g1, 256, c->sm_zinv, c->st>>>((const C*)c->vel, (C*)c->T1, g, c->pz, (const C*)c->twz,
                                                c->YB1, 0, g.ny1);
     CKL();
     dim3 g2(g.nz2 / c->ZR, (g.ny - 1 + c->KC - 1) / c->KC);
+    prof_begin(c, "k_xflux");
     if (lin)
       k_xflux<T, true><<<g2, 256, c->sm_xflux, c->st>>>((const C*)c->T1, (C*)c->T2, g, c->px, (const C*)c->twx,
                                                          c->gd, (const T*)c->fringe, c->has_fringe, c->ZR, c->KC,
@@ -272,9 +317,11 @@ struct Impl {
                                                           c->cflbits, do_cfl);
     CKL();
     dim3 g3(g.nxh, (g.ny1 + c->YB3 - 1) / c->YB3);
+    prof_begin(c, "k_zfwd");
     k_zfwd<T><<<g3, 256, c->sm_zfwd, c->st>>>((const C*)c->T2, (C*)c->vel, g, c->pz, (const C*)c->twz, c->gd, c->YB3);
     CKL();
     if (do_cfl) {
+      prof_begin(c, "k_cfl_finalize");
       if (lin)
         k_cfl_finalize<true><<<1, 256, 0, c->st>>>(c->cflbits, g, c->gd, c->sc, c->cflp, c->p.lx, c->p.lz,
                                                     c->p.dt_flag, c->p.cfl_max, step);
@@ -289,14 +336,25 @@ struct Impl {
   template <int MM>
   static int rhs_m(cfg_ctx* c, int rk, int mode) {
     const Geom& g = c->g;
-    const int nlist = g.nw - 1;
-    if (nlist > 0) {
-      dim3 gr((nlist + 3) / 4);
-      k_rhs<T, MM><<<gr, 128, c->sm_rhs, c->st>>>((C*)c->vel, (C*)c->cru, (C*)c->prs, (const C*)c->cbc + 3 * (size_t)g.nw,
-                                                  (const C*)c->cbc, g, c->gd, c->sc, c->rkt, rk, c->p.re, mode,
-                                                  nullptr, nlist);
+    if (c->n_fast > 0) {
+      dim3 gr((c->n_fast + 3) / 4);
+      prof_begin(c, "k_rhs");
+      k_rhs<T, T, MM><<<gr, 128, c->sm_rhs, c->st>>>((C*)c->vel, (C*)c->cru, (C*)c->prs,
+                                                     (const C*)c->cbc + 3 * (size_t)g.nw, (const C*)c->cbc, g,
+                                                     c->gd, c->sc, c->rkt, rk, c->p.re, mode, c->wl_fast, c->n_fast);
       CKL();
     }
+    if (c->n_prec > 0) {
+      dim3 gr((c->n_prec + 3) / 4);
+      prof_begin(c, "k_rhs_fp64");
+      k_rhs<double, T, MM><<<gr, 128, c->sm_rhs64, c->st>>>((C*)c->vel, (C*)c->cru, (C*)c->prs,
+                                                            (const C*)c->cbc + 3 * (size_t)g.nw, (const C*)c->cbc, g,
+                                                            c->gd, c->sc, c->rkt, rk, c->p.re, mode, c->wl_prec,
+                                                            c->n_prec);
+      CKL();
+    }
+    if (mode == 0) c->mean64_valid = true;
+    prof_begin(c, "k_rhs_mean");
     k_rhs_mean<T, MM><<<1, 32, 0, c->st>>>((C*)c->vel, (C*)c->cru, (C*)c->prs, c->mvel64, c->mcru64,
                                           (const C*)c->cbc + 3 * (size_t)g.nw, (const C*)c->cbc, g, c->gd, c->sc,
                                           c->d_um_dy, c->rkt, rk, c->p.re, c->p.beta, c->p.fix_mass, mode);
@@ -319,10 +377,12 @@ struct Impl {
   static int planes_c2r(cfg_ctx* c, const C* in, PlaneIn L, const int* plist_dev, int np, T* phys) {
     const Geom& g = c->g;
     const int smp = (int)(sizeof(C) * (g.nz2 + 2 * L.nc * g.nz2));
+    prof_begin(c, "k_pz_inv");
     k_pz_inv<T><<<dim3(g.nxh, np), 128, smp, c->st>>>(in, L, plist_dev, np, (C*)c->pw_H, g.nxh, g.nz, g.nz2, 1,
                                                        g.nx2 > g.nx, c->pz, (const C*)c->twz);
     CKL();
     const int smx = (int)(sizeof(C) * 3 * g.nx2);
+    prof_begin(c, "k_px_inv");
     k_px_inv<T><<<dim3((g.nz2 + 1) / 2, np * L.nc), 128, smx, c->st>>>((const C*)c->pw_H, phys, g.nxh, g.nz2, g.nx2,
                                                                         c->px, (const C*)c->twx);
     CKL();
@@ -331,11 +391,13 @@ struct Impl {
   static int planes_r2c(cfg_ctx* c, const T* phys, int np, C* out, size_t osp, size_t oskx, size_t oskz) {
     const Geom& g = c->g;
     const int smx = (int)(sizeof(C) * 3 * g.nx2);
+    prof_begin(c, "k_px_fwd");
     k_px_fwd<T><<<dim3((g.nz2 + 1) / 2, np), 128, smx, c->st>>>(phys, (C*)c->pw_H, g.nxh, g.nz2, g.nx2, c->px,
                                                                 (const C*)c->twx);
     CKL();
     const int smz = (int)(sizeof(C) * 3 * g.nz2);
     const T scale = (T)(1.0 / ((double)g.nx2 * (double)g.nz2));
+    prof_begin(c, "k_pz_fwd");
     k_pz_fwd<T><<<dim3(g.nxh, np), 128, smz, c->st>>>((const C*)c->pw_H, out, osp, oskx, oskz, g.nxh, g.nz2, g.nz, 1,
                                                       scale, c->pz, (const C*)c->twz);
     CKL();
@@ -355,6 +417,7 @@ struct Impl {
       if (r) return r;
       const double* dm = nullptr;
       (void)dm;
+      prof_begin(c, "k_feedback");
       k_feedback<T><<<grid1d(np), 256, 0, c->st>>>((const T*)c->pw_phys, (T*)c->pw_phys2, np, c->hdm[0], c->hdm[1],
                                                    c->hdm[2], c->hdm[3], c->hdm[4], c->hdm[5], gain, off);
       CKL();
@@ -369,10 +432,12 @@ struct Impl {
     CK(cudaMemsetAsync(c->l2acc, 0, sizeof(double) * g.ny1, c->st));
     const int smp = (int)(sizeof(C) * (g.nz2 + 2 * 3 * g.nz2));
     PlaneIn L{1, (size_t)g.ny1, (size_t)g.nz * 3 * g.ny1, (size_t)3 * g.ny1, 3};
+    prof_begin(c, "k_pz_inv");
     k_pz_inv<T><<<dim3(g.nxh, g.ny), 128, smp, c->st>>>((const C*)c->vel, L, nullptr, g.ny, (C*)c->T1, g.nxh, g.nz,
                                                         g.nz2, 1, g.nx2 > g.nx, c->pz, (const C*)c->twz);
     CKL();
     const int smx = (int)(sizeof(C) * 3 * g.nx2);
+    prof_begin(c, "k_l2_rows");
     k_l2_rows<T><<<dim3((g.nz2 + 1) / 2, 3 * g.ny), 128, smx, c->st>>>((const C*)c->T1, g.nxh, g.nz2, g.nx2, c->px,
                                                                        (const C*)c->twx, c->gd.y, g.ny, c->l2acc);
     CKL();
@@ -418,6 +483,7 @@ extern "C" {
 
 const char* cfg_last_error(const cfg_ctx* c) { return c ? c->err.c_str() : "null context"; }
 long long cfg_launch_count(const cfg_ctx* c) { return c ? c->launches : 0; }
+void* cfg_stream(cfg_ctx* c) { return c ? (void*)c->st : nullptr; }
 
 int cfg_create(const cfg_params* p, const cfg_grid* gr, cfg_ctx** out) {
   if (!p || !gr || !out) return CFG_E_ARG;
@@ -531,6 +597,25 @@ int cfg_create(const cfg_params* p, const cfg_grid* gr, cfg_ctx** out) {
   cudaMemcpy(c->sc, &h, sizeof(h), cudaMemcpyHostToDevice);
   int pl[4] = {1, 2, ny - 1, ny - 2};   // planes 2, 3, ny, ny-1 (boundary)
   cudaMemcpy(c->plist, pl, sizeof(pl), cudaMemcpyHostToDevice);
+  {
+    // wavenumber lists: the mean mode has its own kernel; in mixed precision
+    // the wavenumbers with |k| < 4 (ill-conditioned pressure solves on the
+    // stretched grid) run with FP64 arithmetic
+    std::vector<int> fast, prec;
+    for (int w = 1; w < g.nw; ++w) {
+      const double kx = gr->kx[w / g.nz], kz = gr->kz[w % g.nz];
+      const double k2 = kx * kx + kz * kz;
+      if (c->mixed && k2 < 16.0) prec.push_back(w);
+      else fast.push_back(w);
+    }
+    c->n_fast = (int)fast.size();
+    c->n_prec = (int)prec.size();
+    if (cudaMalloc(&c->wl_fast, sizeof(int) * std::max<size_t>(1, fast.size())) != cudaSuccess ||
+        cudaMalloc(&c->wl_prec, sizeof(int) * std::max<size_t>(1, prec.size())) != cudaSuccess)
+      return bad(CFG_E_NOMEM);
+    if (!fast.empty()) cudaMemcpy(c->wl_fast, fast.data(), sizeof(int) * fast.size(), cudaMemcpyHostToDevice);
+    if (!prec.empty()) cudaMemcpy(c->wl_prec, prec.data(), sizeof(int) * prec.size(), cudaMemcpyHostToDevice);
+  }
   if (gr->buffer) {
     bool any = false;
     for (size_t i = 0; i < (size_t)g.nx2 * g.nz2; ++i) any = any || gr->buffer[i] != 0.0;
@@ -562,9 +647,11 @@ void cfg_destroy(cfg_ctx* c) {
   if (c->st) cudaStreamSynchronize(c->st);
   void* bufs[] = {c->dgrid, c->fringe, c->vel, c->cru, c->prs, c->mvel64, c->mcru64, c->T1, c->T2, c->cbc,
                   c->sc, c->d_um_dy, c->cflp, c->cflbits, c->l2acc, c->divbits, c->plist, c->pw_H,
-                  c->pw_phys, c->pw_phys2, c->pw_in, c->stage, c->twx, c->twz, c->twxs, c->twzs};
+                  c->pw_phys, c->pw_phys2, c->pw_in, c->stage, c->twx, c->twz, c->twxs, c->twzs,
+                  c->wl_fast, c->wl_prec};
   for (void* b : bufs)
     if (b) cudaFree(b);
+  for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
 }
@@ -578,6 +665,7 @@ int cfg_upload_state(cfg_ctx* c, const double* d1, const double* d2, const doubl
   if (r) return r;
   if (d1) {
     CK(cudaMemcpyAsync(c->stage, d1, sizeof(double2) * nf, cudaMemcpyHostToDevice, c->st));
+    c->mean64_valid = true;
     if (c->mixed) k_data1_in<float><<<grid1d(nf), 256, 0, c->st>>>(c->stage, (float2*)c->vel, c->mvel64, g);
     else k_data1_in<double><<<grid1d(nf), 256, 0, c->st>>>(c->stage, (double2*)c->vel, nullptr, g);
     CKL();
@@ -607,7 +695,7 @@ int cfg_download_state(cfg_ctx* c, double* d1, double* d2, double* d4) {
   int r = ensure_stage(c, nf);
   if (r) return r;
   if (d1) {
-    if (c->mixed) k_data1_out<float><<<grid1d(nf), 256, 0, c->st>>>((const float2*)c->vel, c->mvel64, c->stage, g);
+    if (c->mixed) k_data1_out<float><<<grid1d(nf), 256, 0, c->st>>>((const float2*)c->vel, c->mean64_valid ? c->mvel64 : nullptr, c->stage, g);
     else k_data1_out<double><<<grid1d(nf), 256, 0, c->st>>>((const double2*)c->vel, nullptr, c->stage, g);
     CKL();
     CK(cudaMemcpyAsync(d1, c->stage, sizeof(double2) * nf, cudaMemcpyDeviceToHost, c->st));
@@ -747,6 +835,7 @@ static int timestep_impl(cfg_ctx* c, int nsteps, bool lin) {
       r = DISPATCH(c, rhs(c, rk, 0));
       if (r) return r;
     }
+    prof_begin(c, "k_advance_time");
     k_advance_time<<<1, 1, 0, c->st>>>(c->sc);
     CKL();
   }
@@ -778,6 +867,7 @@ int cfg_compute_initial_pressure(cfg_ctx* c, int linearized) {
   const size_t nf = (size_t)c->g.nw * 3 * c->g.ny1;
   CK(cudaMemcpyAsync(c->vel, c->cru, csize(c) * nf, cudaMemcpyDeviceToDevice, c->st));
   if (c->mixed) CK(cudaMemcpyAsync(c->mvel64, c->mcru64, sizeof(double2) * 3 * c->g.ny1, cudaMemcpyDeviceToDevice, c->st));
+  c->mean64_valid = true;
   CK(cudaStreamSynchronize(c->st));
   return CFG_OK;
 }
@@ -886,6 +976,44 @@ int cfg_status(cfg_ctx* c) {
   if (!c) return CFG_E_ARG;
   cudaSetDevice(c->dev);
   return check_status(c);
+}
+
+int cfg_profile_enable(cfg_ctx* c, int on) {
+  if (!c) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  CK(cudaStreamSynchronize(c->st));
+  c->recs.clear();
+  c->ev_used = 0;
+  c->prof_on = on != 0;
+  return CFG_OK;
+}
+
+int cfg_profile_read(cfg_ctx* c, int idx, char* name, int namelen, int* launches, double* total_ms) {
+  if (!c) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  CK(cudaStreamSynchronize(c->st));
+  // distinct kernel names in first-seen order
+  std::vector<const char*> names;
+  for (auto& r : c->recs) {
+    bool seen = false;
+    for (const char* n : names) seen = seen || strcmp(n, r.name) == 0;
+    if (!seen) names.push_back(r.name);
+  }
+  if (idx < 0) return (int)names.size();
+  if (idx >= (int)names.size()) return CFG_E_ARG;
+  int n = 0;
+  double ms = 0;
+  for (auto& r : c->recs) {
+    if (strcmp(r.name, names[idx]) != 0) continue;
+    float t = 0;
+    CK(cudaEventElapsedTime(&t, r.a, r.b));
+    ms += t;
+    ++n;
+  }
+  if (name && namelen > 0) snprintf(name, namelen, "%s", names[idx]);
+  if (launches) *launches = n;
+  if (total_ms) *total_ms = ms;
+  return CFG_OK;
 }
 
 int cfg_synchronize(cfg_ctx* c) {

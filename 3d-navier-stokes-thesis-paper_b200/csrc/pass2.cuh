@@ -127,14 +127,18 @@ template <int M> struct ColIdx {
   __device__ static __forceinline__ int at(int j) { return (j / M) * LS + (j % M); }
 };
 
+// conversion between the storage and compute complex types
+template <typename C, typename SC>
+__device__ __forceinline__ C cvt(SC v) { return mk<C>((decltype(C::x))v.x, (decltype(C::x))v.y); }
+
 // Load a global y-column [0, n) into a shared column (coalesced), zero-padded.
-template <typename C, int M>
-__device__ __forceinline__ void load_col(C* s, const C* __restrict__ gsrc, int n, int lane) {
-  for (int j = lane; j < 32 * M; j += 32) s[ColIdx<M>::at(j)] = (j < n) ? gsrc[j] : czero<C>();
+template <typename C, int M, typename SC>
+__device__ __forceinline__ void load_col(C* s, const SC* __restrict__ gsrc, int n, int lane) {
+  for (int j = lane; j < 32 * M; j += 32) s[ColIdx<M>::at(j)] = (j < n) ? cvt<C>(gsrc[j]) : czero<C>();
 }
-template <typename C, int M>
-__device__ __forceinline__ void store_col(C* __restrict__ gdst, const C* s, int n, int lane) {
-  for (int j = lane; j < n; j += 32) gdst[j] = s[ColIdx<M>::at(j)];
+template <typename C, int M, typename SC>
+__device__ __forceinline__ void store_col(SC* __restrict__ gdst, const C* s, int n, int lane) {
+  for (int j = lane; j < n; j += 32) gdst[j] = cvt<SC>(s[ColIdx<M>::at(j)]);
 }
 
 // Second difference d2_dy (PFC/diff_int.f90:31-46) at row j of an n-row
@@ -254,12 +258,14 @@ __device__ __forceinline__ void sub_grad(cplx_t<T>* su, cplx_t<T>* sv, cplx_t<T>
 // with coef 1, PFC/init_vel.f90:518-536).  mode 2: solve_continuous_poisson
 // (PFC/init_vel.f90:477-513): pressure from the velocity held in cru and the
 // nonlinear term in vel.
-template <typename T, int M>
-__global__ void __launch_bounds__(128) k_rhs(cplx_t<T>* __restrict__ vel,
-                                             cplx_t<T>* __restrict__ cru,
-                                             cplx_t<T>* __restrict__ prs,
-                                             const cplx_t<T>* __restrict__ cbc_top,
-                                             const cplx_t<T>* __restrict__ cbc_bot, Geom g,
+// T is the arithmetic precision, S the storage precision of the state: the
+// mixed path runs its low-|k| wavenumbers with T = double over S = float.
+template <typename T, typename S, int M>
+__global__ void __launch_bounds__(128) k_rhs(cplx_t<S>* __restrict__ vel,
+                                             cplx_t<S>* __restrict__ cru,
+                                             cplx_t<S>* __restrict__ prs,
+                                             const cplx_t<S>* __restrict__ cbc_top,
+                                             const cplx_t<S>* __restrict__ cbc_bot, Geom g,
                                              GridDev gd, const DevScalars* __restrict__ sc,
                                              RkTab rkt, int rk, double re, int mode,
                                              const int* __restrict__ wlist, int nlist) {
@@ -274,15 +280,16 @@ __global__ void __launch_bounds__(128) k_rhs(cplx_t<T>* __restrict__ vel,
   const int kxi = w / NZ, kzi = w % NZ;
   const T kx = (T)gd.kx[kxi], kz = (T)gd.kz[kzi];
   const T k2 = (T)(gd.kx[kxi] * gd.kx[kxi] + gd.kz[kzi] * gd.kz[kzi]);
-  C* S = reinterpret_cast<C*>(smem_raw) + warp * 5 * CI::SIZE;
-  C* su = S;
-  C* sv = S + CI::SIZE;
-  C* sw = S + 2 * CI::SIZE;
-  C* sp = S + 3 * CI::SIZE;
-  C* sh = S + 4 * CI::SIZE;
-  C* gvel = vel + (size_t)w * 3 * n1;
-  C* gcru = cru + (size_t)w * 3 * n1;
-  C* gprs = prs + (size_t)w * n1;
+  C* sbase = reinterpret_cast<C*>(smem_raw) + warp * 5 * CI::SIZE;
+  C* su = sbase;
+  C* sv = sbase + CI::SIZE;
+  C* sw = sbase + 2 * CI::SIZE;
+  C* sp = sbase + 3 * CI::SIZE;
+  C* sh = sbase + 4 * CI::SIZE;
+  using SC = cplx_t<S>;
+  SC* gvel = vel + (size_t)w * 3 * n1;
+  SC* gcru = cru + (size_t)w * 3 * n1;
+  SC* gprs = prs + (size_t)w * n1;
   const size_t nw = (size_t)g.nw;
 
   if (mode == 1) {
@@ -304,11 +311,11 @@ __global__ void __launch_bounds__(128) k_rhs(cplx_t<T>* __restrict__ vel,
       if (j < n1) {
         const C u = sp[CI::at(j)], v = sh[CI::at(j)];
         const C du = d2_row<T, M>(sp, gd.d2h, j, n1);
-        r[0][i] = cadd(cscale((T)-1, gvel[j]), cscale(visc, csub(du, cscale(k2, u))));
+        r[0][i] = cadd(cscale((T)-1, cvt<C>(gvel[j])), cscale(visc, csub(du, cscale(k2, u))));
         if (j < ny) {
           const C dv = d2_row<T, M>(sh, gd.d2n, j, ny);
-          r[1][i] = cadd(cscale((T)-1, gvel[n1 + j]), cscale(visc, csub(dv, cscale(k2, v))));
-        } else r[1][i] = cscale((T)-1, gvel[n1 + j]);
+          r[1][i] = cadd(cscale((T)-1, cvt<C>(gvel[n1 + j])), cscale(visc, csub(dv, cscale(k2, v))));
+        } else r[1][i] = cscale((T)-1, cvt<C>(gvel[n1 + j]));
       } else { r[0][i] = czero<C>(); r[1][i] = czero<C>(); }
     }
     __syncwarp();
@@ -320,7 +327,7 @@ __global__ void __launch_bounds__(128) k_rhs(cplx_t<T>* __restrict__ vel,
       if (j < n1) {
         const C ww = sp[CI::at(j)];
         const C dw = d2_row<T, M>(sp, gd.d2h, j, n1);
-        r[2][i] = cadd(cscale((T)-1, gvel[2 * n1 + j]), cscale(visc, csub(dw, cscale(k2, ww))));
+        r[2][i] = cadd(cscale((T)-1, cvt<C>(gvel[2 * n1 + j])), cscale(visc, csub(dw, cscale(k2, ww))));
       } else r[2][i] = czero<C>();
     }
     __syncwarp();
@@ -348,7 +355,7 @@ __global__ void __launch_bounds__(128) k_rhs(cplx_t<T>* __restrict__ vel,
         const int j = lane * M + i;
         if (j < n1) {
           const C cr = scol[q][CI::at(j)];
-          const C nl = gvel[q * n1 + j];
+          const C nl = cvt<C>(gvel[q * n1 + j]);
           C v = mk<C>(cr.x - coef * nl.x, cr.y - coef * nl.y);
           if (rk == 1 && j < nq) {
             const C du = d2_row<T, M>(scol[q], d2, j, nq);
@@ -368,9 +375,9 @@ __global__ void __launch_bounds__(128) k_rhs(cplx_t<T>* __restrict__ vel,
     // ---- stage B: Helmholtz solves for u, w (ny+1 rows, d2h) and v (ny rows, d2n)
     const T vis_imp = (T)(rkt.d[rk] * (dt / re));
     const T alpha = (T)1 + vis_imp * k2;
-    helmholtz_col<T, M>(su, n1, alpha, vis_imp, gd.d2h, cbc_top[w], cbc_bot[w], lane);
-    helmholtz_col<T, M>(sw, n1, alpha, vis_imp, gd.d2h, cbc_top[2 * nw + w], cbc_bot[2 * nw + w], lane);
-    helmholtz_col<T, M>(sv, ny, alpha, vis_imp, gd.d2n, cbc_top[nw + w], cbc_bot[nw + w], lane);
+    helmholtz_col<T, M>(su, n1, alpha, vis_imp, gd.d2h, cvt<C>(cbc_top[w]), cvt<C>(cbc_bot[w]), lane);
+    helmholtz_col<T, M>(sw, n1, alpha, vis_imp, gd.d2h, cvt<C>(cbc_top[2 * nw + w]), cvt<C>(cbc_bot[2 * nw + w]), lane);
+    helmholtz_col<T, M>(sv, ny, alpha, vis_imp, gd.d2n, cvt<C>(cbc_top[nw + w]), cvt<C>(cbc_bot[nw + w]), lane);
     if (lane == 0) sv[CI::at(ny)] = czero<C>();
     __syncwarp();
   }
@@ -443,7 +450,7 @@ __global__ void __launch_bounds__(128) k_rhs(cplx_t<T>* __restrict__ vel,
         const int j = lane * M + i;
         if (j >= n1) continue;
         const C cv = scol[q][CI::at(j)];
-        const C nl = gvel[q * n1 + j];
+        const C nl = cvt<C>(gvel[q * n1 + j]);
         C v = mk<C>(cv.x - coef2 * nl.x, cv.y - coef2 * nl.y);
         if (j < nq) {
           const C du = d2_row<T, M>(scol[q], d2, j, nq);
@@ -458,7 +465,7 @@ __global__ void __launch_bounds__(128) k_rhs(cplx_t<T>* __restrict__ vel,
             v = csub(v, cscale(rkp2 * (T)gd.dn[j], csub(pp, p)));
           }
         }
-        gcru[q * n1 + j] = v;
+        gcru[q * n1 + j] = cvt<SC>(v);
       }
     }
   } else {

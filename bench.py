@@ -1,0 +1,358 @@
+"""Benchmark of the channel-flow DNS time step on B200.
+
+Workload: one time step (3 RK3/Crank-Nicolson substeps: nonlinear term with
+dealiased x-z transforms, per-wavenumber implicit y-solves) of the channel at
+256x193x256 (dealiased 384x384), Re 2500, tanh stretch 1.5, laminar 1-y^2
+plus seeded 1e-3 k^-2 divergence-free noise, constant bulk flux, dt 0.005.
+Metric: Mpts*steps/s with Mpts = nx*ny*nz = 12.648.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W]        our arm
+  python bench.py --impl reference [--steps K] [--warmup W]  the CPU arm
+
+With N > 1 (torchrun, one process per GPU) every rank advances its own
+independent domain (replicas, weak scaling); the timed region is bracketed by a
+barrier and the maximum device time over ranks is used.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX, NY, NZ = 256, 193, 256
+RE, DT, STRETCH, AMPL, SEED = 2500.0, 0.005, 1.5, 1e-3, 1
+METRIC = "Mpts·steps/s/GPU at 256×193×256, mixed vs FP64; NN-LES speedup at equal U+ error"
+UNIT = "Mpts·steps/s"
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def mpts(nx, ny, nz):
+    return nx * ny * nz / 1e6
+
+
+def workload_config(nx, ny, nz, precision):
+    return {
+        "workload": f"channel-flow DNS time step (3 RK3/CN substeps) at {nx}x{ny}x{nz} "
+                    f"(dealiased {3 * nx // 2}x{3 * nz // 2}), Re {RE:g}, stretch {STRETCH}, "
+                    f"laminar + {AMPL:g} k^-2 noise, constant flux, dt {DT}",
+        "grid": [nx, ny, nz], "dealiased": [3 * nx // 2, 3 * nz // 2],
+        "precision": precision, "mpts": round(mpts(nx, ny, nz), 4),
+        "cache": "no L2 flush: the per-step state (>= 1 GB) is larger than the 126 MB L2",
+        "parallelism": "replicas (one independent domain per GPU)",
+    }
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d, "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+# --------------------------------------------------------------------------
+# CPU arm: the oracle (FP64 C restatement of the reference, OpenMP)
+def time_oracle(nx, ny, nz, steps, warmup, budget_s=150.0):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import orc
+    nthreads = os.cpu_count() or 1
+    o = orc.Oracle(nx, ny, nz, re=RE, dt=DT, stretch=STRETCH, nthreads=nthreads)
+    o.init_field(10, seed=SEED, ampl=AMPL)
+    t0 = time.perf_counter()
+    o.timestep(1)
+    t_step = time.perf_counter() - t0
+    sample_ny = ny
+    total = (steps + warmup) * t_step
+    if total > budget_s:
+        # bounded sample: the same x-z grid on fewer y planes
+        frac = budget_s / total
+        sample_ny = max(9, int(ny * frac))
+        o.close()
+        o = orc.Oracle(nx, sample_ny, nz, re=RE, dt=DT, stretch=STRETCH, nthreads=nthreads)
+        o.init_field(10, seed=SEED, ampl=AMPL)
+    for _ in range(max(0, warmup - 1)):
+        o.timestep(1)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.timestep(1)
+    el = time.perf_counter() - t0
+    o.close()
+    value = mpts(nx, sample_ny, nz) * steps / el
+    sample = (f"{steps} full time steps of the oracle at {nx}x{sample_ny}x{nz}"
+              + ("" if sample_ny == ny else f" (bounded sample: {sample_ny} of {ny} y-planes)"))
+    return value, el / steps * 1e3, nthreads, sample
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    value, ms, cores, sample = time_oracle(args.nx, args.ny, args.nz, args.steps, args.warmup)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": workload_config(args.nx, args.ny, args.nz, "fp64"),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": sample + "; reference Fortran binary unbuildable here "
+                                            "(no Fortran compiler, MPI or FFTW)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    def __init__(self, device):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-i", str(device), "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        for ln in open(self.f.name):
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i]
+                          and "Not" not in r[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def make_flow(cf, nx, ny, nz, precision, device):
+    grid = cf.Grid(nx, ny, nz, lx=4 * np.pi, lz=2 * np.pi, stretch=STRETCH)
+    flow = cf.ChannelFlow(grid, re=RE, dt=DT, fix_mass=1, precision=precision, device=device)
+    flow.define_initial_field(10, seed=SEED, ampl=AMPL)
+    return flow
+
+
+def timed_steps(torch, flow, steps, profile=False):
+    stream = torch.cuda.ExternalStream(flow.stream_ptr())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    flow.synchronize()
+    if profile:
+        flow.profile_enable(True)
+    n0 = flow.launch_count()
+    e0.record(stream)
+    flow.timestep(steps)
+    e1.record(stream)
+    e1.synchronize()
+    n1 = flow.launch_count()
+    prof = flow.profile_read() if profile else None
+    if profile:
+        flow.profile_enable(False)
+    return e0.elapsed_time(e1), n1 - n0, prof
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    import __graft_entry__
+    cf = __graft_entry__.load_package()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    nx, ny, nz, K, W = args.nx, args.ny, args.nz, args.steps, args.warmup
+    units = mpts(nx, ny, nz)
+    results = {}
+    for prec_name, prec in (("mixed", cf.MIXED), ("fp64", cf.FP64)):
+        if prec_name == "fp64" and args.no_fp64:
+            continue
+        flow = make_flow(cf, nx, ny, nz, prec, dev)
+        flow.timestep(W)
+        flow.synchronize()
+        barrier()
+        clocks = Clocks(dev) if prec_name == "mixed" else None
+        ms, nlaunch, prof = timed_steps(torch, flow, K, profile=True)
+        cl = clocks.stop() if clocks else None
+        barrier()
+        ms_max = max_over_ranks(ms)
+        st = flow.status()
+        q, div = flow.diagnostics()
+        results[prec_name] = {"ms_total": ms_max, "launches": sum_over_ranks(nlaunch), "prof": prof,
+                              "clocks": cl, "status": st, "div": div, "q": q}
+        if prec_name == "mixed":
+            # end to end through the public API with host buffers: every step
+            # uploads data1/data2/data4 from pinned host memory, advances one
+            # step and downloads data1/data2/data4 (a host-owned state).
+            ke = max(1, min(K, args.e2e_steps))
+            s1, s2, s4 = flow.shapes()
+            pin = [torch.empty(int(np.prod(s)) * 2, dtype=torch.float64, pin_memory=True) for s in (s1, s2, s4)]
+            d1, d2, d4 = flow.download_state()
+            for t, a in zip(pin, (d1, d2, d4)):
+                t.numpy()[:] = np.asfortranarray(a).ravel(order="F").view(np.float64)
+            ptr = [t.data_ptr() for t in pin]
+            L = flow.L
+            stream = torch.cuda.ExternalStream(flow.stream_ptr())
+            barrier()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(ke):
+                flow._chk(L.cfg_upload_state(flow.h, ptr[0], ptr[1], ptr[2]))
+                flow.timestep(1)
+                flow._chk(L.cfg_download_state(flow.h, ptr[0], ptr[1], ptr[2]))
+            e1.record(stream)
+            e1.synchronize()
+            e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+            nbytes = sum(t.numel() * 8 for t in pin)
+            results["e2e"] = {"value": world * units * ke / (e2e_ms / 1e3), "unit": UNIT,
+                              "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes}
+        flow.close()
+        torch.cuda.synchronize()
+
+    # CPU baseline on rank 0 at N = 1
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        v, ms, cores, sample = time_oracle(nx, ny, nz, steps=1, warmup=1, budget_s=30.0)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        mix = results["mixed"]
+        ms_step = mix["ms_total"] / K
+        value = world * units * K / (mix["ms_total"] / 1e3)
+        pk, pk_kind = peaks()
+        hbm = float(pk.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
+        nf = nz * (nx // 2 + 1) * (ny + 1)
+        sc = 8  # FP32 complex bytes
+        # algorithmic bytes: pass1 reads u,v,w and writes the nonlinear term (6
+        # fields); pass2 reads NL, cru, p and writes u,v,w, cru, p (14 fields)
+        groups = {"pass1 (k_zinv+k_xflux+k_zfwd)": (("k_zinv", "k_xflux", "k_zfwd"), 6 * nf * sc),
+                  "pass2 (k_rhs, k_rhs_fp64, k_rhs_mean)": (("k_rhs", "k_rhs_fp64", "k_rhs_mean"), 14 * nf * sc)}
+        prof = mix["prof"] or {}
+        tot_prof = sum(v[1] for v in prof.values()) or 1.0
+        kernels = {k: {"launches": v[0], "ms_per_launch": v[1] / max(v[0], 1),
+                       "share": v[1] / tot_prof} for k, v in prof.items()}
+        traffic = {}
+        tp = os.path.join(ROOT, "profiles", "traffic_per_substep.json")
+        if os.path.exists(tp):
+            traffic = json.load(open(tp))
+        best = None
+        for gname, (ks, abytes) in groups.items():
+            g_ms = sum(prof.get(k, (0, 0.0))[1] for k in ks) / (3 * K)   # per substep launch group
+            if g_ms <= 0:
+                continue
+            t_g = None
+            if traffic and all(k in traffic.get("bytes", {}) for k in ks if k in prof):
+                t_g = sum(traffic["bytes"].get(k, 0.0) for k in ks)
+            ent = {"bound": "hbm", "kernel": gname, "achieved": abytes / (g_ms / 1e3) / 1e9,
+                   "peak": hbm, "unit": "GB/s", "frac": abytes / (g_ms / 1e3) / 1e9 / hbm,
+                   "traffic": t_g, "algorithmic_bytes": abytes, "ms_per_launch": g_ms,
+                   "peak_kind": f"{pk_kind} (MEASURED_PEAKS.json hbm_gbs)" if pk_kind == "measured" else pk_kind}
+            if best is None or g_ms > best["ms_per_launch"]:
+                best = ent
+        step_bytes = 3 * 20 * nf * sc
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (f64 mean mode and |k|<4 solves)", "data": "synthetic (seeded initial field)",
+            "config": workload_config(nx, ny, nz, "mixed"),
+            "roofline": best,
+            "roofline_step": {"bound": "hbm", "achieved": step_bytes / (ms_step / 1e3) / 1e9, "peak": hbm,
+                              "unit": "GB/s", "frac": step_bytes / (ms_step / 1e3) / 1e9 / hbm,
+                              "algorithmic_bytes": step_bytes},
+            "kernels": kernels,
+            "e2e": results.get("e2e"),
+            "gpu_launches": int(mix["launches"]),
+            "clocks": mix["clocks"],
+            "cpu_baseline": cpu,
+            "checks": {"status": mix["status"], "max_divergence": mix["div"], "bulk_flux": mix["q"]},
+        }
+        if "fp64" in results:
+            f = results["fp64"]
+            line["value_fp64"] = world * units * K / (f["ms_total"] / 1e3)
+            line["ms_per_step_fp64"] = f["ms_total"] / K
+            line["fp64_roofline_step"] = {
+                "achieved": 3 * 20 * nf * 16 / (f["ms_total"] / K / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
+                "frac": 3 * 20 * nf * 16 / (f["ms_total"] / K / 1e3) / 1e9 / hbm}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nx", type=int, default=NX)
+    ap.add_argument("--ny", type=int, default=NY)
+    ap.add_argument("--nz", type=int, default=NZ)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

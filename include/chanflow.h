@@ -159,8 +159,21 @@ int cfg_diagnostics(cfg_ctx *c, double *bulk_flux, double *max_divergence);
 int cfg_status(cfg_ctx *c);
 int cfg_synchronize(cfg_ctx *c);
 
+/* The CUDA stream (cudaStream_t) every call of this context is issued on,
+ * for callers that order their own work or timing events against it. */
+void *cfg_stream(cfg_ctx *c);
+
 /* Number of kernel launches this context has issued (for accounting). */
 long long cfg_launch_count(const cfg_ctx *c);
+
+/* Per-kernel timing with CUDA events recorded on the context's stream around
+ * each hot-path launch.  cfg_profile_enable(c, 1) clears and starts the
+ * record; cfg_profile_read(c, -1, ...) returns the number of distinct
+ * kernels, cfg_profile_read(c, i, name, len, &launches, &ms) the i-th one's
+ * launch count and summed device time.  Both synchronise. */
+int cfg_profile_enable(cfg_ctx *c, int on);
+int cfg_profile_read(cfg_ctx *c, int idx, char *name, int namelen, int *launches,
+                     double *total_ms);
 
 #ifdef __cplusplus
 }
