@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -12,7 +13,9 @@
 #include "chanflow.h"
 #include "pass1.cuh"
 #include "pass2.cuh"
+#include "pass1_fast.h"
 #include "planes.cuh"
+#include "regfft.cuh"
 
 using namespace cfd;
 
@@ -147,6 +150,9 @@ struct cfg_ctx {
   int* wl_prec = nullptr;
   int n_fast = 0, n_prec = 0;
   size_t sm_rhs64 = 0;
+  // register-FFT pass-1 kernels (when the lengths are compiled in)
+  bool fast_z = false, fast_x = false;
+  int fYB1 = 1, fYB3 = 1, fZR = 1;
   // optional per-launch CUDA-event timing on the context stream
   bool prof_on = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -287,6 +293,25 @@ struct Impl {
       RHS_ATTR(2) RHS_ATTR(3) RHS_ATTR(4) RHS_ATTR(5) RHS_ATTR(6) RHS_ATTR(7) RHS_ATTR(8)
 #undef RHS_ATTR
     }
+    // register-FFT kernels: tile sizes that keep two blocks per SM
+    const bool f32 = sizeof(T) == 4;
+    c->fast_z = regfft_supported(g.nz2);
+    c->fast_x = regfft_supported(g.nx2);
+    if (c->fast_z) {
+      c->fYB1 = 1;
+      for (int yb = 8; yb >= 1; --yb)
+        if (p1_fast_smem(0, g.nz2, f32, yb, g.nxh) <= budget) { c->fYB1 = yb; break; }
+      c->fYB3 = 1;
+      for (int yb = 4; yb >= 1; --yb)
+        if (p1_fast_smem(2, g.nz2, f32, yb, g.nxh) <= budget) { c->fYB3 = yb; break; }
+    }
+    if (c->fast_x) {
+      c->fZR = 1;
+      for (int zr : {4, 2})
+        if (g.nz2 % zr == 0 && p1_fast_smem(1, g.nx2, f32, zr, g.nxh) <= budget) { c->fZR = zr; break; }
+      if (p1_fast_smem(1, g.nx2, f32, c->fZR, g.nxh) > 220 * 1024) c->fast_x = false;
+    }
+    if (getenv("CHANFLOW_GENERIC_FFT")) c->fast_x = c->fast_z = false;
     c->twx = make_twiddles<T>(g.nx2);
     c->twz = make_twiddles<T>(g.nz2);
     c->twxs = make_twiddles<T>(g.nx);
@@ -300,14 +325,25 @@ struct Impl {
     c->mean64_valid = false;
     const int do_cfl = (rk == 1);
     if (do_cfl) CK(cudaMemsetAsync(c->cflbits, 0, sizeof(unsigned long long) * 3 * g.ny1, c->st));
+    P1Launch a{};
+    a.vel = c->vel; a.T1 = c->T1; a.T2 = c->T2; a.velout = c->vel; a.g = g; a.twx = c->twx; a.twz = c->twz;
+    a.gd = c->gd; a.fringe = c->fringe; a.has_fringe = c->has_fringe; a.YB1 = c->fYB1; a.YB3 = c->fYB3;
+    a.ZR = c->fZR; a.cflbits = c->cflbits; a.do_cfl = do_cfl; a.lin = lin ? 1 : 0; a.st = c->st;
+    a.KC = (int)std::max(2L, std::min(16L, (long)(g.ny - 1) * (g.nz2 / c->fZR) / 592));
+    const bool f32 = sizeof(T) == 4;
     dim3 g1(g.nxh, (g.ny1 + c->YB1 - 1) / c->YB1);
     prof_begin(c, "k_zinv");
-    k_zinv<T><<<g1, 256, c->sm_zinv, c->st>>>((const C*)c->vel, (C*)c->T1, g, c->pz, (const C*)c->twz,
-                                               c->YB1, 0, g.ny1);
+    if (c->fast_z) {
+      if (p1_fast_launch(0, g.nz2, f32, a) != 0) return fail(c, CFG_E_CUDA, "k_zinv_r launch");
+    } else
+      k_zinv<T><<<g1, 256, c->sm_zinv, c->st>>>((const C*)c->vel, (C*)c->T1, g, c->pz, (const C*)c->twz,
+                                                 c->YB1, 0, g.ny1);
     CKL();
     dim3 g2(g.nz2 / c->ZR, (g.ny - 1 + c->KC - 1) / c->KC);
     prof_begin(c, "k_xflux");
-    if (lin)
+    if (c->fast_x) {
+      if (p1_fast_launch(1, g.nx2, f32, a) != 0) return fail(c, CFG_E_CUDA, "k_xflux_r launch");
+    } else if (lin)
       k_xflux<T, true><<<g2, 256, c->sm_xflux, c->st>>>((const C*)c->T1, (C*)c->T2, g, c->px, (const C*)c->twx,
                                                          c->gd, (const T*)c->fringe, c->has_fringe, c->ZR, c->KC,
                                                          c->cflbits, do_cfl);
@@ -318,7 +354,10 @@ struct Impl {
     CKL();
     dim3 g3(g.nxh, (g.ny1 + c->YB3 - 1) / c->YB3);
     prof_begin(c, "k_zfwd");
-    k_zfwd<T><<<g3, 256, c->sm_zfwd, c->st>>>((const C*)c->T2, (C*)c->vel, g, c->pz, (const C*)c->twz, c->gd, c->YB3);
+    if (c->fast_z) {
+      if (p1_fast_launch(2, g.nz2, f32, a) != 0) return fail(c, CFG_E_CUDA, "k_zfwd_r launch");
+    } else
+      k_zfwd<T><<<g3, 256, c->sm_zfwd, c->st>>>((const C*)c->T2, (C*)c->vel, g, c->pz, (const C*)c->twz, c->gd, c->YB3);
     CKL();
     if (do_cfl) {
       prof_begin(c, "k_cfl_finalize");

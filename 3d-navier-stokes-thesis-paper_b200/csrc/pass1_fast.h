@@ -1,0 +1,35 @@
+// pass1_fast.h -- launch interface of the register-FFT pass-1 kernels, one
+// translation unit per transform length (pass1_n<N>.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "pass1.cuh"
+
+namespace cfd {
+
+struct P1Launch {
+  const void* vel;      // spectral velocity (k_zinv input)
+  void* T1;             // hybrid planes
+  void* T2;             // x-transformed fluxes
+  void* velout;         // nonlinear term (k_zfwd output)
+  Geom g;
+  const void* twx;      // W_nx2^m
+  const void* twz;      // W_nz2^m
+  GridDev gd;
+  const void* fringe;
+  int has_fringe;
+  int YB1, YB3, ZR, KC;
+  unsigned long long* cflbits;
+  int do_cfl;
+  int lin;
+  cudaStream_t st;
+};
+
+// which: 0 k_zinv_r, 1 k_xflux_r, 2 k_zfwd_r.  Returns 0, or -1 when the
+// length is not compiled in, or -2 on a launch error.
+int p1_fast_launch(int which, int n, bool f32, const P1Launch& a);
+// shared memory bytes of kernel `which` at length n with its tile parameter
+// (YB for 0/2, ZR for 1); 0 when unsupported.
+size_t p1_fast_smem(int which, int n, bool f32, int param, int nxh);
+
+}  // namespace cfd

@@ -1,0 +1,433 @@
+// pass1_reg.cuh -- the pass-1 kernels of pass1.cuh (same arithmetic, same
+// layouts) built on the register-resident two-stage FFTs of regfft.cuh for the
+// hot-path lengths (48 ... 576).  See pass1.cuh for what each kernel computes
+// and which reference routine it replaces.
+#pragma once
+#include "cfd_common.cuh"
+#include "pass1.cuh"
+#include "regfft.cuh"
+
+namespace cfd {
+
+// per-sequence stride of the stage exchange buffer (+1 spreads the banks when
+// consecutive threads work on consecutive sequences)
+template <int N> struct SeqPitch {
+  static constexpr int V = Split<N>::N1 * (Split<N>::N2 + 1) + 1;
+};
+
+// --------------------------------------------------------------------------
+// k_zinv_r: grid (nxh, ceil(ny1/YB)), block 256.  Inverse z transform of the
+// 3/2-padded columns (xz_fft_complex_to_real_parallel, PFC/transform.f90:345-368).
+template <typename T, int NZ2>
+__global__ void __launch_bounds__(256) k_zinv_r(const cplx_t<T>* __restrict__ vel,
+                                                cplx_t<T>* __restrict__ T1, Geom g,
+                                                const cplx_t<T>* __restrict__ twz, int YB) {
+  using C = cplx_t<T>;
+  constexpr int N1 = Split<NZ2>::N1, N2 = Split<NZ2>::N2, PITCH = N2 + 1, SEQ = SeqPitch<NZ2>::V;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  C* Y = tw + NZ2;
+  const int NZ = g.nz, NY1 = g.ny1, NXH = g.nxh;
+  const int kx = blockIdx.x;
+  const int j0 = blockIdx.y * YB;
+  const int nj = min(YB, NY1 - j0);
+  const int nseq = 3 * YB;
+  for (int m = threadIdx.x; m < NZ2; m += blockDim.x) tw[m] = twz[m];
+  __syncthreads();
+  const T half = (T)0.5;
+  const bool halve_x = (g.nx2 > g.nx) && (kx == NXH - 1) && (NZ2 > NZ);
+  const C* col = vel + (size_t)kx * NZ * 3 * NY1;
+  // stage 1: consecutive threads take consecutive sequences (planes fastest)
+  for (int t = threadIdx.x; t < nseq * N2; t += blockDim.x) {
+    const int s = t % nseq, n2 = t / nseq;
+    const int jj = s % YB, c = s / YB;
+    C v[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) {
+      const int m = N2 * n1 + n2;
+      C x = czero<C>();
+      if (jj < nj) {
+        const size_t base = (size_t)c * NY1 + j0 + jj;
+        if (NZ2 > NZ) {
+          if (m < NZ / 2) x = col[(size_t)m * 3 * NY1 + base];
+          else if (m == NZ / 2) x = cscale(half, col[(size_t)(NZ / 2) * 3 * NY1 + base]);
+          else if (m == NZ2 - NZ / 2) x = cscale(half, cconj(col[(size_t)(NZ / 2) * 3 * NY1 + base]));
+          else if (m > NZ2 - NZ / 2) x = col[(size_t)(m - (NZ2 - NZ)) * 3 * NY1 + base];
+          if (halve_x) x = cscale(half, x);
+        } else {
+          x = col[(size_t)m * 3 * NY1 + base];
+        }
+      }
+      v[n1] = x;
+    }
+    SmallFFT<T, N1, +1>::template run<1>(v);
+    C* y = Y + s * SEQ + n2;
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) {
+      C x = v[k1];
+      if (k1 != 0) x = cmul(x, cconj(tw[n2 * k1]));
+      y[k1 * PITCH] = x;
+    }
+  }
+  __syncthreads();
+  // stage 2: consecutive threads take consecutive rows k1 (coalesced stores)
+  for (int t = threadIdx.x; t < nseq * N1; t += blockDim.x) {
+    const int k1 = t % N1, s = t / N1;
+    const int jj = s % YB, c = s / YB;
+    C u[N2];
+    const C* y = Y + s * SEQ + k1 * PITCH;
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) u[n2] = y[n2];
+    SmallFFT<T, N2, +1>::template run<1>(u);
+    if (jj < nj) {
+      C* out = T1 + (((size_t)(j0 + jj) * 3 + c) * NXH + kx) * NZ2;
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) out[k1 + N1 * k2] = u[k2];
+    }
+  }
+}
+
+// --------------------------------------------------------------------------
+// k_zfwd_r: grid (nxh, ceil(ny1/YB)), block 256.  Forward z transform, fold,
+// scale and ikz combine (PFC/transform.f90:317-333, 639-688).
+template <typename T, int NZ2>
+__global__ void __launch_bounds__(256) k_zfwd_r(const cplx_t<T>* __restrict__ T2,
+                                                cplx_t<T>* __restrict__ vel, Geom g,
+                                                const cplx_t<T>* __restrict__ twz, GridDev gd,
+                                                int YB) {
+  using C = cplx_t<T>;
+  constexpr int N1 = Split<NZ2>::N1, N2 = Split<NZ2>::N2, PITCH = N2 + 1, SEQ = SeqPitch<NZ2>::V;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  const int nseq = 6 * YB;
+  C* Y = tw + NZ2;
+  C* Z = Y + nseq * SEQ;
+  const int NZ = g.nz, NY1 = g.ny1, NXH = g.nxh, ny = g.ny;
+  const int kx = blockIdx.x;
+  const int j0 = 1 + blockIdx.y * YB;   // 1-based first plane
+  for (int m = threadIdx.x; m < NZ2; m += blockDim.x) tw[m] = twz[m];
+  __syncthreads();
+  for (int t = threadIdx.x; t < nseq * N2; t += blockDim.x) {
+    const int s = t / N2, n2 = t - s * N2;
+    const int jj = s / 6, e = (s / 2) % 3, part = s & 1;
+    const int j = j0 + jj;
+    const bool valid = (j >= 2 && j <= ny) && !(e == 1 && j == ny);
+    C v[N1];
+    const C* src = T2 + ((((size_t)(j - 1) * 3 + e) * 2 + part) * NXH + kx) * NZ2;
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) v[n1] = valid ? src[N2 * n1 + n2] : czero<C>();
+    SmallFFT<T, N1, -1>::template run<1>(v);
+    C* y = Y + s * SEQ + n2;
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) {
+      C x = v[k1];
+      if (k1 != 0) x = cmul(x, tw[n2 * k1]);
+      y[k1 * PITCH] = x;
+    }
+  }
+  __syncthreads();
+  const int off = NZ2 - NZ;
+  for (int t = threadIdx.x; t < nseq * N1; t += blockDim.x) {
+    const int k1 = t % N1, s = t / N1;
+    C u[N2];
+    const C* y = Y + s * SEQ + k1 * PITCH;
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) u[n2] = y[n2];
+    SmallFFT<T, N2, -1>::template run<1>(u);
+    C* z = Z + s * NZ2;
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) {
+      const int k = k1 + N1 * k2;
+      if (k <= NZ / 2 || k >= off + NZ / 2) z[k] = u[k2];
+    }
+  }
+  __syncthreads();
+  const T scale = (T)(1.0 / ((double)g.nx2 * (double)g.nz2));
+  const T wsc = (kx == NXH - 1) ? (T)2 * scale : scale;
+  for (int idx = threadIdx.x; idx < NZ * 3 * YB; idx += blockDim.x) {
+    const int jj = idx % YB, e = (idx / YB) % 3, kz = idx / (3 * YB);
+    const int j = j0 + jj;
+    if (j > NY1) continue;
+    const bool valid = (j >= 2 && j <= ny) && !(e == 1 && j == ny);
+    C out = czero<C>();
+    if (valid) {
+      const C* A = Z + ((jj * 3 + e) * 2 + 0) * NZ2;
+      const C* Zc = Z + ((jj * 3 + e) * 2 + 1) * NZ2;
+      C fa, fz;
+      if (kz < NZ / 2) { fa = A[kz]; fz = Zc[kz]; }
+      else if (kz == NZ / 2) {
+        fa = cadd(A[NZ / 2], cconj(A[off + NZ / 2]));
+        fz = cadd(Zc[NZ / 2], cconj(Zc[off + NZ / 2]));
+      } else { fa = A[off + kz]; fz = Zc[off + kz]; }
+      const C tz = cscale(wsc, fz);
+      out = cadd(cimul<C>((T)gd.kz[kz], tz), cscale(wsc, fa));
+    }
+    vel[((size_t)(kx * NZ + kz) * 3 + e) * NY1 + (j - 1)] = out;
+  }
+}
+
+// --------------------------------------------------------------------------
+// k_xflux_r: grid (nz2/ZR, nchunks), block 256.  Same computation as k_xflux.
+template <typename T, int NX2, bool LIN>
+__global__ void __launch_bounds__(256) k_xflux_r(const cplx_t<T>* __restrict__ T1,
+                                                 cplx_t<T>* __restrict__ T2, Geom g,
+                                                 const cplx_t<T>* __restrict__ twx, GridDev gd,
+                                                 const T* __restrict__ fringe, int has_fringe,
+                                                 int ZR, int KC,
+                                                 unsigned long long* __restrict__ cflbits,
+                                                 int do_cfl) {
+  using C = cplx_t<T>;
+  constexpr int N1 = Split<NX2>::N1, N2 = Split<NX2>::N2, PITCH = N2 + 1, SEQ = SeqPitch<NX2>::V;
+  constexpr int N = NX2, Nh = NX2 / 2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int NXH = g.nxh, NZ2 = g.nz2, ny = g.ny;
+  const int NSEQ = 4 * ZR + (ZR + 1) / 2;
+  const int NREAL = 3 * ZR, NINV = (3 * ZR + 1) / 2;
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  T* win = reinterpret_cast<T*>(tw + N);                       // [3 slots][3][ZR][N]
+  C* raw = reinterpret_cast<C*>(win + 9 * ZR * N);             // [3*ZR][NXH]
+  C* Y = raw + 3 * ZR * NXH;                                   // [max(NSEQ,NINV)][SEQ]
+  C* F = Y + NSEQ * SEQ;                                       // [NSEQ][N]
+  const int z0 = blockIdx.x * ZR;
+  const int k0 = 2 + blockIdx.y * KC;
+  const int k1e = min(k0 + KC, ny + 1);
+  if (k0 > ny) return;
+  for (int m = threadIdx.x; m < N; m += blockDim.x) tw[m] = twx[m];
+  __shared__ T red[3][8];
+
+  auto load_plane = [&](int p, int slot) {
+    const bool vok = (p <= ny);
+    for (int idx = threadIdx.x; idx < 3 * NXH * ZR; idx += blockDim.x) {
+      const int r = idx % ZR, kx = (idx / ZR) % NXH, c = idx / (ZR * NXH);
+      C v = czero<C>();
+      if (c != 1 || vok) v = T1[(((size_t)(p - 1) * 3 + c) * NXH + kx) * NZ2 + z0 + r];
+      raw[(c * ZR + r) * NXH + kx] = v;
+    }
+    __syncthreads();
+    // stage 1 on the Hermitian-extended pairs z = x1 + i x2
+    for (int t = threadIdx.x; t < NINV * N2; t += blockDim.x) {
+      const int i = t / N2, n2 = t - i * N2;
+      const int s1 = 2 * i, s2 = 2 * i + 1;
+      C v[N1];
+#pragma unroll
+      for (int n1 = 0; n1 < N1; ++n1) {
+        const int k = N2 * n1 + n2;
+        const int kk = (k <= Nh) ? k : N - k;
+        C x1 = czero<C>(), x2 = czero<C>();
+        if (kk < NXH) {
+          x1 = raw[s1 * NXH + kk];
+          if (s2 < NREAL) x2 = raw[s2 * NXH + kk];
+        }
+        C z;
+        if (k == 0 || k == Nh) z = mk<C>(x1.x, x2.x);
+        else if (k < Nh) z = mk<C>(x1.x - x2.y, x1.y + x2.x);
+        else z = mk<C>(x1.x + x2.y, -x1.y + x2.x);
+        v[n1] = z;
+      }
+      SmallFFT<T, N1, +1>::template run<1>(v);
+      C* y = Y + i * SEQ + n2;
+#pragma unroll
+      for (int q = 0; q < N1; ++q) {
+        C x = v[q];
+        if (q != 0) x = cmul(x, cconj(tw[n2 * q]));
+        y[q * PITCH] = x;
+      }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < NINV * N1; t += blockDim.x) {
+      const int q = t % N1, i = t / N1;
+      const int s1 = 2 * i, s2 = 2 * i + 1;
+      C u[N2];
+      const C* y = Y + i * SEQ + q * PITCH;
+#pragma unroll
+      for (int n2 = 0; n2 < N2; ++n2) u[n2] = y[n2];
+      SmallFFT<T, N2, +1>::template run<1>(u);
+      T* w1 = win + ((slot * 3) * ZR + s1) * N;
+      T* w2 = win + ((slot * 3) * ZR + s2) * N;
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) {
+        w1[q + N1 * k2] = u[k2].x;
+        if (s2 < NREAL) w2[q + N1 * k2] = u[k2].y;
+      }
+    }
+    __syncthreads();
+  };
+
+  __syncthreads();
+  load_plane(k0 - 1, (k0 - 1) % 3);
+  load_plane(k0, k0 % 3);
+  const T half = (T)0.5, two = (T)2.0;
+  for (int k = k0; k < k1e; ++k) {
+    load_plane(k + 1, (k + 1) % 3);
+    const int sm = (k - 1) % 3, s0 = k % 3, sp = (k + 1) % 3;
+    const T dhk = (T)gd.dh[k - 1];
+    const T dnk = (k <= ny - 1) ? (T)gd.dn[k - 1] : (T)0;
+    const T iu1 = (k <= ny - 1) ? (T)gd.iu[2 * (k - 1)] : (T)0;
+    const T iu2 = (k <= ny - 1) ? (T)gd.iu[2 * (k - 1) + 1] : (T)0;
+    const T tu = (T)gd.target[(k - 1)], tv = (T)gd.target[(ny + 1) + (k - 1)];
+    const T tw_ = (T)gd.target[2 * (ny + 1) + (k - 1)];
+    T B0[3] = {0, 0, 0}, Bm[3] = {0, 0, 0}, Bp[3] = {0, 0, 0};
+    if (LIN) {
+      for (int q = 0; q < 3; ++q) {
+        B0[q] = (T)gd.baseflow[q * (ny + 1) + k - 1];
+        Bm[q] = (T)gd.baseflow[q * (ny + 1) + k - 2];
+        Bp[q] = (T)gd.baseflow[q * (ny + 1) + k];
+      }
+    }
+    const bool veq = (k <= ny - 1);
+    T ma = 0, mb = 0, mc = 0;
+    for (int idx = threadIdx.x; idx < ZR * N; idx += blockDim.x) {
+      const int x = idx % N, r = idx / N;
+#define WIN(s, c) win[(((s) * 3 + (c)) * ZR + r) * N + x]
+      const T U = WIN(s0, 0), V = WIN(s0, 1), W = WIN(s0, 2);
+      const T Up = WIN(sp, 0), Wp = WIN(sp, 2);
+      const T Vp = (k < ny) ? WIN(sp, 1) : V;
+      const T Um = WIN(sm, 0), Vm = WIN(sm, 1), Wm = WIN(sm, 2);
+#undef WIN
+      const T fr = has_fringe ? fringe[(size_t)(z0 + r) * N + x] : (T)0;
+      T fpu0, fpw0, fpu, fpw, xfu, zfu, xfw, zfw;
+      if (!LIN) {
+        if (k == 2) { fpu0 = Vm * Um; fpw0 = Vm * Wm; }
+        else { fpu0 = Vm * half * (Um + U); fpw0 = Vm * half * (Wm + W); }
+        if (k < ny) { fpu = V * half * (U + Up); fpw = V * half * (W + Wp); }
+        else { fpu = V * Up; fpw = V * Wp; }
+        xfu = U * U; zfu = W * U; xfw = U * W; zfw = W * W;
+      } else {
+        if (k == 2) { fpu0 = Bm[1] * Um + Vm * Bm[0]; fpw0 = Bm[1] * Wm + Vm * Bm[2]; }
+        else {
+          fpu0 = Bm[1] * half * (Um + U) + Vm * half * (Bm[0] + B0[0]);
+          fpw0 = Bm[1] * half * (Wm + W) + Vm * half * (Bm[2] + B0[2]);
+        }
+        if (k < ny) {
+          fpu = B0[1] * half * (U + Up) + V * half * (B0[0] + Bp[0]);
+          fpw = B0[1] * half * (W + Wp) + V * half * (B0[2] + Bp[2]);
+        } else {
+          fpu = B0[1] * Up + V * Bp[0];
+          fpw = B0[1] * Wp + V * Bp[2];
+        }
+        xfu = two * B0[0] * U; zfu = B0[2] * U + W * B0[0];
+        xfw = B0[2] * U + W * B0[0]; zfw = two * B0[2] * W;
+      }
+      const T dyu = dhk * (fpu - fpu0) + fr * (U - tu);
+      const T dyw = dhk * (fpw - fpw0) + fr * (W - tw_);
+      T xfv = 0, dyv = 0, zfv = 0;
+      if (veq) {
+        T fp0, fp;
+        if (!LIN) {
+          const T t0 = half * (Vm + V), t1 = half * (V + Vp);
+          fp0 = t0 * t0; fp = t1 * t1;
+          xfv = V * (iu1 * U + iu2 * Up);
+          zfv = V * (iu1 * W + iu2 * Wp);
+        } else {
+          const T t0 = half * (Vm + V), b0v = half * (Bm[1] + B0[1]);
+          const T t1 = half * (V + Vp), b1v = half * (B0[1] + Bp[1]);
+          fp0 = two * t0 * b0v; fp = two * t1 * b1v;
+          xfv = B0[1] * (iu1 * U + iu2 * Up) + V * (iu1 * B0[0] + iu2 * Bp[0]);
+          zfv = B0[1] * (iu1 * W + iu2 * Wp) + V * (iu1 * B0[2] + iu2 * Bp[2]);
+        }
+        dyv = dnk * (fp - fp0) + fr * (V - tv);
+      }
+      F[(4 * r + 0) * N + x] = mk<C>(xfu, dyu);
+      F[(4 * r + 1) * N + x] = mk<C>(xfw, dyw);
+      F[(4 * r + 2) * N + x] = mk<C>(xfv, dyv);
+      F[(4 * r + 3) * N + x] = mk<C>(zfu, zfw);
+      T* p4 = reinterpret_cast<T*>(F + (4 * ZR + r / 2) * N + x);
+      p4[r & 1] = zfv;
+      if ((ZR & 1) && r == ZR - 1) p4[1] = 0;
+      if (do_cfl) {
+        ma = fmax(ma, fabs(U + Up));
+        mb = fmax(mb, fabs(V));
+        mc = fmax(mc, fabs(W + Wp));
+      }
+    }
+    if (do_cfl) {
+      for (int o = 16; o > 0; o >>= 1) {
+        ma = fmax(ma, __shfl_xor_sync(0xffffffffu, ma, o));
+        mb = fmax(mb, __shfl_xor_sync(0xffffffffu, mb, o));
+        mc = fmax(mc, __shfl_xor_sync(0xffffffffu, mc, o));
+      }
+      const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+      if (lane == 0) { red[0][wid] = ma; red[1][wid] = mb; red[2][wid] = mc; }
+    }
+    __syncthreads();
+    if (do_cfl && threadIdx.x < 3) {
+      T m = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, red[threadIdx.x][w]);
+      atomicMax(&cflbits[(size_t)(k - 1) * 3 + threadIdx.x],
+                (unsigned long long)__double_as_longlong((double)m));
+    }
+    // forward x FFT of the NSEQ packed sequences: F -> Y -> F
+    for (int t = threadIdx.x; t < NSEQ * N2; t += blockDim.x) {
+      const int i = t / N2, n2 = t - i * N2;
+      C v[N1];
+      const C* src = F + i * N + n2;
+#pragma unroll
+      for (int n1 = 0; n1 < N1; ++n1) v[n1] = src[N2 * n1];
+      SmallFFT<T, N1, -1>::template run<1>(v);
+      C* y = Y + i * SEQ + n2;
+#pragma unroll
+      for (int q = 0; q < N1; ++q) {
+        C x = v[q];
+        if (q != 0) x = cmul(x, tw[n2 * q]);
+        y[q * PITCH] = x;
+      }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < NSEQ * N1; t += blockDim.x) {
+      const int q = t % N1, i = t / N1;
+      C u[N2];
+      const C* y = Y + i * SEQ + q * PITCH;
+#pragma unroll
+      for (int n2 = 0; n2 < N2; ++n2) u[n2] = y[n2];
+      SmallFFT<T, N2, -1>::template run<1>(u);
+      C* f = F + i * N;
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) f[q + N1 * k2] = u[k2];
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < NXH * ZR; idx += blockDim.x) {
+      const int r = idx % ZR, kx = idx / ZR;
+      const T kxv = (T)gd.kx[kx];
+      const int km = (kx == 0) ? 0 : N - kx;
+      const size_t base = (size_t)(k - 1) * 6;
+#define OUT(e, part) T2[((base + (e) * 2 + (part)) * NXH + kx) * NZ2 + z0 + r]
+      for (int e4 = 0; e4 < 4; ++e4) {
+        if (e4 == 2 && !veq) continue;
+        const C zk = F[(4 * r + e4) * N + kx], zm = F[(4 * r + e4) * N + km];
+        const C E = mk<C>(half * (zk.x + zm.x), half * (zk.y - zm.y));
+        const C O = mk<C>(half * (zk.y + zm.y), -half * (zk.x - zm.x));
+        if (e4 < 3) {
+          const int e = (e4 == 0) ? 0 : (e4 == 1 ? 2 : 1);
+          OUT(e, 0) = cadd(O, cimul<C>(kxv, E));
+        } else {
+          OUT(0, 1) = E;
+          OUT(2, 1) = O;
+        }
+      }
+      if (veq) {
+        const int i = 4 * ZR + r / 2;
+        const C zk = F[i * N + kx], zm = F[i * N + km];
+        C v;
+        if ((r & 1) == 0) v = mk<C>(half * (zk.x + zm.x), half * (zk.y - zm.y));
+        else v = mk<C>(half * (zk.y + zm.y), -half * (zk.x - zm.x));
+        OUT(1, 1) = v;
+      }
+#undef OUT
+    }
+    __syncthreads();
+  }
+}
+
+// smem sizes (bytes) of the three kernels
+template <typename T, int N> constexpr size_t zinv_r_smem(int YB) {
+  return sizeof(cplx_t<T>) * (N + (size_t)3 * YB * SeqPitch<N>::V);
+}
+template <typename T, int N> constexpr size_t zfwd_r_smem(int YB) {
+  return sizeof(cplx_t<T>) * (N + (size_t)6 * YB * SeqPitch<N>::V + (size_t)6 * YB * N);
+}
+template <typename T, int N> constexpr size_t xflux_r_smem(int ZR, int NXH) {
+  return sizeof(cplx_t<T>) * N + sizeof(T) * 9 * (size_t)ZR * N + sizeof(cplx_t<T>) * (3 * (size_t)ZR * NXH)
+         + sizeof(cplx_t<T>) * (size_t)(4 * ZR + (ZR + 1) / 2) * (SeqPitch<N>::V + N);
+}
+
+}  // namespace cfd
