@@ -15,6 +15,28 @@ template <int N> struct SeqPitch {
   static constexpr int V = Split<N>::N1 * (Split<N>::N2 + 1) + 1;
 };
 
+// Stage-1 twiddles W_N^(n2*q) stored as tw2[q*N2 + n2] so that consecutive
+// threads (consecutive n2) read consecutive words.
+template <typename T, int N>
+__device__ __forceinline__ void load_tw2(cplx_t<T>* tw2, const cplx_t<T>* __restrict__ tw) {
+  constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
+  for (int i = threadIdx.x; i < N1 * N2; i += blockDim.x) {
+    const int q = i / N2, n2 = i - q * N2;
+    tw2[i] = tw[n2 * q];
+  }
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
 // --------------------------------------------------------------------------
 // k_zinv_r: grid (nxh, ceil(ny1/YB)), block 256.  Inverse z transform of the
 // 3/2-padded columns (xz_fft_complex_to_real_parallel, PFC/transform.f90:345-368).
@@ -32,7 +54,7 @@ __global__ void __launch_bounds__(256) k_zinv_r(const cplx_t<T>* __restrict__ ve
   const int j0 = blockIdx.y * YB;
   const int nj = min(YB, NY1 - j0);
   const int nseq = 3 * YB;
-  for (int m = threadIdx.x; m < NZ2; m += blockDim.x) tw[m] = twz[m];
+  load_tw2<T, NZ2>(tw, twz);
   __syncthreads();
   const T half = (T)0.5;
   const bool halve_x = (g.nx2 > g.nx) && (kx == NXH - 1) && (NZ2 > NZ);
@@ -65,7 +87,7 @@ __global__ void __launch_bounds__(256) k_zinv_r(const cplx_t<T>* __restrict__ ve
 #pragma unroll
     for (int k1 = 0; k1 < N1; ++k1) {
       C x = v[k1];
-      if (k1 != 0) x = cmul(x, cconj(tw[n2 * k1]));
+      if (k1 != 0) x = cmul(x, cconj(tw[k1 * N2 + n2]));
       y[k1 * PITCH] = x;
     }
   }
@@ -105,7 +127,7 @@ __global__ void __launch_bounds__(256) k_zfwd_r(const cplx_t<T>* __restrict__ T2
   const int NZ = g.nz, NY1 = g.ny1, NXH = g.nxh, ny = g.ny;
   const int kx = blockIdx.x;
   const int j0 = 1 + blockIdx.y * YB;   // 1-based first plane
-  for (int m = threadIdx.x; m < NZ2; m += blockDim.x) tw[m] = twz[m];
+  load_tw2<T, NZ2>(tw, twz);
   __syncthreads();
   for (int t = threadIdx.x; t < nseq * N2; t += blockDim.x) {
     const int s = t / N2, n2 = t - s * N2;
@@ -121,7 +143,7 @@ __global__ void __launch_bounds__(256) k_zfwd_r(const cplx_t<T>* __restrict__ T2
 #pragma unroll
     for (int k1 = 0; k1 < N1; ++k1) {
       C x = v[k1];
-      if (k1 != 0) x = cmul(x, tw[n2 * k1]);
+      if (k1 != 0) x = cmul(x, tw[k1 * N2 + n2]);
       y[k1 * PITCH] = x;
     }
   }
@@ -168,6 +190,10 @@ __global__ void __launch_bounds__(256) k_zfwd_r(const cplx_t<T>* __restrict__ T2
 
 // --------------------------------------------------------------------------
 // k_xflux_r: grid (nz2/ZR, nchunks), block 256.  Same computation as k_xflux.
+// Per plane: the T1 rows of the next plane are gathered with cp.async into a
+// second buffer while the current plane is transformed; the forward x FFT runs
+// in place in a padded buffer (row pitch N2+1), which also hosts the inverse
+// transform's exchange.
 template <typename T, int NX2, bool LIN>
 __global__ void __launch_bounds__(256) k_xflux_r(const cplx_t<T>* __restrict__ T1,
                                                  cplx_t<T>* __restrict__ T2, Geom g,
@@ -183,31 +209,45 @@ __global__ void __launch_bounds__(256) k_xflux_r(const cplx_t<T>* __restrict__ T
   const int NXH = g.nxh, NZ2 = g.nz2, ny = g.ny;
   const int NSEQ = 4 * ZR + (ZR + 1) / 2;
   const int NREAL = 3 * ZR, NINV = (3 * ZR + 1) / 2;
-  C* tw = reinterpret_cast<C*>(smem_raw);
+  C* tw = reinterpret_cast<C*>(smem_raw);                      // tw2[q*N2 + n2]
   T* win = reinterpret_cast<T*>(tw + N);                       // [3 slots][3][ZR][N]
-  C* raw = reinterpret_cast<C*>(win + 9 * ZR * N);             // [3*ZR][NXH]
-  C* Y = raw + 3 * ZR * NXH;                                   // [max(NSEQ,NINV)][SEQ]
-  C* F = Y + NSEQ * SEQ;                                       // [NSEQ][N]
+  C* rawb = reinterpret_cast<C*>(win + 9 * ZR * N);            // 2 x [3][NXH][ZR]
+  C* FP = rawb + 2 * 3 * NXH * ZR;                             // [NSEQ][SEQ] padded
   const int z0 = blockIdx.x * ZR;
   const int k0 = 2 + blockIdx.y * KC;
   const int k1e = min(k0 + KC, ny + 1);
   if (k0 > ny) return;
-  for (int m = threadIdx.x; m < N; m += blockDim.x) tw[m] = twx[m];
+  load_tw2<T, N>(tw, twx);
   __shared__ T red[3][8];
+  // position of element x of a sequence in the padded layout
+  auto px = [](int x) { return (x / N2) * PITCH + (x % N2); };
 
-  auto load_plane = [&](int p, int slot) {
+  const int chunk_bytes = (int)sizeof(C) * ZR;
+  const bool v16 = (chunk_bytes % 16) == 0;
+  const int ncp = v16 ? chunk_bytes / 16 : chunk_bytes / 8;
+  auto issue_gather = [&](int p, C* raw) {
     const bool vok = (p <= ny);
-    for (int idx = threadIdx.x; idx < 3 * NXH * ZR; idx += blockDim.x) {
-      const int r = idx % ZR, kx = (idx / ZR) % NXH, c = idx / (ZR * NXH);
-      C v = czero<C>();
-      if (c != 1 || vok) v = T1[(((size_t)(p - 1) * 3 + c) * NXH + kx) * NZ2 + z0 + r];
-      raw[(c * ZR + r) * NXH + kx] = v;
+    for (int idx = threadIdx.x; idx < 3 * NXH * ncp; idx += blockDim.x) {
+      const int part = idx % ncp, kx = (idx / ncp) % NXH, c = idx / (ncp * NXH);
+      char* dst = reinterpret_cast<char*>(raw + (c * NXH + kx) * ZR) + part * (v16 ? 16 : 8);
+      if (c == 1 && !vok) {
+        if (v16) *reinterpret_cast<float4*>(dst) = make_float4(0.f, 0.f, 0.f, 0.f);
+        else *reinterpret_cast<float2*>(dst) = make_float2(0.f, 0.f);
+      } else {
+        const char* src = reinterpret_cast<const char*>(T1 + (((size_t)(p - 1) * 3 + c) * NXH + kx) * NZ2 + z0) +
+                          part * (v16 ? 16 : 8);
+        if (v16) cp_async16(dst, src);
+        else cp_async8(dst, src);
+      }
     }
-    __syncthreads();
-    // stage 1 on the Hermitian-extended pairs z = x1 + i x2
+  };
+
+  // inverse x transform of the gathered plane into window slot `slot`
+  auto inverse = [&](const C* raw, int slot) {
     for (int t = threadIdx.x; t < NINV * N2; t += blockDim.x) {
       const int i = t / N2, n2 = t - i * N2;
       const int s1 = 2 * i, s2 = 2 * i + 1;
+      const int c1 = s1 / ZR, r1 = s1 % ZR, c2 = s2 / ZR, r2 = s2 % ZR;
       C v[N1];
 #pragma unroll
       for (int n1 = 0; n1 < N1; ++n1) {
@@ -215,8 +255,8 @@ __global__ void __launch_bounds__(256) k_xflux_r(const cplx_t<T>* __restrict__ T
         const int kk = (k <= Nh) ? k : N - k;
         C x1 = czero<C>(), x2 = czero<C>();
         if (kk < NXH) {
-          x1 = raw[s1 * NXH + kk];
-          if (s2 < NREAL) x2 = raw[s2 * NXH + kk];
+          x1 = raw[(c1 * NXH + kk) * ZR + r1];
+          if (s2 < NREAL) x2 = raw[(c2 * NXH + kk) * ZR + r2];
         }
         C z;
         if (k == 0 || k == Nh) z = mk<C>(x1.x, x2.x);
@@ -225,11 +265,11 @@ __global__ void __launch_bounds__(256) k_xflux_r(const cplx_t<T>* __restrict__ T
         v[n1] = z;
       }
       SmallFFT<T, N1, +1>::template run<1>(v);
-      C* y = Y + i * SEQ + n2;
+      C* y = FP + i * SEQ + n2;
 #pragma unroll
       for (int q = 0; q < N1; ++q) {
         C x = v[q];
-        if (q != 0) x = cmul(x, cconj(tw[n2 * q]));
+        if (q != 0) x = cmul(x, cconj(tw[q * N2 + n2]));
         y[q * PITCH] = x;
       }
     }
@@ -238,7 +278,7 @@ __global__ void __launch_bounds__(256) k_xflux_r(const cplx_t<T>* __restrict__ T
       const int q = t % N1, i = t / N1;
       const int s1 = 2 * i, s2 = 2 * i + 1;
       C u[N2];
-      const C* y = Y + i * SEQ + q * PITCH;
+      const C* y = FP + i * SEQ + q * PITCH;
 #pragma unroll
       for (int n2 = 0; n2 < N2; ++n2) u[n2] = y[n2];
       SmallFFT<T, N2, +1>::template run<1>(u);
@@ -253,12 +293,8 @@ __global__ void __launch_bounds__(256) k_xflux_r(const cplx_t<T>* __restrict__ T
     __syncthreads();
   };
 
-  __syncthreads();
-  load_plane(k0 - 1, (k0 - 1) % 3);
-  load_plane(k0, k0 % 3);
   const T half = (T)0.5, two = (T)2.0;
-  for (int k = k0; k < k1e; ++k) {
-    load_plane(k + 1, (k + 1) % 3);
+  auto flux_plane = [&](int k) {
     const int sm = (k - 1) % 3, s0 = k % 3, sp = (k + 1) % 3;
     const T dhk = (T)gd.dh[k - 1];
     const T dnk = (k <= ny - 1) ? (T)gd.dn[k - 1] : (T)0;
@@ -327,11 +363,12 @@ __global__ void __launch_bounds__(256) k_xflux_r(const cplx_t<T>* __restrict__ T
         }
         dyv = dnk * (fp - fp0) + fr * (V - tv);
       }
-      F[(4 * r + 0) * N + x] = mk<C>(xfu, dyu);
-      F[(4 * r + 1) * N + x] = mk<C>(xfw, dyw);
-      F[(4 * r + 2) * N + x] = mk<C>(xfv, dyv);
-      F[(4 * r + 3) * N + x] = mk<C>(zfu, zfw);
-      T* p4 = reinterpret_cast<T*>(F + (4 * ZR + r / 2) * N + x);
+      const int pxx = px(x);
+      FP[(4 * r + 0) * SEQ + pxx] = mk<C>(xfu, dyu);
+      FP[(4 * r + 1) * SEQ + pxx] = mk<C>(xfw, dyw);
+      FP[(4 * r + 2) * SEQ + pxx] = mk<C>(xfv, dyv);
+      FP[(4 * r + 3) * SEQ + pxx] = mk<C>(zfu, zfw);
+      T* p4 = reinterpret_cast<T*>(FP + (4 * ZR + r / 2) * SEQ + pxx);
       p4[r & 1] = zfv;
       if ((ZR & 1) && r == ZR - 1) p4[1] = 0;
       if (do_cfl) {
@@ -356,35 +393,35 @@ __global__ void __launch_bounds__(256) k_xflux_r(const cplx_t<T>* __restrict__ T
       atomicMax(&cflbits[(size_t)(k - 1) * 3 + threadIdx.x],
                 (unsigned long long)__double_as_longlong((double)m));
     }
-    // forward x FFT of the NSEQ packed sequences: F -> Y -> F
+    // forward x FFT of the NSEQ packed sequences, in place
     for (int t = threadIdx.x; t < NSEQ * N2; t += blockDim.x) {
       const int i = t / N2, n2 = t - i * N2;
       C v[N1];
-      const C* src = F + i * N + n2;
+      C* col = FP + i * SEQ + n2;
 #pragma unroll
-      for (int n1 = 0; n1 < N1; ++n1) v[n1] = src[N2 * n1];
+      for (int n1 = 0; n1 < N1; ++n1) v[n1] = col[n1 * PITCH];
       SmallFFT<T, N1, -1>::template run<1>(v);
-      C* y = Y + i * SEQ + n2;
 #pragma unroll
       for (int q = 0; q < N1; ++q) {
         C x = v[q];
-        if (q != 0) x = cmul(x, tw[n2 * q]);
-        y[q * PITCH] = x;
+        if (q != 0) x = cmul(x, tw[q * N2 + n2]);
+        col[q * PITCH] = x;
       }
     }
     __syncthreads();
     for (int t = threadIdx.x; t < NSEQ * N1; t += blockDim.x) {
       const int q = t % N1, i = t / N1;
       C u[N2];
-      const C* y = Y + i * SEQ + q * PITCH;
+      C* row = FP + i * SEQ + q * PITCH;
 #pragma unroll
-      for (int n2 = 0; n2 < N2; ++n2) u[n2] = y[n2];
+      for (int n2 = 0; n2 < N2; ++n2) u[n2] = row[n2];
       SmallFFT<T, N2, -1>::template run<1>(u);
-      C* f = F + i * N;
+      // X[q + N1*k2] is kept at row q, column k2
 #pragma unroll
-      for (int k2 = 0; k2 < N2; ++k2) f[q + N1 * k2] = u[k2];
+      for (int k2 = 0; k2 < N2; ++k2) row[k2] = u[k2];
     }
     __syncthreads();
+    auto X = [&](int i, int kk) -> C { return FP[i * SEQ + (kk % N1) * PITCH + kk / N1]; };
     for (int idx = threadIdx.x; idx < NXH * ZR; idx += blockDim.x) {
       const int r = idx % ZR, kx = idx / ZR;
       const T kxv = (T)gd.kx[kx];
@@ -393,7 +430,7 @@ __global__ void __launch_bounds__(256) k_xflux_r(const cplx_t<T>* __restrict__ T
 #define OUT(e, part) T2[((base + (e) * 2 + (part)) * NXH + kx) * NZ2 + z0 + r]
       for (int e4 = 0; e4 < 4; ++e4) {
         if (e4 == 2 && !veq) continue;
-        const C zk = F[(4 * r + e4) * N + kx], zm = F[(4 * r + e4) * N + km];
+        const C zk = X(4 * r + e4, kx), zm = X(4 * r + e4, km);
         const C E = mk<C>(half * (zk.x + zm.x), half * (zk.y - zm.y));
         const C O = mk<C>(half * (zk.y + zm.y), -half * (zk.x - zm.x));
         if (e4 < 3) {
@@ -406,7 +443,7 @@ __global__ void __launch_bounds__(256) k_xflux_r(const cplx_t<T>* __restrict__ T
       }
       if (veq) {
         const int i = 4 * ZR + r / 2;
-        const C zk = F[i * N + kx], zm = F[i * N + km];
+        const C zk = X(i, kx), zm = X(i, km);
         C v;
         if ((r & 1) == 0) v = mk<C>(half * (zk.x + zm.x), half * (zk.y - zm.y));
         else v = mk<C>(half * (zk.y + zm.y), -half * (zk.x - zm.x));
@@ -415,6 +452,20 @@ __global__ void __launch_bounds__(256) k_xflux_r(const cplx_t<T>* __restrict__ T
 #undef OUT
     }
     __syncthreads();
+  };
+
+  // software pipeline over the planes k0-1 .. k1e: gather(p+1) overlaps the
+  // inverse transform of p and the fluxes / forward transform of p-1
+  const int pfirst = k0 - 1, plast = k1e;
+  issue_gather(pfirst, rawb);
+  cp_async_commit();
+  for (int p = pfirst; p <= plast; ++p) {
+    if (p + 1 <= plast) issue_gather(p + 1, rawb + ((p + 1 - pfirst) & 1) * 3 * NXH * ZR);
+    cp_async_commit();
+    cp_async_wait1();
+    __syncthreads();
+    inverse(rawb + ((p - pfirst) & 1) * 3 * NXH * ZR, p % 3);
+    if (p >= k0 + 1) flux_plane(p - 1);
   }
 }
 
@@ -426,8 +477,8 @@ template <typename T, int N> constexpr size_t zfwd_r_smem(int YB) {
   return sizeof(cplx_t<T>) * (N + (size_t)6 * YB * SeqPitch<N>::V + (size_t)6 * YB * N);
 }
 template <typename T, int N> constexpr size_t xflux_r_smem(int ZR, int NXH) {
-  return sizeof(cplx_t<T>) * N + sizeof(T) * 9 * (size_t)ZR * N + sizeof(cplx_t<T>) * (3 * (size_t)ZR * NXH)
-         + sizeof(cplx_t<T>) * (size_t)(4 * ZR + (ZR + 1) / 2) * (SeqPitch<N>::V + N);
+  return sizeof(cplx_t<T>) * N + sizeof(T) * 9 * (size_t)ZR * N + sizeof(cplx_t<T>) * (6 * (size_t)ZR * NXH)
+         + sizeof(cplx_t<T>) * (size_t)(4 * ZR + (ZR + 1) / 2) * SeqPitch<N>::V;
 }
 
 }  // namespace cfd
