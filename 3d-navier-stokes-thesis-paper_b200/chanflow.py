@@ -31,6 +31,7 @@ MIXED = 1
 ERRORS = {
     -1: "invalid argument", -2: "CUDA error", -3: "out of device memory",
     -4: "CFL IS TOO BIG", -5: "DT IS TOO BIG", -6: "call out of sequence",
+    -7: "size beyond the fixed scratch capacity",
 }
 
 
@@ -110,6 +111,7 @@ SYMBOLS = {
     "cfg_synchronize": (C.c_int, [_VP]),
     "cfg_launch_count": (C.c_longlong, [_VP]),
     "cfg_stream": (_VP, [_VP]),
+    "cfg_xz_c2r_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _VP, _VP, _VP]),
     "cfg_profile_enable": (C.c_int, [_VP, C.c_int]),
     "cfg_profile_read": (C.c_int, [_VP, C.c_int, C.c_char_p, C.c_int, C.POINTER(C.c_int), _DP]),
     "cfh_run_defaults": (None, [C.POINTER(CfhRun)]),

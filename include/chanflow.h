@@ -36,6 +36,7 @@ extern "C" {
 #define CFG_E_CFL (-4)        /* 'CFL IS TOO BIG', PFC/pass1.f90:235-244 */
 #define CFG_E_DT (-5)         /* 'DT IS TOO BIG', PFC/pass1.f90:228-233 */
 #define CFG_E_STATE (-6)      /* call out of sequence */
+#define CFG_E_SIZE (-7)       /* size beyond a fixed scratch capacity */
 
 #define CFG_FP64 0            /* every kernel in FP64 */
 #define CFG_MIXED 1           /* FP32 transforms/products/solves, FP64 mean mode */
@@ -174,6 +175,32 @@ long long cfg_launch_count(const cfg_ctx *c);
 int cfg_profile_enable(cfg_ctx *c, int on);
 int cfg_profile_read(cfg_ctx *c, int idx, char *name, int namelen, int *launches,
                      double *total_ms);
+
+/* cfg_xz_c2r_noalloc -- no counterpart in the reference.  The inverse x-z
+ * transform of one plane (the semantics of cfg_xz_c2r /
+ * xz_fft_complex_to_real) for callers that cannot allocate device memory:
+ * hosts whose device memory is pre-assigned at start-up by another owner (a
+ * framework's caching allocator, a communication library's registered
+ * buffers), where one more cudaMalloc would fail or fragment that pool, and
+ * step loops that cannot take the device-wide synchronisation that
+ * cudaMalloc/cudaFree imply.  It allocates nothing and needs no context.
+ *
+ *   cdata  device pointer, (nz, nx/2+1) complex FP64 (interleaved re, im)
+ *   data   device pointer, (nx2, nz2) real FP64 (written)
+ *   stream cudaStream_t to run on (NULL: the legacy default stream)
+ *
+ * Its intermediate plane and twiddle tables live in one fixed file-scope
+ * device array of 4.06 MiB that every GPU loading the library holds until
+ * exit.  Limits: (nx/2+1)*nz2 <= 262144 and nx2, nz2 <= 2048 (2^a 3^b, even);
+ * larger planes return CFG_E_SIZE.  Every call shares that array and it keeps
+ * the previous call's contents (each call rewrites all it reads, nothing must
+ * start at zero), so calls whose executions overlap on the GPU -- other
+ * streams, other host threads -- race; serialise them.  The first call on a
+ * device performs a one-time set-up (it looks up the array's device address
+ * with that device current); make that first call before any stream capture.
+ * Returns CFG_OK, CFG_E_ARG, CFG_E_SIZE or CFG_E_CUDA. */
+int cfg_xz_c2r_noalloc(int nx, int nz, int nx2, int nz2, const double *cdata,
+                       double *data, void *stream);
 
 #ifdef __cplusplus
 }
