@@ -14,6 +14,7 @@
 #include "pass1.cuh"
 #include "pass2.cuh"
 #include "pass1_fast.h"
+#include "pass2v2.h"
 #include "planes.cuh"
 #include "regfft.cuh"
 
@@ -152,6 +153,7 @@ struct cfg_ctx {
   size_t sm_rhs64 = 0;
   // register-FFT pass-1 kernels (when the lengths are compiled in)
   bool fast_z = false, fast_x = false;
+  bool use_rhs2 = true;
   int fYB1 = 1, fYB3 = 1, fZR = 1;
   // optional per-launch CUDA-event timing on the context stream
   bool prof_on = false;
@@ -312,6 +314,7 @@ struct Impl {
       if (p1_fast_smem(1, g.nx2, f32, c->fZR, g.nxh) > 220 * 1024) c->fast_x = false;
     }
     if (getenv("CHANFLOW_GENERIC_FFT")) c->fast_x = c->fast_z = false;
+    c->use_rhs2 = rhs2_supported(g.ny1) && !getenv("CHANFLOW_RHS_V1");
     c->twx = make_twiddles<T>(g.nx2);
     c->twz = make_twiddles<T>(g.nz2);
     c->twxs = make_twiddles<T>(g.nx);
@@ -375,7 +378,16 @@ struct Impl {
   template <int MM>
   static int rhs_m(cfg_ctx* c, int rk, int mode) {
     const Geom& g = c->g;
-    if (c->n_fast > 0) {
+    if (c->n_fast > 0 && mode == 0 && c->use_rhs2) {
+      Rhs2Launch a{};
+      a.vel = c->vel; a.cru = c->cru; a.prs = c->prs;
+      a.cbc_top = (const C*)c->cbc + 3 * (size_t)g.nw; a.cbc_bot = c->cbc;
+      a.g = g; a.gd = c->gd; a.sc = c->sc; a.rkt = c->rkt; a.rk = rk; a.re = c->p.re;
+      a.wlist = c->wl_fast; a.nlist = c->n_fast; a.warps = sizeof(T) == 4 ? 4 : 2; a.st = c->st;
+      prof_begin(c, "k_rhs");
+      if (rhs2_launch(sizeof(T) == 4, a) != 0) return fail(c, CFG_E_CUDA, "k_rhs2 launch");
+      CKL();
+    } else if (c->n_fast > 0) {
       dim3 gr((c->n_fast + 3) / 4);
       prof_begin(c, "k_rhs");
       k_rhs<T, T, MM><<<gr, 128, c->sm_rhs, c->st>>>((C*)c->vel, (C*)c->cru, (C*)c->prs,

@@ -1,0 +1,430 @@
+// pass2v2.cuh -- the RK3/Crank-Nicolson substep of PFC/pass2.f90:184-352
+// (PHASE1) for the (kx,kz) != (0,0) wavenumbers, G lanes per wavenumber
+// (G = 16 or 32, 32/G wavenumbers per warp).  Same arithmetic as k_rhs
+// (pass2.cuh) mode 0, organised for throughput:
+//   - the seven input columns (NL u,v,w; cru u,v,w; p) are copied into shared
+//     memory with cp.async at the start, contiguous per column;
+//   - u and w share one partition solve (same Helmholtz matrix, two right-hand
+//     sides); every solve multiplies by reciprocals;
+//   - the outputs are staged in shared memory and stored coalesced.
+#pragma once
+#include "cfd_common.cuh"
+#include "pass1.cuh"
+#include "pass1_reg.cuh"
+#include "pass2.cuh"
+
+namespace cfd {
+
+// One strided PCR step (stride 2t in interface rows = t lanes) of one slot.
+template <typename T, int G, int NR>
+__device__ __forceinline__ void pcr_step(T& A, T& B, T& Cc, cplx_t<T> (&Fv)[NR], int t, int g) {
+  using C = cplx_t<T>;
+  const unsigned full = 0xffffffffu;
+  const bool hasl = g >= t, hasu = g + t < G;
+  T la = __shfl_up_sync(full, A, t, G), lb = __shfl_up_sync(full, B, t, G), lc = __shfl_up_sync(full, Cc, t, G);
+  T ua = __shfl_down_sync(full, A, t, G), ub = __shfl_down_sync(full, B, t, G), uc = __shfl_down_sync(full, Cc, t, G);
+  C lf[NR], uf[NR];
+#pragma unroll
+  for (int r = 0; r < NR; ++r) {
+    lf[r] = mk<C>(__shfl_up_sync(full, Fv[r].x, t, G), __shfl_up_sync(full, Fv[r].y, t, G));
+    uf[r] = mk<C>(__shfl_down_sync(full, Fv[r].x, t, G), __shfl_down_sync(full, Fv[r].y, t, G));
+  }
+  if (!hasl) {
+    la = 0; lb = 1; lc = 0;
+#pragma unroll
+    for (int r = 0; r < NR; ++r) lf[r] = czero<C>();
+  }
+  if (!hasu) {
+    ua = 0; ub = 1; uc = 0;
+#pragma unroll
+    for (int r = 0; r < NR; ++r) uf[r] = czero<C>();
+  }
+  const T k1 = A * ((T)1 / lb), k2 = Cc * ((T)1 / ub);
+  const T nB = B - k1 * lc - k2 * ua;
+#pragma unroll
+  for (int r = 0; r < NR; ++r)
+    Fv[r] = mk<C>(Fv[r].x - k1 * lf[r].x - k2 * uf[r].x, Fv[r].y - k1 * lf[r].y - k2 * uf[r].y);
+  A = -k1 * la;
+  Cc = -k2 * uc;
+  B = nB;
+}
+
+// Partition + PCR solve over the G lanes of a lane group, NR right-hand sides.
+// Row j = g*M + i of lane g:  a[i] x_{j-1} + b[i] x_j + c[i] x_{j+1} = f[r][i].
+// Rows past the system are identity rows.  Solutions overwrite f.
+template <typename T, int M, int G, int NR>
+__device__ __forceinline__ void tri_group_solve(T (&a)[M], T (&b)[M], T (&c)[M],
+                                                cplx_t<T> (&f)[NR][M], int g) {
+  using C = cplx_t<T>;
+  static_assert(M >= 2, "at least two rows per lane");
+  T ap[M], cq[M], rb[M];
+  ap[0] = 0;
+  ap[1] = a[1];
+  rb[0] = (T)1 / b[0];
+#pragma unroll
+  for (int i = 2; i < M; ++i) {
+    const T rr = a[i] * ((T)1 / b[i - 1]);
+    ap[i] = -rr * ap[i - 1];
+    b[i] = b[i] - rr * c[i - 1];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) f[r][i] = mk<C>(f[r][i].x - rr * f[r][i - 1].x, f[r][i].y - rr * f[r][i - 1].y);
+  }
+#pragma unroll
+  for (int i = 1; i < M; ++i) rb[i] = (T)1 / b[i];
+#pragma unroll
+  for (int i = 0; i < M; ++i) cq[i] = 0;
+  if (M > 2) cq[M - 2] = c[M - 2];
+#pragma unroll
+  for (int i = M - 3; i >= 1; --i) {
+    const T rr = c[i] * rb[i + 1];
+    ap[i] = ap[i] - rr * ap[i + 1];
+    cq[i] = -rr * cq[i + 1];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) f[r][i] = mk<C>(f[r][i].x - rr * f[r][i + 1].x, f[r][i].y - rr * f[r][i + 1].y);
+  }
+  T A0 = a[0], B0 = b[0], C0 = c[0];
+  C F0[NR];
+#pragma unroll
+  for (int r = 0; r < NR; ++r) F0[r] = f[r][0];
+  if (M > 2) {
+    const T rr = c[0] * rb[1];
+    B0 = b[0] - rr * ap[1];
+    C0 = -rr * cq[1];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) F0[r] = mk<C>(f[r][0].x - rr * f[r][1].x, f[r][0].y - rr * f[r][1].y);
+  }
+  T A1 = ap[M - 1], B1 = b[M - 1], C1 = c[M - 1];
+  C F1[NR];
+#pragma unroll
+  for (int r = 0; r < NR; ++r) F1[r] = f[r][M - 1];
+  const unsigned full = 0xffffffffu;
+  {
+    // stride 1: slot 0's lower neighbour is lane g-1 slot 1, slot 1's upper is lane g+1 slot 0
+    T la = __shfl_up_sync(full, A1, 1, G), lb = __shfl_up_sync(full, B1, 1, G), lc = __shfl_up_sync(full, C1, 1, G);
+    T ua = __shfl_down_sync(full, A0, 1, G), ub = __shfl_down_sync(full, B0, 1, G), uc = __shfl_down_sync(full, C0, 1, G);
+    C lf[NR], uf[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      lf[r] = mk<C>(__shfl_up_sync(full, F1[r].x, 1, G), __shfl_up_sync(full, F1[r].y, 1, G));
+      uf[r] = mk<C>(__shfl_down_sync(full, F0[r].x, 1, G), __shfl_down_sync(full, F0[r].y, 1, G));
+    }
+    if (g == 0) {
+      la = 0; lb = 1; lc = 0;
+#pragma unroll
+      for (int r = 0; r < NR; ++r) lf[r] = czero<C>();
+    }
+    if (g == G - 1) {
+      ua = 0; ub = 1; uc = 0;
+#pragma unroll
+      for (int r = 0; r < NR; ++r) uf[r] = czero<C>();
+    }
+    const T k1a = A0 * ((T)1 / lb), k2a = C0 * ((T)1 / B1);
+    const T k1b = A1 * ((T)1 / B0), k2b = C1 * ((T)1 / ub);
+    const T nA0 = -k1a * la, nC0 = -k2a * C1, nB0 = B0 - k1a * lc - k2a * A1;
+    const T nA1 = -k1b * A0, nC1 = -k2b * uc, nB1 = B1 - k1b * C0 - k2b * ua;
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      const C nF0 = mk<C>(F0[r].x - k1a * lf[r].x - k2a * F1[r].x, F0[r].y - k1a * lf[r].y - k2a * F1[r].y);
+      const C nF1 = mk<C>(F1[r].x - k1b * F0[r].x - k2b * uf[r].x, F1[r].y - k1b * F0[r].y - k2b * uf[r].y);
+      F0[r] = nF0;
+      F1[r] = nF1;
+    }
+    A0 = nA0; B0 = nB0; C0 = nC0;
+    A1 = nA1; B1 = nB1; C1 = nC1;
+  }
+#pragma unroll
+  for (int t = 1; t < G; t <<= 1) {
+    pcr_step<T, G, NR>(A0, B0, C0, F0, t, g);
+    pcr_step<T, G, NR>(A1, B1, C1, F1, t, g);
+  }
+  const T r0 = (T)1 / B0, r1 = (T)1 / B1;
+#pragma unroll
+  for (int r = 0; r < NR; ++r) {
+    const C x0 = mk<C>(F0[r].x * r0, F0[r].y * r0);
+    const C xl = mk<C>(F1[r].x * r1, F1[r].y * r1);
+#pragma unroll
+    for (int i = 1; i < M - 1; ++i)
+      f[r][i] = mk<C>((f[r][i].x - ap[i] * x0.x - cq[i] * xl.x) * rb[i], (f[r][i].y - ap[i] * x0.y - cq[i] * xl.y) * rb[i]);
+    f[r][0] = x0;
+    f[r][M - 1] = xl;
+  }
+}
+
+// second difference of column s at row j of an n-row system (copied end rows)
+template <typename T>
+__device__ __forceinline__ cplx_t<T> d2c(const cplx_t<T>* s, const double* __restrict__ d, int j, int n) {
+  using C = cplx_t<T>;
+  const int j0 = (j == 0) ? 1 : ((j == n - 1) ? n - 2 : j);
+  const T d1 = (T)__ldg(d + 3 * j), d2 = (T)__ldg(d + 3 * j + 1), d3 = (T)__ldg(d + 3 * j + 2);
+  const C fm = s[j0 - 1], f0 = s[j0], fp = s[j0 + 1];
+  return mk<C>(d1 * fm.x + d2 * f0.x + d3 * fp.x, d1 * fm.y + d2 * f0.y + d3 * fp.y);
+}
+
+// column stride (complex elements) of the staged columns: >= G*M rows, even
+// (16-byte aligned for FP32 complex)
+template <int M, int G> struct Ld2 {
+  static constexpr int V = ((G * M + 1) / 2) * 2;
+};
+
+template <typename T, int M, int G>
+__global__ void __launch_bounds__(128) k_rhs2(cplx_t<T>* __restrict__ vel, cplx_t<T>* __restrict__ cru,
+                                              cplx_t<T>* __restrict__ prs,
+                                              const cplx_t<T>* __restrict__ cbc_top,
+                                              const cplx_t<T>* __restrict__ cbc_bot, Geom g,
+                                              GridDev gd, const DevScalars* __restrict__ sc, RkTab rkt,
+                                              int rk, double re, const int* __restrict__ wlist,
+                                              int nlist) {
+  using C = cplx_t<T>;
+  constexpr int LD = Ld2<M, G>::V;
+  constexpr int GPW = 32 / G;                 // lane groups (wavenumbers) per warp
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int grp = lane / G, gl = lane % G;
+  const int widx = (blockIdx.x * (blockDim.x >> 5) + warp) * GPW + grp;
+  const bool valid = widx < nlist;
+  const int w = valid ? wlist[widx] : 1;
+  const int NZ = g.nz, ny = g.ny, n1 = g.ny1;
+  const size_t nw = (size_t)g.nw;
+  const int kxi = w / NZ, kzi = w % NZ;
+  const T kx = (T)gd.kx[kxi], kz = (T)gd.kz[kzi];
+  const T k2 = valid ? (T)(gd.kx[kxi] * gd.kx[kxi] + gd.kz[kzi] * gd.kz[kzi]) : (T)1;
+  C* S = reinterpret_cast<C*>(smem_raw) + (size_t)(warp * GPW + grp) * 8 * LD;
+  C* sNL = S;            // 3 columns: nonlinear term (then the next accumulator)
+  C* sV = S + 3 * LD;    // 3 columns: cru, then the new velocity cv
+  C* sP = S + 6 * LD;    // pressure
+  C* sH = S + 7 * LD;    // pressure correction
+  C* gvel = vel + (size_t)w * 3 * n1;
+  C* gcru = cru + (size_t)w * 3 * n1;
+  C* gprs = prs + (size_t)w * n1;
+
+  // ---- asynchronous staging of the seven input columns
+  if (valid) {
+    const int cb = (int)(n1 * sizeof(C));
+    if ((cb % 16) == 0) {
+      const int nch = cb / 16;
+      for (int idx = gl; idx < 7 * nch; idx += G) {
+        const int col = idx / nch, part = idx - col * nch;
+        const C* src = (col < 3) ? gvel + col * n1 : (col < 6 ? gcru + (col - 3) * n1 : gprs);
+        cp_async16(reinterpret_cast<char*>(S + col * LD) + part * 16, reinterpret_cast<const char*>(src) + part * 16);
+      }
+    } else {
+      const int nch = cb / 8;
+      for (int idx = gl; idx < 7 * nch; idx += G) {
+        const int col = idx / nch, part = idx - col * nch;
+        const C* src = (col < 3) ? gvel + col * n1 : (col < 6 ? gcru + (col - 3) * n1 : gprs);
+        cp_async8(reinterpret_cast<char*>(S + col * LD) + part * 8, reinterpret_cast<const char*>(src) + part * 8);
+      }
+    }
+  } else {
+    for (int idx = gl; idx < 8 * LD; idx += G) S[idx] = czero<C>();
+  }
+  cp_async_commit();
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  __syncwarp();
+
+  const double dt = sc->dt;
+  const T coef = (T)(rkt.b[rk] * dt);
+  const T vis_imp = (T)(rkt.d[rk] * (dt / re));
+  const T rk_press = (T)((rkt.c[rk] + rkt.d[rk]) * dt);
+  const T alpha = (T)1 + vis_imp * k2;
+  // ---- stage A: cv = cru + coef*cu (+ explicit viscous term and old pressure gradient on rk1)
+  {
+    const T vis_exp = (T)(rkt.c[rk] * (dt / re));
+    C r[3][M];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const double* d2 = (q == 1) ? gd.d2n : gd.d2h;
+      const int nq = (q == 1) ? ny : n1;
+#pragma unroll
+      for (int i = 0; i < M; ++i) {
+        const int j = gl * M + i;
+        C v = czero<C>();
+        if (j < n1) {
+          const C cr = sV[q * LD + j];
+          const C nl = sNL[q * LD + j];
+          v = mk<C>(cr.x - coef * nl.x, cr.y - coef * nl.y);
+          if (rk == 1) {
+            if (j < nq) {
+              const C du = d2c<T>(sV + q * LD, d2, j, nq);
+              v = cadd(v, cscale(vis_exp, csub(du, cscale(k2, cr))));
+            }
+            if (j >= 1 && j <= ny - 1) {
+              const C p = sP[j];
+              if (q == 0) v = csub(v, cimul<C>(rk_press * kx, p));
+              else if (q == 2) v = csub(v, cimul<C>(rk_press * kz, p));
+              else if (j <= ny - 2) v = csub(v, cscale(rk_press * (T)gd.dn[j], csub(sP[j + 1], p)));
+            }
+          }
+        }
+        r[q][i] = v;
+      }
+    }
+    __syncwarp();
+    // ---- stage B: Helmholtz solves, u and w together (d2h), then v (d2n)
+    {
+      T a[M], b[M], c[M];
+      C f[2][M];
+#pragma unroll
+      for (int i = 0; i < M; ++i) {
+        const int j = gl * M + i;
+        if (j == 0) {
+          a[i] = 0; b[i] = 1; c[i] = 0;
+          f[0][i] = cbc_bot[w]; f[1][i] = cbc_bot[2 * nw + w];
+        } else if (j == n1 - 1) {
+          a[i] = 0; b[i] = 1; c[i] = 0;
+          f[0][i] = cbc_top[w]; f[1][i] = cbc_top[2 * nw + w];
+        } else if (j < n1 - 1) {
+          a[i] = -vis_imp * (T)__ldg(gd.d2h + 3 * j);
+          b[i] = -vis_imp * (T)__ldg(gd.d2h + 3 * j + 1) + alpha;
+          c[i] = -vis_imp * (T)__ldg(gd.d2h + 3 * j + 2);
+          f[0][i] = r[0][i]; f[1][i] = r[2][i];
+        } else {
+          a[i] = 0; b[i] = 1; c[i] = 0;
+          f[0][i] = czero<C>(); f[1][i] = czero<C>();
+        }
+      }
+      tri_group_solve<T, M, G, 2>(a, b, c, f, gl);
+#pragma unroll
+      for (int i = 0; i < M; ++i) {
+        const int j = gl * M + i;
+        if (j < LD) { sV[j] = f[0][i]; sV[2 * LD + j] = f[1][i]; }
+      }
+    }
+    {
+      T a[M], b[M], c[M];
+      C f[1][M];
+#pragma unroll
+      for (int i = 0; i < M; ++i) {
+        const int j = gl * M + i;
+        if (j == 0) { a[i] = 0; b[i] = 1; c[i] = 0; f[0][i] = cbc_bot[nw + w]; }
+        else if (j == ny - 1) { a[i] = 0; b[i] = 1; c[i] = 0; f[0][i] = cbc_top[nw + w]; }
+        else if (j < ny - 1) {
+          a[i] = -vis_imp * (T)__ldg(gd.d2n + 3 * j);
+          b[i] = -vis_imp * (T)__ldg(gd.d2n + 3 * j + 1) + alpha;
+          c[i] = -vis_imp * (T)__ldg(gd.d2n + 3 * j + 2);
+          f[0][i] = r[1][i];
+        } else { a[i] = 0; b[i] = 1; c[i] = 0; f[0][i] = czero<C>(); }
+      }
+      tri_group_solve<T, M, G, 1>(a, b, c, f, gl);
+#pragma unroll
+      for (int i = 0; i < M; ++i) {
+        const int j = gl * M + i;
+        if (j < LD) sV[LD + j] = f[0][i];
+      }
+    }
+    __syncwarp();
+  }
+  // ---- stage C: strip_divergence (PFC/solve.f90:14-50) and SOLVE_P
+  {
+    const T tmp = (T)1 / rk_press;
+    T a[M], b[M], c[M];
+    C f[1][M];
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      const int j = gl * M + i;
+      if (j == 0) {
+        const T dn0 = (T)gd.dn[0];
+        a[i] = 0; b[i] = -dn0; c[i] = dn0; f[0][i] = czero<C>();
+      } else if (j == n1 - 1) {
+        const T dnl = (T)gd.dn[ny - 1];
+        a[i] = -dnl; b[i] = dnl; c[i] = 0; f[0][i] = czero<C>();
+      } else if (j < n1 - 1) {
+        const T dh = (T)gd.dh[j], dm1 = (T)gd.dn[j - 1], dn0 = (T)gd.dn[j];
+        a[i] = dh * dm1;
+        b[i] = -(dh * dm1) - dh * dn0 - k2;
+        c[i] = dh * dn0;
+        const C dv = cscale(dh, csub(sV[LD + j], sV[LD + j - 1]));
+        const C s = cadd(cadd(cimul<C>(kx, sV[j]), dv), cimul<C>(kz, sV[2 * LD + j]));
+        f[0][i] = cscale(tmp, s);
+      } else { a[i] = 0; b[i] = 1; c[i] = 0; f[0][i] = czero<C>(); }
+    }
+    tri_group_solve<T, M, G, 1>(a, b, c, f, gl);
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      const int j = gl * M + i;
+      if (j < LD) sH[j] = f[0][i];
+    }
+    __syncwarp();
+    if (gl == 0) {
+      const T m11 = (T)gd.dm[0], m21 = (T)gd.dm[1], m31 = (T)gd.dm[2];
+      const T m12 = (T)gd.dm[3], m22 = (T)gd.dm[4], m32 = (T)gd.dm[5];
+      const C p1 = sH[1], p2 = sH[2], q1 = sH[ny - 2], q2 = sH[ny - 1];
+      sH[0] = mk<C>((-m21 * p1.x - m31 * p2.x) / m11, (-m21 * p1.y - m31 * p2.y) / m11);
+      sH[ny] = mk<C>((-m12 * q1.x - m22 * q2.x) / m32, (-m12 * q1.y - m22 * q2.y) / m32);
+    }
+    __syncwarp();
+    // subtract the correction gradient from cv; p += alpha*ch - vis_imp*D2h(ch)
+    C pn[M];
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      const int j = gl * M + i;
+      pn[i] = czero<C>();
+      if (j < n1) {
+        const C ch = sH[j];
+        if (j >= 1 && j <= ny - 1) {
+          sV[j] = csub(sV[j], cimul<C>(rk_press * kx, ch));
+          sV[2 * LD + j] = csub(sV[2 * LD + j], cimul<C>(rk_press * kz, ch));
+          if (j <= ny - 2) sV[LD + j] = csub(sV[LD + j], cscale(rk_press * (T)gd.dn[j], csub(sH[j + 1], ch)));
+        }
+        const C d2c_ = d2c<T>(sH, gd.d2h, j, n1);
+        const C p = sP[j];
+        pn[i] = mk<C>(p.x + alpha * ch.x - vis_imp * d2c_.x, p.y + alpha * ch.y - vis_imp * d2c_.y);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      const int j = gl * M + i;
+      if (j < n1) sP[j] = pn[i];
+    }
+    __syncwarp();
+  }
+  // ---- stage D: next-substep accumulator (PFC/pass2.f90:312-333) into the NL columns
+  if (rk < 3) {
+    const T coef2 = (T)(dt * rkt.a[rk + 1]);
+    const T vis_exp2 = (T)((dt / re) * rkt.c[rk + 1]);
+    const T rkp2 = (T)((rkt.c[rk + 1] + rkt.d[rk + 1]) * dt);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const double* d2 = (q == 1) ? gd.d2n : gd.d2h;
+      const int nq = (q == 1) ? ny : n1;
+#pragma unroll
+      for (int i = 0; i < M; ++i) {
+        const int j = gl * M + i;
+        if (j >= n1) continue;
+        const C cv = sV[q * LD + j];
+        const C nl = sNL[q * LD + j];
+        C v = mk<C>(cv.x - coef2 * nl.x, cv.y - coef2 * nl.y);
+        if (j < nq) {
+          const C du = d2c<T>(sV + q * LD, d2, j, nq);
+          v = cadd(v, cscale(vis_exp2, csub(du, cscale(k2, cv))));
+        }
+        if (j >= 1 && j <= ny - 1) {
+          const C p = sP[j];
+          if (q == 0) v = csub(v, cimul<C>(rkp2 * kx, p));
+          else if (q == 2) v = csub(v, cimul<C>(rkp2 * kz, p));
+          else if (j <= ny - 2) v = csub(v, cscale(rkp2 * (T)gd.dn[j], csub(sP[j + 1], p)));
+        }
+        sNL[q * LD + j] = v;
+      }
+    }
+  } else {
+    for (int idx = gl; idx < 3 * LD; idx += G) sNL[idx] = sV[idx];
+  }
+  __syncwarp();
+  // ---- coalesced stores: data1 <- cv, data2 <- accumulator, data4 <- p
+  if (valid) {
+    for (int q = 0; q < 3; ++q)
+      for (int j = gl; j < n1; j += G) {
+        gvel[q * n1 + j] = sV[q * LD + j];
+        gcru[q * n1 + j] = sNL[q * LD + j];
+      }
+    for (int j = gl; j < n1; j += G) gprs[j] = sP[j];
+  }
+}
+
+template <typename T, int M, int G>
+constexpr size_t rhs2_smem(int warps) {
+  return sizeof(cplx_t<T>) * (size_t)warps * (32 / G) * 8 * Ld2<M, G>::V;
+}
+
+}  // namespace cfd

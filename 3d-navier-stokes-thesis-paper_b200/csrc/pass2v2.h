@@ -1,0 +1,29 @@
+// pass2v2.h -- launch interface of the v2 RK substep kernel.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "pass1.cuh"
+#include "pass2.cuh"
+
+namespace cfd {
+
+struct Rhs2Launch {
+  void *vel, *cru, *prs;
+  const void *cbc_top, *cbc_bot;
+  Geom g;
+  GridDev gd;
+  const DevScalars* sc;
+  RkTab rkt;
+  int rk;
+  double re;
+  const int* wlist;
+  int nlist;
+  int warps;   // warps per block
+  cudaStream_t st;
+};
+
+// 0 on success, -1 unsupported size, -2 launch error
+int rhs2_launch(bool f32, const Rhs2Launch& a);
+bool rhs2_supported(int ny1);
+
+}  // namespace cfd
