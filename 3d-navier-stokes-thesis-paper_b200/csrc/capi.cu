@@ -107,6 +107,11 @@ struct cfg_ctx {
   bool mixed = false;
   int dev = 0;
   cudaStream_t st = nullptr;
+  // side stream: the small mean-mode and FP64 low-|k| solves run beside the
+  // main per-wavenumber kernel; joined back with events
+  cudaStream_t st2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaStream_t prof_stream = nullptr;
   std::string err;
   long long launches = 0;
   int step = 0;
@@ -177,12 +182,12 @@ static void prof_begin(cfg_ctx* c, const char* name) {
   if (!c->prof_on) return;
   c->cur_name = name;
   c->cur_a = prof_event(c);
-  cudaEventRecord(c->cur_a, c->st);
+  cudaEventRecord(c->cur_a, c->prof_stream ? c->prof_stream : c->st);
 }
 static void prof_end(cfg_ctx* c) {
   if (!c->prof_on || !c->cur_name) return;
   cudaEvent_t b = prof_event(c);
-  cudaEventRecord(b, c->st);
+  cudaEventRecord(b, c->prof_stream ? c->prof_stream : c->st);
   c->recs.push_back({c->cur_name, c->cur_a, b});
   c->cur_name = nullptr;
 }
@@ -295,17 +300,19 @@ struct Impl {
       RHS_ATTR(2) RHS_ATTR(3) RHS_ATTR(4) RHS_ATTR(5) RHS_ATTR(6) RHS_ATTR(7) RHS_ATTR(8)
 #undef RHS_ATTR
     }
-    // register-FFT kernels: tile sizes that keep two blocks per SM
+    // register-FFT kernels: z-kernel tiles that keep four (FP32) or two (FP64)
+    // blocks per SM, matching their launch bounds
     const bool f32 = sizeof(T) == 4;
     c->fast_z = regfft_supported(g.nz2);
     c->fast_x = regfft_supported(g.nx2);
     if (c->fast_z) {
+      const size_t zb = f32 ? 52 * 1024 : 108 * 1024;
       c->fYB1 = 1;
       for (int yb = 8; yb >= 1; --yb)
-        if (p1_fast_smem(0, g.nz2, f32, yb, g.nxh) <= budget) { c->fYB1 = yb; break; }
+        if (p1_fast_smem(0, g.nz2, f32, yb, g.nxh) <= zb) { c->fYB1 = yb; break; }
       c->fYB3 = 1;
       for (int yb = 4; yb >= 1; --yb)
-        if (p1_fast_smem(2, g.nz2, f32, yb, g.nxh) <= budget) { c->fYB3 = yb; break; }
+        if (p1_fast_smem(2, g.nz2, f32, yb, g.nxh) <= zb) { c->fYB3 = yb; break; }
     }
     if (c->fast_x) {
       c->fZR = 1;
@@ -378,6 +385,27 @@ struct Impl {
   template <int MM>
   static int rhs_m(cfg_ctx* c, int rk, int mode) {
     const Geom& g = c->g;
+    // fork: the mean mode and the FP64 low-|k| list on the side stream
+    CK(cudaEventRecord(c->ev_fork, c->st));
+    CK(cudaStreamWaitEvent(c->st2, c->ev_fork, 0));
+    c->prof_stream = c->st2;
+    if (c->n_prec > 0) {
+      dim3 gr((c->n_prec + 3) / 4);
+      prof_begin(c, "k_rhs_fp64");
+      k_rhs<double, T, MM><<<gr, 128, c->sm_rhs64, c->st2>>>((C*)c->vel, (C*)c->cru, (C*)c->prs,
+                                                             (const C*)c->cbc + 3 * (size_t)g.nw, (const C*)c->cbc, g,
+                                                             c->gd, c->sc, c->rkt, rk, c->p.re, mode, c->wl_prec,
+                                                             c->n_prec);
+      CKL();
+    }
+    if (mode == 0) c->mean64_valid = true;
+    prof_begin(c, "k_rhs_mean");
+    k_rhs_mean<T, MM><<<1, 32, 0, c->st2>>>((C*)c->vel, (C*)c->cru, (C*)c->prs, c->mvel64, c->mcru64,
+                                           (const C*)c->cbc + 3 * (size_t)g.nw, (const C*)c->cbc, g, c->gd, c->sc,
+                                           c->d_um_dy, c->rkt, rk, c->p.re, c->p.beta, c->p.fix_mass, mode);
+    CKL();
+    c->prof_stream = nullptr;
+    CK(cudaEventRecord(c->ev_join, c->st2));
     if (c->n_fast > 0 && mode == 0 && c->use_rhs2) {
       Rhs2Launch a{};
       a.vel = c->vel; a.cru = c->cru; a.prs = c->prs;
@@ -395,21 +423,8 @@ struct Impl {
                                                      c->gd, c->sc, c->rkt, rk, c->p.re, mode, c->wl_fast, c->n_fast);
       CKL();
     }
-    if (c->n_prec > 0) {
-      dim3 gr((c->n_prec + 3) / 4);
-      prof_begin(c, "k_rhs_fp64");
-      k_rhs<double, T, MM><<<gr, 128, c->sm_rhs64, c->st>>>((C*)c->vel, (C*)c->cru, (C*)c->prs,
-                                                            (const C*)c->cbc + 3 * (size_t)g.nw, (const C*)c->cbc, g,
-                                                            c->gd, c->sc, c->rkt, rk, c->p.re, mode, c->wl_prec,
-                                                            c->n_prec);
-      CKL();
-    }
-    if (mode == 0) c->mean64_valid = true;
-    prof_begin(c, "k_rhs_mean");
-    k_rhs_mean<T, MM><<<1, 32, 0, c->st>>>((C*)c->vel, (C*)c->cru, (C*)c->prs, c->mvel64, c->mcru64,
-                                          (const C*)c->cbc + 3 * (size_t)g.nw, (const C*)c->cbc, g, c->gd, c->sc,
-                                          c->d_um_dy, c->rkt, rk, c->p.re, c->p.beta, c->p.fix_mass, mode);
-    CKL();
+    // join
+    CK(cudaStreamWaitEvent(c->st, c->ev_join, 0));
     return CFG_OK;
   }
   static int rhs(cfg_ctx* c, int rk, int mode) {
@@ -562,7 +577,13 @@ int cfg_create(const cfg_params* p, const cfg_grid* gr, cfg_ctx** out) {
   }
   c->dev = p->device;
   if (cudaSetDevice(c->dev) != cudaSuccess) { fail(c, CFG_E_CUDA, "cudaSetDevice"); delete c; return CFG_E_CUDA; }
-  if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) { delete c; return CFG_E_CUDA; }
+  if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+    delete c;
+    return CFG_E_CUDA;
+  }
   // RK constants: single-precision literals widened (PFC/pass2.f90:14-18)
   const float ra[3] = {0.0f, -17.0f / 60.0f, -5.0f / 12.0f}, rb[3] = {8.0f / 15.0f, 5.0f / 12.0f, 3.0f / 4.0f};
   const float rc[3] = {29.0f / 96.0f, -3.0f / 40.0f, 1.0f / 6.0f}, rd[3] = {37.0f / 160.0f, 5.0f / 24.0f, 1.0f / 6.0f};
@@ -703,6 +724,9 @@ void cfg_destroy(cfg_ctx* c) {
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
+  if (c->st2) cudaStreamDestroy(c->st2);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
 }

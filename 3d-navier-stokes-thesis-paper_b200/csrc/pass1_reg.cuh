@@ -41,7 +41,7 @@ __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_g
 // k_zinv_r: grid (nxh, ceil(ny1/YB)), block 256.  Inverse z transform of the
 // 3/2-padded columns (xz_fft_complex_to_real_parallel, PFC/transform.f90:345-368).
 template <typename T, int NZ2>
-__global__ void __launch_bounds__(256) k_zinv_r(const cplx_t<T>* __restrict__ vel,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_zinv_r(const cplx_t<T>* __restrict__ vel,
                                                 cplx_t<T>* __restrict__ T1, Geom g,
                                                 const cplx_t<T>* __restrict__ twz, int YB) {
   using C = cplx_t<T>;
@@ -113,17 +113,19 @@ __global__ void __launch_bounds__(256) k_zinv_r(const cplx_t<T>* __restrict__ ve
 // k_zfwd_r: grid (nxh, ceil(ny1/YB)), block 256.  Forward z transform, fold,
 // scale and ikz combine (PFC/transform.f90:317-333, 639-688).
 template <typename T, int NZ2>
-__global__ void __launch_bounds__(256) k_zfwd_r(const cplx_t<T>* __restrict__ T2,
-                                                cplx_t<T>* __restrict__ vel, Geom g,
-                                                const cplx_t<T>* __restrict__ twz, GridDev gd,
-                                                int YB) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_zfwd_r(const cplx_t<T>* __restrict__ T2,
+                                                   cplx_t<T>* __restrict__ vel, Geom g,
+                                                   const cplx_t<T>* __restrict__ twz, GridDev gd,
+                                                   int YB) {
   using C = cplx_t<T>;
   constexpr int N1 = Split<NZ2>::N1, N2 = Split<NZ2>::N2, PITCH = N2 + 1, SEQ = SeqPitch<NZ2>::V;
+  constexpr int ZP = NZ2 + 1;   // pitch of the stage-2 output (spreads banks across sequences)
+  static_assert(ZP <= SEQ, "stage-2 output must fit in the exchange buffer");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tw = reinterpret_cast<C*>(smem_raw);
   const int nseq = 6 * YB;
   C* Y = tw + NZ2;
-  C* Z = Y + nseq * SEQ;
+  C* Z = Y;                      // stage 2 reads Y into registers, then overwrites it
   const int NZ = g.nz, NY1 = g.ny1, NXH = g.nxh, ny = g.ny;
   const int kx = blockIdx.x;
   const int j0 = 1 + blockIdx.y * YB;   // 1-based first plane
@@ -149,19 +151,30 @@ __global__ void __launch_bounds__(256) k_zfwd_r(const cplx_t<T>* __restrict__ T2
   }
   __syncthreads();
   const int off = NZ2 - NZ;
-  for (int t = threadIdx.x; t < nseq * N1; t += blockDim.x) {
-    const int k1 = t % N1, s = t / N1;
+  // stage 2 in rounds of whole sequences: read all rows of the round, then
+  // synchronise before overwriting the exchange buffer with the outputs (the
+  // output of sequence s only overlaps exchange rows of sequences <= s)
+  const int spr = blockDim.x / N1;
+  for (int s0 = 0; s0 < nseq; s0 += spr) {
+    const int s = s0 + (int)threadIdx.x / N1, k1 = (int)threadIdx.x % N1;
+    const bool act = ((int)threadIdx.x < spr * N1) && s < nseq;
     C u[N2];
-    const C* y = Y + s * SEQ + k1 * PITCH;
+    if (act) {
+      const C* y = Y + s * SEQ + k1 * PITCH;
 #pragma unroll
-    for (int n2 = 0; n2 < N2; ++n2) u[n2] = y[n2];
-    SmallFFT<T, N2, -1>::template run<1>(u);
-    C* z = Z + s * NZ2;
-#pragma unroll
-    for (int k2 = 0; k2 < N2; ++k2) {
-      const int k = k1 + N1 * k2;
-      if (k <= NZ / 2 || k >= off + NZ / 2) z[k] = u[k2];
+      for (int n2 = 0; n2 < N2; ++n2) u[n2] = y[n2];
     }
+    __syncthreads();
+    if (act) {
+      SmallFFT<T, N2, -1>::template run<1>(u);
+      C* z = Z + s * ZP;
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) {
+        const int k = k1 + N1 * k2;
+        if (k <= NZ / 2 || k >= off + NZ / 2) z[k] = u[k2];
+      }
+    }
+    if (s0 + spr < nseq) __syncthreads();
   }
   __syncthreads();
   const T scale = (T)(1.0 / ((double)g.nx2 * (double)g.nz2));
@@ -173,8 +186,8 @@ __global__ void __launch_bounds__(256) k_zfwd_r(const cplx_t<T>* __restrict__ T2
     const bool valid = (j >= 2 && j <= ny) && !(e == 1 && j == ny);
     C out = czero<C>();
     if (valid) {
-      const C* A = Z + ((jj * 3 + e) * 2 + 0) * NZ2;
-      const C* Zc = Z + ((jj * 3 + e) * 2 + 1) * NZ2;
+      const C* A = Z + ((jj * 3 + e) * 2 + 0) * ZP;
+      const C* Zc = Z + ((jj * 3 + e) * 2 + 1) * ZP;
       C fa, fz;
       if (kz < NZ / 2) { fa = A[kz]; fz = Zc[kz]; }
       else if (kz == NZ / 2) {
@@ -474,7 +487,7 @@ template <typename T, int N> constexpr size_t zinv_r_smem(int YB) {
   return sizeof(cplx_t<T>) * (N + (size_t)3 * YB * SeqPitch<N>::V);
 }
 template <typename T, int N> constexpr size_t zfwd_r_smem(int YB) {
-  return sizeof(cplx_t<T>) * (N + (size_t)6 * YB * SeqPitch<N>::V + (size_t)6 * YB * N);
+  return sizeof(cplx_t<T>) * (N + (size_t)6 * YB * SeqPitch<N>::V);
 }
 template <typename T, int N> constexpr size_t xflux_r_smem(int ZR, int NXH) {
   return sizeof(cplx_t<T>) * N + sizeof(T) * 9 * (size_t)ZR * N + sizeof(cplx_t<T>) * (6 * (size_t)ZR * NXH)

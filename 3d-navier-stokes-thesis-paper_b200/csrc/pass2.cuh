@@ -16,6 +16,15 @@ namespace cfd {
 
 struct RkTab {   // RK3 constants as the reference widens them (PFC/pass2.f90:14-18)
   double a[4], b[4], c[4], d[4];
+  // select by substep without indexing a kernel parameter at run time (which
+  // would copy the table to a local stack frame)
+  __device__ __forceinline__ static double pick(const double (&v)[4], int k) {
+    return k == 1 ? v[1] : (k == 2 ? v[2] : (k == 3 ? v[3] : v[0]));
+  }
+  __device__ __forceinline__ double A(int k) const { return pick(a, k); }
+  __device__ __forceinline__ double B(int k) const { return pick(b, k); }
+  __device__ __forceinline__ double Cc(int k) const { return pick(c, k); }
+  __device__ __forceinline__ double D(int k) const { return pick(d, k); }
 };
 
 // Partition + PCR solve of a tridiagonal system distributed M rows per lane
@@ -340,9 +349,9 @@ __global__ void __launch_bounds__(128) k_rhs(cplx_t<S>* __restrict__ vel,
   } else {
     // ---- stage A: cv = cru + coef*cu (+ explicit viscous, old pressure on rk1)
     const double dt = sc->dt;
-    const T coef = (T)(rkt.b[rk] * dt);
-    const T vis_exp = (T)(rkt.c[rk] * (dt / re));
-    const T rk_press = (T)((rkt.c[rk] + rkt.d[rk]) * dt);
+    const T coef = (T)(rkt.B(rk) * dt);
+    const T vis_exp = (T)(rkt.Cc(rk) * (dt / re));
+    const T rk_press = (T)((rkt.Cc(rk) + rkt.D(rk)) * dt);
     C* scol[3] = {su, sv, sw};
     for (int q = 0; q < 3; ++q) load_col<C, M>(scol[q], gcru + q * n1, n1, lane);
     __syncwarp();
@@ -373,7 +382,7 @@ __global__ void __launch_bounds__(128) k_rhs(cplx_t<S>* __restrict__ vel,
     __syncwarp();
     if (rk == 1) sub_grad<T, M>(su, sv, sw, sp, rk_press, kx, kz, ny, gd, lane);
     // ---- stage B: Helmholtz solves for u, w (ny+1 rows, d2h) and v (ny rows, d2n)
-    const T vis_imp = (T)(rkt.d[rk] * (dt / re));
+    const T vis_imp = (T)(rkt.D(rk) * (dt / re));
     const T alpha = (T)1 + vis_imp * k2;
     helmholtz_col<T, M>(su, n1, alpha, vis_imp, gd.d2h, cvt<C>(cbc_top[w]), cvt<C>(cbc_bot[w]), lane);
     helmholtz_col<T, M>(sw, n1, alpha, vis_imp, gd.d2h, cvt<C>(cbc_top[2 * nw + w]), cvt<C>(cbc_bot[2 * nw + w]), lane);
@@ -384,7 +393,7 @@ __global__ void __launch_bounds__(128) k_rhs(cplx_t<S>* __restrict__ vel,
 
   // ---- stage C: strip_divergence (PFC/solve.f90:14-50)
   const double dt = sc->dt;
-  const T rk_press = (mode == 0) ? (T)((rkt.c[rk] + rkt.d[rk]) * dt) : (T)1;
+  const T rk_press = (mode == 0) ? (T)((rkt.Cc(rk) + rkt.D(rk)) * dt) : (T)1;
   {
     const T tmp = (T)1 / rk_press;
     C r[M];
@@ -417,7 +426,7 @@ __global__ void __launch_bounds__(128) k_rhs(cplx_t<S>* __restrict__ vel,
     return;
   }
   // ---- p = p + alpha*ch - vis_imp*D2h(ch)  (Brown, Cortez & Minion)
-  const T vis_imp = (T)(rkt.d[rk] * (dt / re));
+  const T vis_imp = (T)(rkt.D(rk) * (dt / re));
   const T alpha = (T)1 + vis_imp * k2;
   {
     C r[M];
@@ -439,9 +448,9 @@ __global__ void __launch_bounds__(128) k_rhs(cplx_t<S>* __restrict__ vel,
   // ---- stage D: next-substep accumulator (PFC/pass2.f90:312-333) and stores
   C* scol[3] = {su, sv, sw};
   if (rk < 3) {
-    const T coef2 = (T)(dt * rkt.a[rk + 1]);
-    const T vis_exp2 = (T)((dt / re) * rkt.c[rk + 1]);
-    const T rkp2 = (T)((rkt.c[rk + 1] + rkt.d[rk + 1]) * dt);
+    const T coef2 = (T)(dt * rkt.A(rk + 1));
+    const T vis_exp2 = (T)((dt / re) * rkt.Cc(rk + 1));
+    const T rkp2 = (T)((rkt.Cc(rk + 1) + rkt.D(rk + 1)) * dt);
     for (int q = 0; q < 3; ++q) {
       const double* d2 = (q == 1) ? gd.d2n : gd.d2h;
       const int nq = (q == 1) ? ny : n1;
@@ -544,9 +553,9 @@ __global__ void __launch_bounds__(32) k_rhs_mean(cplx_t<T>* __restrict__ vel,
     return;
   }
   const double dt = sc->dt;
-  const double coef = rkt.b[rk] * dt;
-  const double vis_imp = rkt.d[rk] * (dt / re);
-  const double rk_press = (rkt.c[rk] + rkt.d[rk]) * dt;
+  const double coef = rkt.B(rk) * dt;
+  const double vis_imp = rkt.D(rk) * (dt / re);
+  const double rk_press = (rkt.Cc(rk) + rkt.D(rk)) * dt;
   C* scol[3] = {su, sv, sw};
   // cv = cru + coef*cu (+ explicit viscous on rk1)
   for (int q = 0; q < 3; ++q) {
@@ -561,7 +570,7 @@ __global__ void __launch_bounds__(32) k_rhs_mean(cplx_t<T>* __restrict__ vel,
         const cplx_t<T> nl = vel[q * n1 + j];
         v = mk<C>(cr.x - coef * (double)nl.x, cr.y - coef * (double)nl.y);
         if (rk == 1 && j < nq) {
-          const double vis_exp = rkt.c[rk] * (dt / re);
+          const double vis_exp = rkt.Cc(rk) * (dt / re);
           const C du = d2_row<double, M>(st, d2, j, nq);
           v = cadd(v, cscale(vis_exp, du));
         }
@@ -598,8 +607,8 @@ __global__ void __launch_bounds__(32) k_rhs_mean(cplx_t<T>* __restrict__ vel,
       const C cv = scol[q][CI::at(j)];
       C v = cv;
       if (rk < 3) {
-        const double coef2 = dt * rkt.a[rk + 1];
-        const double vis_exp2 = (dt / re) * rkt.c[rk + 1];
+        const double coef2 = dt * rkt.A(rk + 1);
+        const double vis_exp2 = (dt / re) * rkt.Cc(rk + 1);
         const cplx_t<T> nl = vel[q * n1 + j];
         v = mk<C>(cv.x - coef2 * (double)nl.x, cv.y - coef2 * (double)nl.y);
         if (j < nq) v = cadd(v, cscale(vis_exp2, d2_row<double, M>(scol[q], d2, j, nq)));

@@ -188,48 +188,48 @@ __global__ void __launch_bounds__(128) k_rhs2(cplx_t<T>* __restrict__ vel, cplx_
   const int kxi = w / NZ, kzi = w % NZ;
   const T kx = (T)gd.kx[kxi], kz = (T)gd.kz[kzi];
   const T k2 = valid ? (T)(gd.kx[kxi] * gd.kx[kxi] + gd.kz[kzi] * gd.kz[kzi]) : (T)1;
-  C* S = reinterpret_cast<C*>(smem_raw) + (size_t)(warp * GPW + grp) * 8 * LD;
-  C* sNL = S;            // 3 columns: nonlinear term (then the next accumulator)
-  C* sV = S + 3 * LD;    // 3 columns: cru, then the new velocity cv
-  C* sP = S + 6 * LD;    // pressure
-  C* sH = S + 7 * LD;    // pressure correction
+  C* S = reinterpret_cast<C*>(smem_raw) + (size_t)(warp * GPW + grp) * 5 * LD;
+  C* sV = S;             // 3 columns: cru, then the new velocity cv
+  C* sP = S + 3 * LD;    // pressure
+  C* sH = S + 4 * LD;    // pressure correction
   C* gvel = vel + (size_t)w * 3 * n1;
   C* gcru = cru + (size_t)w * 3 * n1;
   C* gprs = prs + (size_t)w * n1;
 
-  // ---- asynchronous staging of the seven input columns
+  // ---- asynchronous staging of the four input columns cru (u,v,w) and p;
+  // the nonlinear term is read at each lane's own rows, where it is used
   if (valid) {
     const int cb = (int)(n1 * sizeof(C));
     if ((cb % 16) == 0) {
       const int nch = cb / 16;
-      for (int idx = gl; idx < 7 * nch; idx += G) {
+      for (int idx = gl; idx < 4 * nch; idx += G) {
         const int col = idx / nch, part = idx - col * nch;
-        const C* src = (col < 3) ? gvel + col * n1 : (col < 6 ? gcru + (col - 3) * n1 : gprs);
+        const C* src = (col < 3) ? gcru + col * n1 : gprs;
         cp_async16(reinterpret_cast<char*>(S + col * LD) + part * 16, reinterpret_cast<const char*>(src) + part * 16);
       }
     } else {
       const int nch = cb / 8;
-      for (int idx = gl; idx < 7 * nch; idx += G) {
+      for (int idx = gl; idx < 4 * nch; idx += G) {
         const int col = idx / nch, part = idx - col * nch;
-        const C* src = (col < 3) ? gvel + col * n1 : (col < 6 ? gcru + (col - 3) * n1 : gprs);
+        const C* src = (col < 3) ? gcru + col * n1 : gprs;
         cp_async8(reinterpret_cast<char*>(S + col * LD) + part * 8, reinterpret_cast<const char*>(src) + part * 8);
       }
     }
   } else {
-    for (int idx = gl; idx < 8 * LD; idx += G) S[idx] = czero<C>();
+    for (int idx = gl; idx < 5 * LD; idx += G) S[idx] = czero<C>();
   }
   cp_async_commit();
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   __syncwarp();
 
   const double dt = sc->dt;
-  const T coef = (T)(rkt.b[rk] * dt);
-  const T vis_imp = (T)(rkt.d[rk] * (dt / re));
-  const T rk_press = (T)((rkt.c[rk] + rkt.d[rk]) * dt);
+  const T coef = (T)(rkt.B(rk) * dt);
+  const T vis_imp = (T)(rkt.D(rk) * (dt / re));
+  const T rk_press = (T)((rkt.Cc(rk) + rkt.D(rk)) * dt);
   const T alpha = (T)1 + vis_imp * k2;
   // ---- stage A: cv = cru + coef*cu (+ explicit viscous term and old pressure gradient on rk1)
   {
-    const T vis_exp = (T)(rkt.c[rk] * (dt / re));
+    const T vis_exp = (T)(rkt.Cc(rk) * (dt / re));
     C r[3][M];
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
@@ -241,7 +241,7 @@ __global__ void __launch_bounds__(128) k_rhs2(cplx_t<T>* __restrict__ vel, cplx_
         C v = czero<C>();
         if (j < n1) {
           const C cr = sV[q * LD + j];
-          const C nl = sNL[q * LD + j];
+          const C nl = valid ? gvel[q * n1 + j] : czero<C>();
           v = mk<C>(cr.x - coef * nl.x, cr.y - coef * nl.y);
           if (rk == 1) {
             if (j < nq) {
@@ -378,53 +378,53 @@ __global__ void __launch_bounds__(128) k_rhs2(cplx_t<T>* __restrict__ vel, cplx_
     }
     __syncwarp();
   }
-  // ---- stage D: next-substep accumulator (PFC/pass2.f90:312-333) into the NL columns
-  if (rk < 3) {
-    const T coef2 = (T)(dt * rkt.a[rk + 1]);
-    const T vis_exp2 = (T)((dt / re) * rkt.c[rk + 1]);
-    const T rkp2 = (T)((rkt.c[rk + 1] + rkt.d[rk + 1]) * dt);
+  // ---- stage D: next-substep accumulator (PFC/pass2.f90:312-333), stored
+  // from each lane's own rows; then data1 <- cv and data4 <- p, coalesced
+  if (valid) {
+    if (rk < 3) {
+      const T coef2 = (T)(dt * rkt.A(rk + 1));
+      const T vis_exp2 = (T)((dt / re) * rkt.Cc(rk + 1));
+      const T rkp2 = (T)((rkt.Cc(rk + 1) + rkt.D(rk + 1)) * dt);
 #pragma unroll
-    for (int q = 0; q < 3; ++q) {
-      const double* d2 = (q == 1) ? gd.d2n : gd.d2h;
-      const int nq = (q == 1) ? ny : n1;
+      for (int q = 0; q < 3; ++q) {
+        const double* d2 = (q == 1) ? gd.d2n : gd.d2h;
+        const int nq = (q == 1) ? ny : n1;
 #pragma unroll
-      for (int i = 0; i < M; ++i) {
-        const int j = gl * M + i;
-        if (j >= n1) continue;
-        const C cv = sV[q * LD + j];
-        const C nl = sNL[q * LD + j];
-        C v = mk<C>(cv.x - coef2 * nl.x, cv.y - coef2 * nl.y);
-        if (j < nq) {
-          const C du = d2c<T>(sV + q * LD, d2, j, nq);
-          v = cadd(v, cscale(vis_exp2, csub(du, cscale(k2, cv))));
+        for (int i = 0; i < M; ++i) {
+          const int j = gl * M + i;
+          if (j >= n1) continue;
+          const C cv = sV[q * LD + j];
+          const C nl = gvel[q * n1 + j];
+          C v = mk<C>(cv.x - coef2 * nl.x, cv.y - coef2 * nl.y);
+          if (j < nq) {
+            const C du = d2c<T>(sV + q * LD, d2, j, nq);
+            v = cadd(v, cscale(vis_exp2, csub(du, cscale(k2, cv))));
+          }
+          if (j >= 1 && j <= ny - 1) {
+            const C p = sP[j];
+            if (q == 0) v = csub(v, cimul<C>(rkp2 * kx, p));
+            else if (q == 2) v = csub(v, cimul<C>(rkp2 * kz, p));
+            else if (j <= ny - 2) v = csub(v, cscale(rkp2 * (T)gd.dn[j], csub(sP[j + 1], p)));
+          }
+          gcru[q * n1 + j] = v;
         }
-        if (j >= 1 && j <= ny - 1) {
-          const C p = sP[j];
-          if (q == 0) v = csub(v, cimul<C>(rkp2 * kx, p));
-          else if (q == 2) v = csub(v, cimul<C>(rkp2 * kz, p));
-          else if (j <= ny - 2) v = csub(v, cscale(rkp2 * (T)gd.dn[j], csub(sP[j + 1], p)));
-        }
-        sNL[q * LD + j] = v;
       }
+    } else {
+      for (int q = 0; q < 3; ++q)
+        for (int j = gl; j < n1; j += G) gcru[q * n1 + j] = sV[q * LD + j];
     }
-  } else {
-    for (int idx = gl; idx < 3 * LD; idx += G) sNL[idx] = sV[idx];
   }
   __syncwarp();
-  // ---- coalesced stores: data1 <- cv, data2 <- accumulator, data4 <- p
   if (valid) {
     for (int q = 0; q < 3; ++q)
-      for (int j = gl; j < n1; j += G) {
-        gvel[q * n1 + j] = sV[q * LD + j];
-        gcru[q * n1 + j] = sNL[q * LD + j];
-      }
+      for (int j = gl; j < n1; j += G) gvel[q * n1 + j] = sV[q * LD + j];
     for (int j = gl; j < n1; j += G) gprs[j] = sP[j];
   }
 }
 
 template <typename T, int M, int G>
 constexpr size_t rhs2_smem(int warps) {
-  return sizeof(cplx_t<T>) * (size_t)warps * (32 / G) * 8 * Ld2<M, G>::V;
+  return sizeof(cplx_t<T>) * (size_t)warps * (32 / G) * 5 * Ld2<M, G>::V;
 }
 
 }  // namespace cfd
