@@ -124,6 +124,10 @@ struct cfg_ctx {
   void *vel = nullptr, *cru = nullptr, *prs = nullptr;
   double2 *mvel64 = nullptr, *mcru64 = nullptr;
   void *T1 = nullptr, *T2 = nullptr;
+  // physical planes of the split x stage (k_xinv_r -> k_flux_r)
+  void* P = nullptr;
+  bool split_x = false;
+  int flux_zr = 4;
   void* cbc = nullptr;   // [bot, top][3][nw]
   DevScalars* sc = nullptr;
   double* d_um_dy = nullptr;
@@ -321,6 +325,17 @@ struct Impl {
       if (p1_fast_smem(1, g.nx2, f32, c->fZR, g.nxh) > 220 * 1024) c->fast_x = false;
     }
     if (getenv("CHANFLOW_GENERIC_FFT")) c->fast_x = c->fast_z = false;
+    // split x stage: physical planes written once, fluxes read three of them
+    c->flux_zr = getenv("CHANFLOW_FLUX_ZR") ? atoi(getenv("CHANFLOW_FLUX_ZR")) : 4;
+    if (c->flux_zr != 2) c->flux_zr = 4;
+    c->split_x = c->fast_x && !getenv("CHANFLOW_FUSED_XFLUX") && g.nz2 % (f32 ? 16 : 8) == 0 &&
+                 g.nz2 % c->flux_zr == 0 && p1_fast_smem(3, g.nx2, f32, 0, g.nxh) <= 200 * 1024 &&
+                 p1_fast_smem(4, g.nx2, f32, c->flux_zr, g.nxh) <= 200 * 1024;
+    if (c->split_x &&
+        cudaMalloc(&c->P, sizeof(T) * (size_t)(g.ny + 1) * 3 * g.nz2 * g.nx2) != cudaSuccess) {
+      cudaGetLastError();
+      c->split_x = false;
+    }
     c->use_rhs2 = rhs2_supported(g.ny1) && !getenv("CHANFLOW_RHS_V1");
     c->twx = make_twiddles<T>(g.nx2);
     c->twz = make_twiddles<T>(g.nz2);
@@ -350,17 +365,28 @@ struct Impl {
                                                  c->YB1, 0, g.ny1);
     CKL();
     dim3 g2(g.nz2 / c->ZR, (g.ny - 1 + c->KC - 1) / c->KC);
-    prof_begin(c, "k_xflux");
-    if (c->fast_x) {
+    a.P = c->P;
+    a.FZR = c->flux_zr;
+    if (c->split_x) {
+      prof_begin(c, "k_xinv");
+      if (p1_fast_launch(3, g.nx2, f32, a) != 0) return fail(c, CFG_E_CUDA, "k_xinv_r launch");
+      CKL();
+      prof_begin(c, "k_flux");
+      if (p1_fast_launch(4, g.nx2, f32, a) != 0) return fail(c, CFG_E_CUDA, "k_flux_r launch");
+    } else if (c->fast_x) {
+      prof_begin(c, "k_xflux");
       if (p1_fast_launch(1, g.nx2, f32, a) != 0) return fail(c, CFG_E_CUDA, "k_xflux_r launch");
-    } else if (lin)
+    } else if (lin) {
+      prof_begin(c, "k_xflux");
       k_xflux<T, true><<<g2, 256, c->sm_xflux, c->st>>>((const C*)c->T1, (C*)c->T2, g, c->px, (const C*)c->twx,
                                                          c->gd, (const T*)c->fringe, c->has_fringe, c->ZR, c->KC,
                                                          c->cflbits, do_cfl);
-    else
+    } else {
+      prof_begin(c, "k_xflux");
       k_xflux<T, false><<<g2, 256, c->sm_xflux, c->st>>>((const C*)c->T1, (C*)c->T2, g, c->px, (const C*)c->twx,
                                                           c->gd, (const T*)c->fringe, c->has_fringe, c->ZR, c->KC,
                                                           c->cflbits, do_cfl);
+    }
     CKL();
     dim3 g3(g.nxh, (g.ny1 + c->YB3 - 1) / c->YB3);
     prof_begin(c, "k_zfwd");
@@ -717,7 +743,7 @@ void cfg_destroy(cfg_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->dev);
   if (c->st) cudaStreamSynchronize(c->st);
-  void* bufs[] = {c->dgrid, c->fringe, c->vel, c->cru, c->prs, c->mvel64, c->mcru64, c->T1, c->T2, c->cbc,
+  void* bufs[] = {c->dgrid, c->fringe, c->vel, c->cru, c->prs, c->mvel64, c->mcru64, c->T1, c->T2, c->P, c->cbc,
                   c->sc, c->d_um_dy, c->cflp, c->cflbits, c->l2acc, c->divbits, c->plist, c->pw_H,
                   c->pw_phys, c->pw_phys2, c->pw_in, c->stage, c->twx, c->twz, c->twxs, c->twzs,
                   c->wl_fast, c->wl_prec};

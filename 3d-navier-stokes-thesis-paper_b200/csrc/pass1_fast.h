@@ -22,14 +22,16 @@ struct P1Launch {
   unsigned long long* cflbits;
   int do_cfl;
   int lin;
+  void* P;              // physical planes (split x stage)
+  int FZR;              // z rows per k_flux_r block (2 or 4)
   cudaStream_t st;
 };
 
-// which: 0 k_zinv_r, 1 k_xflux_r, 2 k_zfwd_r.  Returns 0, or -1 when the
-// length is not compiled in, or -2 on a launch error.
+// which: 0 k_zinv_r, 1 k_xflux_r, 2 k_zfwd_r, 3 k_xinv_r, 4 k_flux_r.
+// Returns 0, or -1 when the length is not compiled in, or -2 on a launch error.
 int p1_fast_launch(int which, int n, bool f32, const P1Launch& a);
 // shared memory bytes of kernel `which` at length n with its tile parameter
-// (YB for 0/2, ZR for 1); 0 when unsupported.
+// (YB for 0/2, ZR for 1 and 4, unused for 3); 0 when unsupported.
 size_t p1_fast_smem(int which, int n, bool f32, int param, int nxh);
 
 }  // namespace cfd

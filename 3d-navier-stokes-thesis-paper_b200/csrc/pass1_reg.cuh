@@ -482,12 +482,296 @@ __global__ void __launch_bounds__(256) k_xflux_r(const cplx_t<T>* __restrict__ T
   }
 }
 
+// --------------------------------------------------------------------------
+// Split x stage: k_xinv_r writes the physical planes once, k_flux_r forms the
+// fluxes from three neighbouring physical planes and transforms them forward.
+// Physical planes P[(pl*3 + c)*nz2 + z][x], pl = 0 .. ny (plane pl+1 of the
+// reference's 1-based y index), c = u, v, w.
+
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// row pitch (complex values) of the gathered hybrid rows: 16 bytes of padding
+// keeps the 16-byte cp.async destinations aligned and the stage-1 reads
+// (consecutive threads on consecutive kx) free of bank conflicts
+template <typename T, int ZB> struct RawPitch {
+  static constexpr int V = ZB + 16 / (int)sizeof(cplx_t<T>);
+};
+
+// k_xinv_r: grid (nz2/ZB, 3, ny+1), block 128.  Inverse x transform of ZB
+// hybrid rows (one plane, one component) into physical rows, two real rows per
+// complex FFT (the x part of xz_fft_complex_to_real_parallel,
+// PFC/transform.f90:345-368).  v of plane ny+1 is not formed: no flux reads it.
+template <typename T, int NX2, int ZB>
+__global__ void __launch_bounds__(128) k_xinv_r(const cplx_t<T>* __restrict__ T1, T* __restrict__ P, Geom g,
+                                                const cplx_t<T>* __restrict__ twx) {
+  using C = cplx_t<T>;
+  constexpr int N1 = Split<NX2>::N1, N2 = Split<NX2>::N2, PITCH = N2 + 1, SEQ = SeqPitch<NX2>::V;
+  constexpr int N = NX2, Nh = NX2 / 2, NS = ZB / 2, RP = RawPitch<T, ZB>::V;
+  constexpr int CH = ZB * (int)sizeof(C) / 16;   // 16-byte chunks per hybrid row
+  static_assert(ZB % 2 == 0 && (ZB * sizeof(C)) % 16 == 0, "ZB rows must pack in pairs and 16-byte chunks");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int NXH = g.nxh, NZ2 = g.nz2;
+  C* tw = reinterpret_cast<C*>(smem_raw);   // [N]
+  C* raw = tw + N;                          // [NXH][RP]
+  C* Y = raw + NXH * RP;                    // [NS][SEQ]
+  const int z0 = blockIdx.x * ZB, c = blockIdx.y, pl = blockIdx.z;
+  if (c == 1 && pl == g.ny) return;
+  const C* src = T1 + ((size_t)pl * 3 + c) * NXH * NZ2 + z0;
+  for (int idx = threadIdx.x; idx < NXH * CH; idx += blockDim.x) {
+    const int kx = idx / CH, part = idx - kx * CH;
+    cp_async16(reinterpret_cast<char*>(raw + kx * RP) + part * 16,
+               reinterpret_cast<const char*>(src + (size_t)kx * NZ2) + part * 16);
+  }
+  cp_async_commit();
+  load_tw2<T, N>(tw, twx);
+  cp_async_wait0();
+  __syncthreads();
+  for (int t = threadIdx.x; t < NS * N2; t += blockDim.x) {
+    const int i = t / N2, n2 = t - i * N2;
+    C v[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) {
+      const int k = N2 * n1 + n2;
+      const int kk = (k <= Nh) ? k : N - k;
+      C x1 = czero<C>(), x2 = czero<C>();
+      if (kk < NXH) {
+        x1 = raw[kk * RP + 2 * i];
+        x2 = raw[kk * RP + 2 * i + 1];
+      }
+      C z;
+      if (k == 0 || k == Nh) z = mk<C>(x1.x, x2.x);
+      else if (k < Nh) z = mk<C>(x1.x - x2.y, x1.y + x2.x);
+      else z = mk<C>(x1.x + x2.y, -x1.y + x2.x);
+      v[n1] = z;
+    }
+    SmallFFT<T, N1, +1>::template run<1>(v);
+    C* y = Y + i * SEQ + n2;
+#pragma unroll
+    for (int q = 0; q < N1; ++q) {
+      C x = v[q];
+      if (q != 0) x = cmul(x, cconj(tw[q * N2 + n2]));
+      y[q * PITCH] = x;
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < NS * N1; t += blockDim.x) {
+    const int q = t % N1, i = t / N1;
+    C u[N2];
+    const C* y = Y + i * SEQ + q * PITCH;
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) u[n2] = y[n2];
+    SmallFFT<T, N2, +1>::template run<1>(u);
+    T* w1 = P + (((size_t)pl * 3 + c) * NZ2 + z0 + 2 * i) * N;
+    T* w2 = w1 + N;
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) {
+      w1[q + N1 * k2] = u[k2].x;
+      w2[q + N1 * k2] = u[k2].y;
+    }
+  }
+}
+
+// k_flux_r: grid (nz2/ZR, ny-1), block NT.  Fluxes of plane k = 2 + blockIdx.y
+// on ZR rows of z from the physical planes k-1, k, k+1, then the forward x
+// transform and the Hermitian unpacking into T2 -- the same arithmetic and
+// output as k_xflux_r (PFC/pass1.f90:134-226, PFC/transform.f90:287-315).
+template <typename T, int NX2, int ZR, int NT, bool LIN>
+__global__ void __launch_bounds__(NT) k_flux_r(const T* __restrict__ P, cplx_t<T>* __restrict__ T2, Geom g,
+                                               const cplx_t<T>* __restrict__ twx, GridDev gd,
+                                               const T* __restrict__ fringe, int has_fringe,
+                                               unsigned long long* __restrict__ cflbits, int do_cfl) {
+  using C = cplx_t<T>;
+  constexpr int N1 = Split<NX2>::N1, N2 = Split<NX2>::N2, PITCH = N2 + 1, SEQ = SeqPitch<NX2>::V;
+  constexpr int N = NX2;
+  constexpr int NSEQ = 4 * ZR + (ZR + 1) / 2;
+  constexpr int NW = NT / 32;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);   // tw2[q*N2 + n2]
+  C* FP = tw + N;                           // [NSEQ][SEQ] padded sequences
+  __shared__ T red[3][NW];
+  const int NXH = g.nxh, NZ2 = g.nz2, ny = g.ny;
+  const int z0 = blockIdx.x * ZR;
+  const int k = 2 + blockIdx.y;
+  load_tw2<T, N>(tw, twx);
+  auto px = [](int x) { return (x / N2) * PITCH + (x % N2); };
+  const T half = (T)0.5, two = (T)2.0;
+  const T dhk = (T)gd.dh[k - 1];
+  const bool veq = (k <= ny - 1);
+  const T dnk = veq ? (T)gd.dn[k - 1] : (T)0;
+  const T iu1 = veq ? (T)gd.iu[2 * (k - 1)] : (T)0;
+  const T iu2 = veq ? (T)gd.iu[2 * (k - 1) + 1] : (T)0;
+  const T tu = (T)gd.target[(k - 1)], tv = (T)gd.target[(ny + 1) + (k - 1)];
+  const T tw_ = (T)gd.target[2 * (ny + 1) + (k - 1)];
+  T B0[3] = {0, 0, 0}, Bm[3] = {0, 0, 0}, Bp[3] = {0, 0, 0};
+  if (LIN) {
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      B0[q] = (T)gd.baseflow[q * (ny + 1) + k - 1];
+      Bm[q] = (T)gd.baseflow[q * (ny + 1) + k - 2];
+      Bp[q] = (T)gd.baseflow[q * (ny + 1) + k];
+    }
+  }
+  // rows of planes k-1 (index k-2), k, k+1 for component c and row r
+  const size_t pstride = (size_t)3 * NZ2 * N;
+  const T* Pm = P + (size_t)(k - 2) * pstride + (size_t)z0 * N;
+  const T* P0 = Pm + pstride;
+  const T* Pp = P0 + pstride;
+  const size_t cs = (size_t)NZ2 * N;
+  T ma = 0, mb = 0, mc = 0;
+#pragma unroll 2
+  for (int idx = threadIdx.x; idx < ZR * N; idx += NT) {
+    const int x = idx % N, r = idx / N;
+    const size_t o = (size_t)r * N + x;
+    const T U = __ldg(P0 + o), V = __ldg(P0 + cs + o), W = __ldg(P0 + 2 * cs + o);
+    const T Up = __ldg(Pp + o), Wp = __ldg(Pp + 2 * cs + o);
+    const T Vp = (k < ny) ? __ldg(Pp + cs + o) : V;
+    const T Um = __ldg(Pm + o), Vm = __ldg(Pm + cs + o), Wm = __ldg(Pm + 2 * cs + o);
+    const T fr = has_fringe ? fringe[(size_t)(z0 + r) * N + x] : (T)0;
+    T fpu0, fpw0, fpu, fpw, xfu, zfu, xfw, zfw;
+    if (!LIN) {
+      if (k == 2) { fpu0 = Vm * Um; fpw0 = Vm * Wm; }
+      else { fpu0 = Vm * half * (Um + U); fpw0 = Vm * half * (Wm + W); }
+      if (k < ny) { fpu = V * half * (U + Up); fpw = V * half * (W + Wp); }
+      else { fpu = V * Up; fpw = V * Wp; }
+      xfu = U * U; zfu = W * U; xfw = U * W; zfw = W * W;
+    } else {
+      if (k == 2) { fpu0 = Bm[1] * Um + Vm * Bm[0]; fpw0 = Bm[1] * Wm + Vm * Bm[2]; }
+      else {
+        fpu0 = Bm[1] * half * (Um + U) + Vm * half * (Bm[0] + B0[0]);
+        fpw0 = Bm[1] * half * (Wm + W) + Vm * half * (Bm[2] + B0[2]);
+      }
+      if (k < ny) {
+        fpu = B0[1] * half * (U + Up) + V * half * (B0[0] + Bp[0]);
+        fpw = B0[1] * half * (W + Wp) + V * half * (B0[2] + Bp[2]);
+      } else {
+        fpu = B0[1] * Up + V * Bp[0];
+        fpw = B0[1] * Wp + V * Bp[2];
+      }
+      xfu = two * B0[0] * U; zfu = B0[2] * U + W * B0[0];
+      xfw = B0[2] * U + W * B0[0]; zfw = two * B0[2] * W;
+    }
+    const T dyu = dhk * (fpu - fpu0) + fr * (U - tu);
+    const T dyw = dhk * (fpw - fpw0) + fr * (W - tw_);
+    T xfv = 0, dyv = 0, zfv = 0;
+    if (veq) {
+      T fp0, fp;
+      if (!LIN) {
+        const T t0 = half * (Vm + V), t1 = half * (V + Vp);
+        fp0 = t0 * t0; fp = t1 * t1;
+        xfv = V * (iu1 * U + iu2 * Up);
+        zfv = V * (iu1 * W + iu2 * Wp);
+      } else {
+        const T t0 = half * (Vm + V), b0v = half * (Bm[1] + B0[1]);
+        const T t1 = half * (V + Vp), b1v = half * (B0[1] + Bp[1]);
+        fp0 = two * t0 * b0v; fp = two * t1 * b1v;
+        xfv = B0[1] * (iu1 * U + iu2 * Up) + V * (iu1 * B0[0] + iu2 * Bp[0]);
+        zfv = B0[1] * (iu1 * W + iu2 * Wp) + V * (iu1 * B0[2] + iu2 * Bp[2]);
+      }
+      dyv = dnk * (fp - fp0) + fr * (V - tv);
+    }
+    const int pxx = px(x);
+    FP[(4 * r + 0) * SEQ + pxx] = mk<C>(xfu, dyu);
+    FP[(4 * r + 1) * SEQ + pxx] = mk<C>(xfw, dyw);
+    FP[(4 * r + 2) * SEQ + pxx] = mk<C>(xfv, dyv);
+    FP[(4 * r + 3) * SEQ + pxx] = mk<C>(zfu, zfw);
+    T* p4 = reinterpret_cast<T*>(FP + (4 * ZR + r / 2) * SEQ + pxx);
+    p4[r & 1] = zfv;
+    if ((ZR & 1) && r == ZR - 1) p4[1] = 0;
+    if (do_cfl) {
+      ma = fmax(ma, fabs(U + Up));
+      mb = fmax(mb, fabs(V));
+      mc = fmax(mc, fabs(W + Wp));
+    }
+  }
+  if (do_cfl) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      ma = fmax(ma, __shfl_xor_sync(0xffffffffu, ma, o));
+      mb = fmax(mb, __shfl_xor_sync(0xffffffffu, mb, o));
+      mc = fmax(mc, __shfl_xor_sync(0xffffffffu, mc, o));
+    }
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) { red[0][wid] = ma; red[1][wid] = mb; red[2][wid] = mc; }
+  }
+  __syncthreads();
+  if (do_cfl && threadIdx.x < 3) {
+    T m = 0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) m = fmax(m, red[threadIdx.x][w]);
+    atomicMax(&cflbits[(size_t)(k - 1) * 3 + threadIdx.x], (unsigned long long)__double_as_longlong((double)m));
+  }
+  // forward x FFT of the NSEQ packed sequences, in place
+  for (int t = threadIdx.x; t < NSEQ * N2; t += NT) {
+    const int i = t / N2, n2 = t - i * N2;
+    C v[N1];
+    C* col = FP + i * SEQ + n2;
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) v[n1] = col[n1 * PITCH];
+    SmallFFT<T, N1, -1>::template run<1>(v);
+#pragma unroll
+    for (int q = 0; q < N1; ++q) {
+      C x = v[q];
+      if (q != 0) x = cmul(x, tw[q * N2 + n2]);
+      col[q * PITCH] = x;
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < NSEQ * N1; t += NT) {
+    const int q = t % N1, i = t / N1;
+    C u[N2];
+    C* row = FP + i * SEQ + q * PITCH;
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) u[n2] = row[n2];
+    SmallFFT<T, N2, -1>::template run<1>(u);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) row[k2] = u[k2];
+  }
+  __syncthreads();
+  auto X = [&](int i, int kk) -> C { return FP[i * SEQ + (kk % N1) * PITCH + kk / N1]; };
+  const size_t base = (size_t)(k - 1) * 6;
+  for (int idx = threadIdx.x; idx < NXH * ZR; idx += NT) {
+    const int r = idx % ZR, kx = idx / ZR;
+    const T kxv = (T)gd.kx[kx];
+    const int km = (kx == 0) ? 0 : N - kx;
+#define OUT(e, part) T2[((base + (e) * 2 + (part)) * NXH + kx) * NZ2 + z0 + r]
+#pragma unroll
+    for (int e4 = 0; e4 < 4; ++e4) {
+      if (e4 == 2 && !veq) continue;
+      const C zk = X(4 * r + e4, kx), zm = X(4 * r + e4, km);
+      const C E = mk<C>(half * (zk.x + zm.x), half * (zk.y - zm.y));
+      const C O = mk<C>(half * (zk.y + zm.y), -half * (zk.x - zm.x));
+      if (e4 < 3) {
+        const int e = (e4 == 0) ? 0 : (e4 == 1 ? 2 : 1);
+        OUT(e, 0) = cadd(O, cimul<C>(kxv, E));
+      } else {
+        OUT(0, 1) = E;
+        OUT(2, 1) = O;
+      }
+    }
+    if (veq) {
+      const int i = 4 * ZR + r / 2;
+      const C zk = X(i, kx), zm = X(i, km);
+      C v;
+      if ((r & 1) == 0) v = mk<C>(half * (zk.x + zm.x), half * (zk.y - zm.y));
+      else v = mk<C>(half * (zk.y + zm.y), -half * (zk.x - zm.x));
+      OUT(1, 1) = v;
+    }
+#undef OUT
+  }
+}
+
 // smem sizes (bytes) of the three kernels
 template <typename T, int N> constexpr size_t zinv_r_smem(int YB) {
   return sizeof(cplx_t<T>) * (N + (size_t)3 * YB * SeqPitch<N>::V);
 }
 template <typename T, int N> constexpr size_t zfwd_r_smem(int YB) {
   return sizeof(cplx_t<T>) * (N + (size_t)6 * YB * SeqPitch<N>::V);
+}
+template <typename T, int N, int ZB> constexpr size_t xinv_r_smem(int NXH) {
+  return sizeof(cplx_t<T>) * (N + (size_t)NXH * RawPitch<T, ZB>::V + (size_t)(ZB / 2) * SeqPitch<N>::V);
+}
+template <typename T, int N, int ZR> constexpr size_t flux_r_smem() {
+  return sizeof(cplx_t<T>) * (N + (size_t)(4 * ZR + (ZR + 1) / 2) * SeqPitch<N>::V);
 }
 template <typename T, int N> constexpr size_t xflux_r_smem(int ZR, int NXH) {
   return sizeof(cplx_t<T>) * N + sizeof(T) * 9 * (size_t)ZR * N + sizeof(cplx_t<T>) * (6 * (size_t)ZR * NXH)
