@@ -163,6 +163,7 @@ struct cfg_ctx {
   // register-FFT pass-1 kernels (when the lengths are compiled in)
   bool fast_z = false, fast_x = false;
   bool use_rhs2 = true;
+  int rhs2_lanes = 32;
   int fYB1 = 1, fYB3 = 1, fZR = 1;
   // optional per-launch CUDA-event timing on the context stream
   bool prof_on = false;
@@ -337,6 +338,7 @@ struct Impl {
       c->split_x = false;
     }
     c->use_rhs2 = rhs2_supported(g.ny1) && !getenv("CHANFLOW_RHS_V1");
+    c->rhs2_lanes = (getenv("CHANFLOW_RHS2_LANES") && atoi(getenv("CHANFLOW_RHS2_LANES")) == 16) ? 16 : 32;
     c->twx = make_twiddles<T>(g.nx2);
     c->twz = make_twiddles<T>(g.nz2);
     c->twxs = make_twiddles<T>(g.nx);
@@ -437,7 +439,8 @@ struct Impl {
       a.vel = c->vel; a.cru = c->cru; a.prs = c->prs;
       a.cbc_top = (const C*)c->cbc + 3 * (size_t)g.nw; a.cbc_bot = c->cbc;
       a.g = g; a.gd = c->gd; a.sc = c->sc; a.rkt = c->rkt; a.rk = rk; a.re = c->p.re;
-      a.wlist = c->wl_fast; a.nlist = c->n_fast; a.warps = sizeof(T) == 4 ? 4 : 2; a.st = c->st;
+      a.wlist = c->wl_fast; a.nlist = c->n_fast; a.warps = sizeof(T) == 4 ? 4 : 2; a.lanes = c->rhs2_lanes;
+      a.st = c->st;
       prof_begin(c, "k_rhs");
       if (rhs2_launch(sizeof(T) == 4, a) != 0) return fail(c, CFG_E_CUDA, "k_rhs2 launch");
       CKL();

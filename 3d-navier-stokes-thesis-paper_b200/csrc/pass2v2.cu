@@ -3,12 +3,11 @@
 #include "pass2v2.cuh"
 #include "pass2v2.h"
 
+
 namespace cfd {
 
-template <typename T, int M>
+template <typename T, int M, int G>
 static int launch_m(const Rhs2Launch& a) {
-  // FP32: 16 lanes per wavenumber; FP64: 32 (keeps the FP64 registers in bounds)
-  constexpr int G = sizeof(T) == 4 ? 16 : 32;
   const size_t sm = rhs2_smem<T, M, G>(a.warps);
   static size_t cur = 48 * 1024;
   if (sm > cur) {
@@ -27,42 +26,49 @@ static int launch_m(const Rhs2Launch& a) {
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
+// 32 lanes per wavenumber: M = ceil(ny1/32) <= 8 rows per lane
 template <typename T>
-static int launch_big(const Rhs2Launch& a, int M) {
-  if constexpr (sizeof(T) == 4) {
-    switch (M) {
-      case 9: return launch_m<T, 9>(a);
-      case 10: return launch_m<T, 10>(a);
-      case 11: return launch_m<T, 11>(a);
-      case 12: return launch_m<T, 12>(a);
-      case 13: return launch_m<T, 13>(a);
-      case 14: return launch_m<T, 14>(a);
-      case 15: return launch_m<T, 15>(a);
-      case 16: return launch_m<T, 16>(a);
-      default: return -1;
-    }
-  }
-  return -1;
-}
-
-template <typename T>
-static int launch_t(const Rhs2Launch& a) {
-  const int G = sizeof(T) == 4 ? 16 : 32;
-  const int M = (a.g.ny1 + G - 1) / G;
-  if (sizeof(T) == 8 && M > 8) return -1;
+static int launch_g32(const Rhs2Launch& a) {
+  const int M = (a.g.ny1 + 31) / 32;
   switch (M < 2 ? 2 : M) {
-    case 2: return launch_m<T, 2>(a);
-    case 3: return launch_m<T, 3>(a);
-    case 4: return launch_m<T, 4>(a);
-    case 5: return launch_m<T, 5>(a);
-    case 6: return launch_m<T, 6>(a);
-    case 7: return launch_m<T, 7>(a);
-    case 8: return launch_m<T, 8>(a);
-    default: return sizeof(T) == 4 ? launch_big<T>(a, M) : -1;
+    case 2: return launch_m<T, 2, 32>(a);
+    case 3: return launch_m<T, 3, 32>(a);
+    case 4: return launch_m<T, 4, 32>(a);
+    case 5: return launch_m<T, 5, 32>(a);
+    case 6: return launch_m<T, 6, 32>(a);
+    case 7: return launch_m<T, 7, 32>(a);
+    case 8: return launch_m<T, 8, 32>(a);
+    default: return -1;
   }
 }
 
-int rhs2_launch(bool f32, const Rhs2Launch& a) { return f32 ? launch_t<float>(a) : launch_t<double>(a); }
+// 16 lanes per wavenumber (FP32 only): M = ceil(ny1/16) <= 16
+static int launch_g16(const Rhs2Launch& a) {
+  const int M = (a.g.ny1 + 15) / 16;
+  switch (M < 2 ? 2 : M) {
+    case 2: return launch_m<float, 2, 16>(a);
+    case 3: return launch_m<float, 3, 16>(a);
+    case 4: return launch_m<float, 4, 16>(a);
+    case 5: return launch_m<float, 5, 16>(a);
+    case 6: return launch_m<float, 6, 16>(a);
+    case 7: return launch_m<float, 7, 16>(a);
+    case 8: return launch_m<float, 8, 16>(a);
+    case 9: return launch_m<float, 9, 16>(a);
+    case 10: return launch_m<float, 10, 16>(a);
+    case 11: return launch_m<float, 11, 16>(a);
+    case 12: return launch_m<float, 12, 16>(a);
+    case 13: return launch_m<float, 13, 16>(a);
+    case 14: return launch_m<float, 14, 16>(a);
+    case 15: return launch_m<float, 15, 16>(a);
+    case 16: return launch_m<float, 16, 16>(a);
+    default: return -1;
+  }
+}
+
+int rhs2_launch(bool f32, const Rhs2Launch& a) {
+  if (f32 && a.lanes == 16) return launch_g16(a);
+  return f32 ? launch_g32<float>(a) : launch_g32<double>(a);
+}
 
 bool rhs2_supported(int ny1) { return ny1 <= 256; }
 

@@ -167,7 +167,7 @@ template <int M, int G> struct Ld2 {
 };
 
 template <typename T, int M, int G>
-__global__ void __launch_bounds__(128) k_rhs2(cplx_t<T>* __restrict__ vel, cplx_t<T>* __restrict__ cru,
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 1) k_rhs2(cplx_t<T>* __restrict__ vel, cplx_t<T>* __restrict__ cru,
                                               cplx_t<T>* __restrict__ prs,
                                               const cplx_t<T>* __restrict__ cbc_top,
                                               const cplx_t<T>* __restrict__ cbc_bot, Geom g,

@@ -19,6 +19,7 @@ struct Rhs2Launch {
   const int* wlist;
   int nlist;
   int warps;   // warps per block
+  int lanes;   // lanes per wavenumber: 32, or 16 (FP32 only)
   cudaStream_t st;
 };
 
