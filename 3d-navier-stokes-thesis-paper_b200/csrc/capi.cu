@@ -109,8 +109,8 @@ struct cfg_ctx {
   cudaStream_t st = nullptr;
   // side stream: the small mean-mode and FP64 low-|k| solves run beside the
   // main per-wavenumber kernel; joined back with events
-  cudaStream_t st2 = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaStream_t st2 = nullptr, st3 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join3 = nullptr;
   cudaStream_t prof_stream = nullptr;
   std::string err;
   long long launches = 0;
@@ -135,6 +135,8 @@ struct cfg_ctx {
   unsigned long long* cflbits = nullptr;
   double* l2acc = nullptr;
   unsigned long long* divbits = nullptr;
+  // lane-major grid coefficients of k_rhs2 (storage precision)
+  void* rhs2_tbl = nullptr;
   int* plist = nullptr;
   // plane work buffers
   void *pw_H = nullptr, *pw_phys = nullptr, *pw_phys2 = nullptr, *pw_in = nullptr;
@@ -413,33 +415,38 @@ struct Impl {
   template <int MM>
   static int rhs_m(cfg_ctx* c, int rk, int mode) {
     const Geom& g = c->g;
-    // fork: the mean mode and the FP64 low-|k| list on the side stream
+    // fork: the FP64 low-|k| list and the mean mode on two side streams, one
+    // warp per wavenumber so that they spread over many SMs beside the main
+    // kernel
     CK(cudaEventRecord(c->ev_fork, c->st));
     CK(cudaStreamWaitEvent(c->st2, c->ev_fork, 0));
-    c->prof_stream = c->st2;
+    CK(cudaStreamWaitEvent(c->st3, c->ev_fork, 0));
     if (c->n_prec > 0) {
-      dim3 gr((c->n_prec + 3) / 4);
+      c->prof_stream = c->st2;
       prof_begin(c, "k_rhs_fp64");
-      k_rhs<double, T, MM><<<gr, 128, c->sm_rhs64, c->st2>>>((C*)c->vel, (C*)c->cru, (C*)c->prs,
-                                                             (const C*)c->cbc + 3 * (size_t)g.nw, (const C*)c->cbc, g,
-                                                             c->gd, c->sc, c->rkt, rk, c->p.re, mode, c->wl_prec,
-                                                             c->n_prec);
+      k_rhs<double, T, MM><<<c->n_prec, 32, c->sm_rhs64 / 4, c->st2>>>((C*)c->vel, (C*)c->cru, (C*)c->prs,
+                                                                     (const C*)c->cbc + 3 * (size_t)g.nw,
+                                                                     (const C*)c->cbc, g, c->gd, c->sc, c->rkt, rk,
+                                                                     c->p.re, mode, c->wl_prec, c->n_prec);
       CKL();
     }
     if (mode == 0) c->mean64_valid = true;
+    c->prof_stream = c->st3;
     prof_begin(c, "k_rhs_mean");
-    k_rhs_mean<T, MM><<<1, 32, 0, c->st2>>>((C*)c->vel, (C*)c->cru, (C*)c->prs, c->mvel64, c->mcru64,
+    k_rhs_mean<T, MM><<<1, 32, 0, c->st3>>>((C*)c->vel, (C*)c->cru, (C*)c->prs, c->mvel64, c->mcru64,
                                            (const C*)c->cbc + 3 * (size_t)g.nw, (const C*)c->cbc, g, c->gd, c->sc,
                                            c->d_um_dy, c->rkt, rk, c->p.re, c->p.beta, c->p.fix_mass, mode);
     CKL();
     c->prof_stream = nullptr;
     CK(cudaEventRecord(c->ev_join, c->st2));
+    CK(cudaEventRecord(c->ev_join3, c->st3));
     if (c->n_fast > 0 && mode == 0 && c->use_rhs2) {
       Rhs2Launch a{};
       a.vel = c->vel; a.cru = c->cru; a.prs = c->prs;
       a.cbc_top = (const C*)c->cbc + 3 * (size_t)g.nw; a.cbc_bot = c->cbc;
       a.g = g; a.gd = c->gd; a.sc = c->sc; a.rkt = c->rkt; a.rk = rk; a.re = c->p.re;
       a.wlist = c->wl_fast; a.nlist = c->n_fast; a.warps = sizeof(T) == 4 ? 4 : 2; a.lanes = c->rhs2_lanes;
+      a.tbl = c->rhs2_tbl;
       a.st = c->st;
       prof_begin(c, "k_rhs");
       if (rhs2_launch(sizeof(T) == 4, a) != 0) return fail(c, CFG_E_CUDA, "k_rhs2 launch");
@@ -454,6 +461,7 @@ struct Impl {
     }
     // join
     CK(cudaStreamWaitEvent(c->st, c->ev_join, 0));
+    CK(cudaStreamWaitEvent(c->st, c->ev_join3, 0));
     return CFG_OK;
   }
   static int rhs(cfg_ctx* c, int rk, int mode) {
@@ -608,6 +616,8 @@ int cfg_create(const cfg_params* p, const cfg_grid* gr, cfg_ctx** out) {
   if (cudaSetDevice(c->dev) != cudaSuccess) { fail(c, CFG_E_CUDA, "cudaSetDevice"); delete c; return CFG_E_CUDA; }
   if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->st3, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_join3, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
     delete c;
@@ -737,6 +747,13 @@ int cfg_create(const cfg_params* p, const cfg_grid* gr, cfg_ctx** out) {
     fprintf(stderr, "cfg_create: %s\n", c->err.c_str());
     return bad(r);
   }
+  if (c->use_rhs2) {
+    const size_t tb = rhs2_table_bytes(c->mixed, g.ny1, c->rhs2_lanes);
+    std::vector<unsigned char> ht(tb);
+    rhs2_table(c->mixed, ny, c->rhs2_lanes, gr->dh, gr->dn, gr->d2h, gr->d2n, ht.data());
+    if (cudaMalloc(&c->rhs2_tbl, tb) != cudaSuccess) return bad(CFG_E_NOMEM);
+    cudaMemcpy(c->rhs2_tbl, ht.data(), tb, cudaMemcpyHostToDevice);
+  }
   if (cudaDeviceSynchronize() != cudaSuccess) return bad(CFG_E_CUDA);
   *out = c;
   return CFG_OK;
@@ -746,7 +763,7 @@ void cfg_destroy(cfg_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->dev);
   if (c->st) cudaStreamSynchronize(c->st);
-  void* bufs[] = {c->dgrid, c->fringe, c->vel, c->cru, c->prs, c->mvel64, c->mcru64, c->T1, c->T2, c->P, c->cbc,
+  void* bufs[] = {c->dgrid, c->fringe, c->vel, c->cru, c->prs, c->mvel64, c->mcru64, c->T1, c->T2, c->P, c->rhs2_tbl, c->cbc,
                   c->sc, c->d_um_dy, c->cflp, c->cflbits, c->l2acc, c->divbits, c->plist, c->pw_H,
                   c->pw_phys, c->pw_phys2, c->pw_in, c->stage, c->twx, c->twz, c->twxs, c->twzs,
                   c->wl_fast, c->wl_prec};
@@ -755,7 +772,9 @@ void cfg_destroy(cfg_ctx* c) {
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   if (c->ev_join) cudaEventDestroy(c->ev_join);
+  if (c->ev_join3) cudaEventDestroy(c->ev_join3);
   if (c->st2) cudaStreamDestroy(c->st2);
+  if (c->st3) cudaStreamDestroy(c->st3);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
 }

@@ -3,12 +3,14 @@
 #include "pass2v2.cuh"
 #include "pass2v2.h"
 
+#include <algorithm>
+
 
 namespace cfd {
 
 template <typename T, int M, int G>
 static int launch_m(const Rhs2Launch& a) {
-  const size_t sm = rhs2_smem<T, M, G>(a.warps);
+  const size_t sm = rhs2_smem<T, M, G>(a.warps, a.g.ny1);
   static size_t cur = 48 * 1024;
   if (sm > cur) {
     if (cudaFuncSetAttribute(k_rhs2<T, M, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) {
@@ -22,7 +24,7 @@ static int launch_m(const Rhs2Launch& a) {
   using C = cplx_t<T>;
   k_rhs2<T, M, G><<<gr, 32 * a.warps, sm, a.st>>>((C*)a.vel, (C*)a.cru, (C*)a.prs, (const C*)a.cbc_top,
                                                   (const C*)a.cbc_bot, a.g, a.gd, a.sc, a.rkt, a.rk, a.re, a.wlist,
-                                                  a.nlist);
+                                                  a.nlist, (const T*)a.tbl);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
@@ -71,5 +73,18 @@ int rhs2_launch(bool f32, const Rhs2Launch& a) {
 }
 
 bool rhs2_supported(int ny1) { return ny1 <= 256; }
+
+int rhs2_rows_per_lane(int ny1, int lanes) { return std::max(2, (ny1 + lanes - 1) / lanes); }
+
+size_t rhs2_table_bytes(bool f32, int ny1, int lanes) {
+  return (f32 ? sizeof(float) : sizeof(double)) * (size_t)RC_NUM * rhs2_rows_per_lane(ny1, lanes) * lanes;
+}
+
+void rhs2_table(bool f32, int ny, int lanes, const double* dh, const double* dn, const double* d2h,
+                const double* d2n, void* out) {
+  const int M = rhs2_rows_per_lane(ny + 1, lanes);
+  if (f32) rhs2_fill_table<float>((float*)out, M, lanes, ny, dh, dn, d2h, d2n);
+  else rhs2_fill_table<double>((double*)out, M, lanes, ny, dh, dn, d2h, d2n);
+}
 
 }  // namespace cfd

@@ -150,22 +150,36 @@ __device__ __forceinline__ void tri_group_solve(T (&a)[M], T (&b)[M], T (&c)[M],
   }
 }
 
-// second difference of column s at row j of an n-row system (copied end rows)
-template <typename T>
-__device__ __forceinline__ cplx_t<T> d2c(const cplx_t<T>* s, const double* __restrict__ d, int j, int n) {
+// Grid coefficients of the RK substep in the storage precision, lane-major:
+// tbl[(kind*M + i)*G + g] is coefficient `kind` of row j = g*M + i (0 past the
+// end of its range), so that the G lanes of a group read consecutive words.
+enum Rhs2Coef { RC_D2H = 0, RC_D2N = 3, RC_DN = 6, RC_DH = 7, RC_DNM1 = 8, RC_NUM = 9 };
+
+template <typename T, int M, int G>
+__device__ __forceinline__ T rc(const T* __restrict__ tbl, int kind, int i, int g) {
+  return __ldg(tbl + (kind * M + i) * G + g);
+}
+
+// second difference of column s at row j = g*M + i of an n-row system (end
+// rows copy their neighbours' stencil), coefficients d2[kind0 .. kind0+2]
+template <typename T, int M, int G>
+__device__ __forceinline__ cplx_t<T> d2c_t(const cplx_t<T>* s, const T* __restrict__ tbl, int kind0, int i, int g,
+                                           int j, int n) {
   using C = cplx_t<T>;
   const int j0 = (j == 0) ? 1 : ((j == n - 1) ? n - 2 : j);
-  const T d1 = (T)__ldg(d + 3 * j), d2 = (T)__ldg(d + 3 * j + 1), d3 = (T)__ldg(d + 3 * j + 2);
+  const T d1 = rc<T, M, G>(tbl, kind0, i, g), d2 = rc<T, M, G>(tbl, kind0 + 1, i, g),
+          d3 = rc<T, M, G>(tbl, kind0 + 2, i, g);
   const C fm = s[j0 - 1], f0 = s[j0], fp = s[j0 + 1];
   return mk<C>(d1 * fm.x + d2 * f0.x + d3 * fp.x, d1 * fm.y + d2 * f0.y + d3 * fp.y);
 }
 
-// column stride (complex elements) of the staged columns: >= G*M rows, even
-// (16-byte aligned for FP32 complex)
-template <int M, int G> struct Ld2 {
-  static constexpr int V = ((G * M + 1) / 2) * 2;
-};
+// column stride (complex elements) of the staged columns: ny+1 rounded up to
+// even (16-byte aligned columns for FP32 complex)
+__host__ __device__ __forceinline__ int rhs2_ld(int n1) { return (n1 + 1) & ~1; }
 
+// Shared memory per wavenumber: eight columns
+//   0-2 cru (u,v,w), overwritten by the new velocity cv;  3 pressure;
+//   4 pressure correction;  5-7 nonlinear term, overwritten by the next cru.
 template <typename T, int M, int G>
 __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 1) k_rhs2(cplx_t<T>* __restrict__ vel, cplx_t<T>* __restrict__ cru,
                                               cplx_t<T>* __restrict__ prs,
@@ -173,9 +187,8 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 1) k_rhs2(cplx_t<T>*
                                               const cplx_t<T>* __restrict__ cbc_bot, Geom g,
                                               GridDev gd, const DevScalars* __restrict__ sc, RkTab rkt,
                                               int rk, double re, const int* __restrict__ wlist,
-                                              int nlist) {
+                                              int nlist, const T* __restrict__ tbl) {
   using C = cplx_t<T>;
-  constexpr int LD = Ld2<M, G>::V;
   constexpr int GPW = 32 / G;                 // lane groups (wavenumbers) per warp
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -184,39 +197,34 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 1) k_rhs2(cplx_t<T>*
   const bool valid = widx < nlist;
   const int w = valid ? wlist[widx] : 1;
   const int NZ = g.nz, ny = g.ny, n1 = g.ny1;
+  const int LD = rhs2_ld(n1);
   const size_t nw = (size_t)g.nw;
   const int kxi = w / NZ, kzi = w % NZ;
   const T kx = (T)gd.kx[kxi], kz = (T)gd.kz[kzi];
   const T k2 = valid ? (T)(gd.kx[kxi] * gd.kx[kxi] + gd.kz[kzi] * gd.kz[kzi]) : (T)1;
-  C* S = reinterpret_cast<C*>(smem_raw) + (size_t)(warp * GPW + grp) * 5 * LD;
+  C* S = reinterpret_cast<C*>(smem_raw) + (size_t)(warp * GPW + grp) * 8 * LD;
   C* sV = S;             // 3 columns: cru, then the new velocity cv
   C* sP = S + 3 * LD;    // pressure
   C* sH = S + 4 * LD;    // pressure correction
+  C* sN = S + 5 * LD;    // 3 columns: nonlinear term, then the next cru
   C* gvel = vel + (size_t)w * 3 * n1;
   C* gcru = cru + (size_t)w * 3 * n1;
   C* gprs = prs + (size_t)w * n1;
 
-  // ---- asynchronous staging of the four input columns cru (u,v,w) and p;
-  // the nonlinear term is read at each lane's own rows, where it is used
+  // ---- asynchronous staging of the seven input columns: cru (u,v,w), p, NL (u,v,w)
   if (valid) {
     const int cb = (int)(n1 * sizeof(C));
-    if ((cb % 16) == 0) {
-      const int nch = cb / 16;
-      for (int idx = gl; idx < 4 * nch; idx += G) {
-        const int col = idx / nch, part = idx - col * nch;
-        const C* src = (col < 3) ? gcru + col * n1 : gprs;
-        cp_async16(reinterpret_cast<char*>(S + col * LD) + part * 16, reinterpret_cast<const char*>(src) + part * 16);
-      }
-    } else {
-      const int nch = cb / 8;
-      for (int idx = gl; idx < 4 * nch; idx += G) {
-        const int col = idx / nch, part = idx - col * nch;
-        const C* src = (col < 3) ? gcru + col * n1 : gprs;
-        cp_async8(reinterpret_cast<char*>(S + col * LD) + part * 8, reinterpret_cast<const char*>(src) + part * 8);
-      }
+    const bool v16 = (cb % 16) == 0;
+    const int csz = v16 ? 16 : 8, nch = cb / csz;
+    for (int idx = gl; idx < 7 * nch; idx += G) {
+      const int col = idx / nch, part = idx - col * nch;
+      const C* src = (col < 3) ? gcru + col * n1 : (col == 3 ? gprs : gvel + (col - 4) * n1);
+      char* dst = reinterpret_cast<char*>(S + (col < 4 ? col : col + 1) * LD) + part * csz;
+      if (v16) cp_async16(dst, reinterpret_cast<const char*>(src) + part * csz);
+      else cp_async8(dst, reinterpret_cast<const char*>(src) + part * csz);
     }
   } else {
-    for (int idx = gl; idx < 5 * LD; idx += G) S[idx] = czero<C>();
+    for (int idx = gl; idx < 8 * LD; idx += G) S[idx] = czero<C>();
   }
   cp_async_commit();
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
@@ -233,7 +241,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 1) k_rhs2(cplx_t<T>*
     C r[3][M];
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
-      const double* d2 = (q == 1) ? gd.d2n : gd.d2h;
+      const int kd = (q == 1) ? RC_D2N : RC_D2H;
       const int nq = (q == 1) ? ny : n1;
 #pragma unroll
       for (int i = 0; i < M; ++i) {
@@ -241,18 +249,19 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 1) k_rhs2(cplx_t<T>*
         C v = czero<C>();
         if (j < n1) {
           const C cr = sV[q * LD + j];
-          const C nl = valid ? gvel[q * n1 + j] : czero<C>();
+          const C nl = sN[q * LD + j];
           v = mk<C>(cr.x - coef * nl.x, cr.y - coef * nl.y);
           if (rk == 1) {
             if (j < nq) {
-              const C du = d2c<T>(sV + q * LD, d2, j, nq);
+              const C du = d2c_t<T, M, G>(sV + q * LD, tbl, kd, i, gl, j, nq);
               v = cadd(v, cscale(vis_exp, csub(du, cscale(k2, cr))));
             }
             if (j >= 1 && j <= ny - 1) {
               const C p = sP[j];
               if (q == 0) v = csub(v, cimul<C>(rk_press * kx, p));
               else if (q == 2) v = csub(v, cimul<C>(rk_press * kz, p));
-              else if (j <= ny - 2) v = csub(v, cscale(rk_press * (T)gd.dn[j], csub(sP[j + 1], p)));
+              else if (j <= ny - 2)
+                v = csub(v, cscale(rk_press * rc<T, M, G>(tbl, RC_DN, i, gl), csub(sP[j + 1], p)));
             }
           }
         }
@@ -274,9 +283,9 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 1) k_rhs2(cplx_t<T>*
           a[i] = 0; b[i] = 1; c[i] = 0;
           f[0][i] = cbc_top[w]; f[1][i] = cbc_top[2 * nw + w];
         } else if (j < n1 - 1) {
-          a[i] = -vis_imp * (T)__ldg(gd.d2h + 3 * j);
-          b[i] = -vis_imp * (T)__ldg(gd.d2h + 3 * j + 1) + alpha;
-          c[i] = -vis_imp * (T)__ldg(gd.d2h + 3 * j + 2);
+          a[i] = -vis_imp * rc<T, M, G>(tbl, RC_D2H, i, gl);
+          b[i] = -vis_imp * rc<T, M, G>(tbl, RC_D2H + 1, i, gl) + alpha;
+          c[i] = -vis_imp * rc<T, M, G>(tbl, RC_D2H + 2, i, gl);
           f[0][i] = r[0][i]; f[1][i] = r[2][i];
         } else {
           a[i] = 0; b[i] = 1; c[i] = 0;
@@ -299,9 +308,9 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 1) k_rhs2(cplx_t<T>*
         if (j == 0) { a[i] = 0; b[i] = 1; c[i] = 0; f[0][i] = cbc_bot[nw + w]; }
         else if (j == ny - 1) { a[i] = 0; b[i] = 1; c[i] = 0; f[0][i] = cbc_top[nw + w]; }
         else if (j < ny - 1) {
-          a[i] = -vis_imp * (T)__ldg(gd.d2n + 3 * j);
-          b[i] = -vis_imp * (T)__ldg(gd.d2n + 3 * j + 1) + alpha;
-          c[i] = -vis_imp * (T)__ldg(gd.d2n + 3 * j + 2);
+          a[i] = -vis_imp * rc<T, M, G>(tbl, RC_D2N, i, gl);
+          b[i] = -vis_imp * rc<T, M, G>(tbl, RC_D2N + 1, i, gl) + alpha;
+          c[i] = -vis_imp * rc<T, M, G>(tbl, RC_D2N + 2, i, gl);
           f[0][i] = r[1][i];
         } else { a[i] = 0; b[i] = 1; c[i] = 0; f[0][i] = czero<C>(); }
       }
@@ -323,13 +332,14 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 1) k_rhs2(cplx_t<T>*
     for (int i = 0; i < M; ++i) {
       const int j = gl * M + i;
       if (j == 0) {
-        const T dn0 = (T)gd.dn[0];
+        const T dn0 = rc<T, M, G>(tbl, RC_DN, i, gl);
         a[i] = 0; b[i] = -dn0; c[i] = dn0; f[0][i] = czero<C>();
       } else if (j == n1 - 1) {
-        const T dnl = (T)gd.dn[ny - 1];
+        const T dnl = rc<T, M, G>(tbl, RC_DNM1, i, gl);
         a[i] = -dnl; b[i] = dnl; c[i] = 0; f[0][i] = czero<C>();
       } else if (j < n1 - 1) {
-        const T dh = (T)gd.dh[j], dm1 = (T)gd.dn[j - 1], dn0 = (T)gd.dn[j];
+        const T dh = rc<T, M, G>(tbl, RC_DH, i, gl), dm1 = rc<T, M, G>(tbl, RC_DNM1, i, gl),
+                dn0 = rc<T, M, G>(tbl, RC_DN, i, gl);
         a[i] = dh * dm1;
         b[i] = -(dh * dm1) - dh * dn0 - k2;
         c[i] = dh * dn0;
@@ -364,9 +374,10 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 1) k_rhs2(cplx_t<T>*
         if (j >= 1 && j <= ny - 1) {
           sV[j] = csub(sV[j], cimul<C>(rk_press * kx, ch));
           sV[2 * LD + j] = csub(sV[2 * LD + j], cimul<C>(rk_press * kz, ch));
-          if (j <= ny - 2) sV[LD + j] = csub(sV[LD + j], cscale(rk_press * (T)gd.dn[j], csub(sH[j + 1], ch)));
+          if (j <= ny - 2)
+            sV[LD + j] = csub(sV[LD + j], cscale(rk_press * rc<T, M, G>(tbl, RC_DN, i, gl), csub(sH[j + 1], ch)));
         }
-        const C d2c_ = d2c<T>(sH, gd.d2h, j, n1);
+        const C d2c_ = d2c_t<T, M, G>(sH, tbl, RC_D2H, i, gl, j, n1);
         const C p = sP[j];
         pn[i] = mk<C>(p.x + alpha * ch.x - vis_imp * d2c_.x, p.y + alpha * ch.y - vis_imp * d2c_.y);
       }
@@ -378,53 +389,72 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 1) k_rhs2(cplx_t<T>*
     }
     __syncwarp();
   }
-  // ---- stage D: next-substep accumulator (PFC/pass2.f90:312-333), stored
-  // from each lane's own rows; then data1 <- cv and data4 <- p, coalesced
-  if (valid) {
-    if (rk < 3) {
-      const T coef2 = (T)(dt * rkt.A(rk + 1));
-      const T vis_exp2 = (T)((dt / re) * rkt.Cc(rk + 1));
-      const T rkp2 = (T)((rkt.Cc(rk + 1) + rkt.D(rk + 1)) * dt);
+  // ---- stage D: next-substep accumulator (PFC/pass2.f90:312-333) at each
+  // lane's own rows into the nonlinear-term columns; then data1 <- cv,
+  // data2 <- accumulator and data4 <- p, coalesced
+  if (rk < 3) {
+    const T coef2 = (T)(dt * rkt.A(rk + 1));
+    const T vis_exp2 = (T)((dt / re) * rkt.Cc(rk + 1));
+    const T rkp2 = (T)((rkt.Cc(rk + 1) + rkt.D(rk + 1)) * dt);
 #pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        const double* d2 = (q == 1) ? gd.d2n : gd.d2h;
-        const int nq = (q == 1) ? ny : n1;
+    for (int q = 0; q < 3; ++q) {
+      const int kd = (q == 1) ? RC_D2N : RC_D2H;
+      const int nq = (q == 1) ? ny : n1;
 #pragma unroll
-        for (int i = 0; i < M; ++i) {
-          const int j = gl * M + i;
-          if (j >= n1) continue;
-          const C cv = sV[q * LD + j];
-          const C nl = gvel[q * n1 + j];
-          C v = mk<C>(cv.x - coef2 * nl.x, cv.y - coef2 * nl.y);
-          if (j < nq) {
-            const C du = d2c<T>(sV + q * LD, d2, j, nq);
-            v = cadd(v, cscale(vis_exp2, csub(du, cscale(k2, cv))));
-          }
-          if (j >= 1 && j <= ny - 1) {
-            const C p = sP[j];
-            if (q == 0) v = csub(v, cimul<C>(rkp2 * kx, p));
-            else if (q == 2) v = csub(v, cimul<C>(rkp2 * kz, p));
-            else if (j <= ny - 2) v = csub(v, cscale(rkp2 * (T)gd.dn[j], csub(sP[j + 1], p)));
-          }
-          gcru[q * n1 + j] = v;
+      for (int i = 0; i < M; ++i) {
+        const int j = gl * M + i;
+        if (j >= n1) continue;
+        const C cv = sV[q * LD + j];
+        const C nl = sN[q * LD + j];
+        C v = mk<C>(cv.x - coef2 * nl.x, cv.y - coef2 * nl.y);
+        if (j < nq) {
+          const C du = d2c_t<T, M, G>(sV + q * LD, tbl, kd, i, gl, j, nq);
+          v = cadd(v, cscale(vis_exp2, csub(du, cscale(k2, cv))));
         }
+        if (j >= 1 && j <= ny - 1) {
+          const C p = sP[j];
+          if (q == 0) v = csub(v, cimul<C>(rkp2 * kx, p));
+          else if (q == 2) v = csub(v, cimul<C>(rkp2 * kz, p));
+          else if (j <= ny - 2) v = csub(v, cscale(rkp2 * rc<T, M, G>(tbl, RC_DN, i, gl), csub(sP[j + 1], p)));
+        }
+        sN[q * LD + j] = v;
       }
-    } else {
-      for (int q = 0; q < 3; ++q)
-        for (int j = gl; j < n1; j += G) gcru[q * n1 + j] = sV[q * LD + j];
     }
   }
   __syncwarp();
   if (valid) {
+    const C* acc = (rk < 3) ? sN : sV;
     for (int q = 0; q < 3; ++q)
-      for (int j = gl; j < n1; j += G) gvel[q * n1 + j] = sV[q * LD + j];
+      for (int j = gl; j < n1; j += G) {
+        gvel[q * n1 + j] = sV[q * LD + j];
+        gcru[q * n1 + j] = acc[q * LD + j];
+      }
     for (int j = gl; j < n1; j += G) gprs[j] = sP[j];
   }
 }
 
 template <typename T, int M, int G>
-constexpr size_t rhs2_smem(int warps) {
-  return sizeof(cplx_t<T>) * (size_t)warps * (32 / G) * 5 * Ld2<M, G>::V;
+size_t rhs2_smem(int warps, int n1) {
+  return sizeof(cplx_t<T>) * (size_t)warps * (32 / G) * 8 * rhs2_ld(n1);
+}
+
+// host: fills the lane-major coefficient table (RC_NUM*M*G values of T)
+template <typename T>
+void rhs2_fill_table(T* out, int M, int G, int ny, const double* dh, const double* dn, const double* d2h,
+                     const double* d2n) {
+  const int n1 = ny + 1;
+  for (int kind = 0; kind < RC_NUM; ++kind)
+    for (int i = 0; i < M; ++i)
+      for (int gg = 0; gg < G; ++gg) {
+        const int j = gg * M + i;
+        double v = 0.0;
+        if (kind < 3) v = (j < n1) ? d2h[3 * j + kind] : 0.0;
+        else if (kind < 6) v = (j < ny) ? d2n[3 * j + kind - 3] : 0.0;
+        else if (kind == RC_DN) v = (j < ny) ? dn[j] : 0.0;
+        else if (kind == RC_DH) v = (j < n1) ? dh[j] : 0.0;
+        else v = (j >= 1 && j - 1 < ny) ? dn[j - 1] : 0.0;
+        out[(kind * M + i) * G + gg] = (T)v;
+      }
 }
 
 }  // namespace cfd
