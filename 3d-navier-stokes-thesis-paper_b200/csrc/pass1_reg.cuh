@@ -576,14 +576,17 @@ __global__ void __launch_bounds__(128) k_xinv_r(const cplx_t<T>* __restrict__ T1
 // transform and the Hermitian unpacking into T2 -- the same arithmetic and
 // output as k_xflux_r (PFC/pass1.f90:134-226, PFC/transform.f90:287-315).
 template <typename T, int NX2, int ZR, int NT, bool LIN>
-__global__ void __launch_bounds__(NT) k_flux_r(const T* __restrict__ P, cplx_t<T>* __restrict__ T2, Geom g,
+__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT == 256 ? 1 : 2)) k_flux_r(const T* __restrict__ P, cplx_t<T>* __restrict__ T2, Geom g,
                                                const cplx_t<T>* __restrict__ twx, GridDev gd,
                                                const T* __restrict__ fringe, int has_fringe,
                                                unsigned long long* __restrict__ cflbits, int do_cfl) {
   using C = cplx_t<T>;
   constexpr int N1 = Split<NX2>::N1, N2 = Split<NX2>::N2, PITCH = N2 + 1, SEQ = SeqPitch<NX2>::V;
   constexpr int N = NX2;
-  constexpr int NSEQ = 4 * ZR + (ZR + 1) / 2;
+  // four packed sequences per row: (xfu,dyu) (xfw,dyw) (xfv,dyv) (zfw,zfv);
+  // zfu = w*u equals xfw = u*w (and likewise in the linearized products), so
+  // its transform is taken from the second sequence
+  constexpr int NSEQ = 4 * ZR;
   constexpr int NW = NT / 32;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tw = reinterpret_cast<C*>(smem_raw);   // tw2[q*N2 + n2]
@@ -618,8 +621,11 @@ __global__ void __launch_bounds__(NT) k_flux_r(const T* __restrict__ P, cplx_t<T
   const T* Pp = P0 + pstride;
   const size_t cs = (size_t)NZ2 * N;
   T ma = 0, mb = 0, mc = 0;
-#pragma unroll 2
-  for (int idx = threadIdx.x; idx < ZR * N; idx += NT) {
+  constexpr int IT = (ZR * N + NT - 1) / NT;
+#pragma unroll
+  for (int it = 0; it < IT; ++it) {
+    const int idx = it * NT + (int)threadIdx.x;
+    if ((ZR * N) % NT != 0 && idx >= ZR * N) break;
     const int x = idx % N, r = idx / N;
     const size_t o = (size_t)r * N + x;
     const T U = __ldg(P0 + o), V = __ldg(P0 + cs + o), W = __ldg(P0 + 2 * cs + o);
@@ -670,13 +676,11 @@ __global__ void __launch_bounds__(NT) k_flux_r(const T* __restrict__ P, cplx_t<T
       dyv = dnk * (fp - fp0) + fr * (V - tv);
     }
     const int pxx = px(x);
+    (void)zfu;
     FP[(4 * r + 0) * SEQ + pxx] = mk<C>(xfu, dyu);
     FP[(4 * r + 1) * SEQ + pxx] = mk<C>(xfw, dyw);
     FP[(4 * r + 2) * SEQ + pxx] = mk<C>(xfv, dyv);
-    FP[(4 * r + 3) * SEQ + pxx] = mk<C>(zfu, zfw);
-    T* p4 = reinterpret_cast<T*>(FP + (4 * ZR + r / 2) * SEQ + pxx);
-    p4[r & 1] = zfv;
-    if ((ZR & 1) && r == ZR - 1) p4[1] = 0;
+    FP[(4 * r + 3) * SEQ + pxx] = mk<C>(zfw, zfv);
     if (do_cfl) {
       ma = fmax(ma, fabs(U + Up));
       mb = fmax(mb, fabs(V));
@@ -743,18 +747,11 @@ __global__ void __launch_bounds__(NT) k_flux_r(const T* __restrict__ P, cplx_t<T
       if (e4 < 3) {
         const int e = (e4 == 0) ? 0 : (e4 == 1 ? 2 : 1);
         OUT(e, 0) = cadd(O, cimul<C>(kxv, E));
+        if (e4 == 1) OUT(0, 1) = E;
       } else {
-        OUT(0, 1) = E;
-        OUT(2, 1) = O;
+        OUT(2, 1) = E;
+        if (veq) OUT(1, 1) = O;
       }
-    }
-    if (veq) {
-      const int i = 4 * ZR + r / 2;
-      const C zk = X(i, kx), zm = X(i, km);
-      C v;
-      if ((r & 1) == 0) v = mk<C>(half * (zk.x + zm.x), half * (zk.y - zm.y));
-      else v = mk<C>(half * (zk.y + zm.y), -half * (zk.x - zm.x));
-      OUT(1, 1) = v;
     }
 #undef OUT
   }
@@ -771,7 +768,7 @@ template <typename T, int N, int ZB> constexpr size_t xinv_r_smem(int NXH) {
   return sizeof(cplx_t<T>) * (N + (size_t)NXH * RawPitch<T, ZB>::V + (size_t)(ZB / 2) * SeqPitch<N>::V);
 }
 template <typename T, int N, int ZR> constexpr size_t flux_r_smem() {
-  return sizeof(cplx_t<T>) * (N + (size_t)(4 * ZR + (ZR + 1) / 2) * SeqPitch<N>::V);
+  return sizeof(cplx_t<T>) * (N + (size_t)(4 * ZR) * SeqPitch<N>::V);
 }
 template <typename T, int N> constexpr size_t xflux_r_smem(int ZR, int NXH) {
   return sizeof(cplx_t<T>) * N + sizeof(T) * 9 * (size_t)ZR * N + sizeof(cplx_t<T>) * (6 * (size_t)ZR * NXH)
