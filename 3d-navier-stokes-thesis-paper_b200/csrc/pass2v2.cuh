@@ -15,6 +15,12 @@
 
 namespace cfd {
 
+// Reciprocal used by the solves: the approximate single-precision divide
+// intrinsic (2 ulp) in FP32, an IEEE divide in FP64.
+template <typename T> __device__ __forceinline__ T rcpv(T x);
+template <> __device__ __forceinline__ float rcpv<float>(float x) { return __fdividef(1.0f, x); }
+template <> __device__ __forceinline__ double rcpv<double>(double x) { return 1.0 / x; }
+
 // One strided PCR step (stride 2t in interface rows = t lanes) of one slot.
 template <typename T, int G, int NR>
 __device__ __forceinline__ void pcr_step(T& A, T& B, T& Cc, cplx_t<T> (&Fv)[NR], int t, int g) {
@@ -39,7 +45,7 @@ __device__ __forceinline__ void pcr_step(T& A, T& B, T& Cc, cplx_t<T> (&Fv)[NR],
 #pragma unroll
     for (int r = 0; r < NR; ++r) uf[r] = czero<C>();
   }
-  const T k1 = A * ((T)1 / lb), k2 = Cc * ((T)1 / ub);
+  const T k1 = A * rcpv(lb), k2 = Cc * rcpv(ub);
   const T nB = B - k1 * lc - k2 * ua;
 #pragma unroll
   for (int r = 0; r < NR; ++r)
@@ -60,17 +66,17 @@ __device__ __forceinline__ void tri_group_solve(T (&a)[M], T (&b)[M], T (&c)[M],
   T ap[M], cq[M], rb[M];
   ap[0] = 0;
   ap[1] = a[1];
-  rb[0] = (T)1 / b[0];
+  rb[0] = rcpv(b[0]);
+  rb[1] = rcpv(b[1]);
 #pragma unroll
   for (int i = 2; i < M; ++i) {
-    const T rr = a[i] * ((T)1 / b[i - 1]);
+    const T rr = a[i] * rb[i - 1];
     ap[i] = -rr * ap[i - 1];
     b[i] = b[i] - rr * c[i - 1];
+    rb[i] = rcpv(b[i]);
 #pragma unroll
     for (int r = 0; r < NR; ++r) f[r][i] = mk<C>(f[r][i].x - rr * f[r][i - 1].x, f[r][i].y - rr * f[r][i - 1].y);
   }
-#pragma unroll
-  for (int i = 1; i < M; ++i) rb[i] = (T)1 / b[i];
 #pragma unroll
   for (int i = 0; i < M; ++i) cq[i] = 0;
   if (M > 2) cq[M - 2] = c[M - 2];
@@ -118,8 +124,9 @@ __device__ __forceinline__ void tri_group_solve(T (&a)[M], T (&b)[M], T (&c)[M],
 #pragma unroll
       for (int r = 0; r < NR; ++r) uf[r] = czero<C>();
     }
-    const T k1a = A0 * ((T)1 / lb), k2a = C0 * ((T)1 / B1);
-    const T k1b = A1 * ((T)1 / B0), k2b = C1 * ((T)1 / ub);
+    const T rB0 = rcpv(B0), rB1 = rcpv(B1);
+    const T k1a = A0 * rcpv(lb), k2a = C0 * rB1;
+    const T k1b = A1 * rB0, k2b = C1 * rcpv(ub);
     const T nA0 = -k1a * la, nC0 = -k2a * C1, nB0 = B0 - k1a * lc - k2a * A1;
     const T nA1 = -k1b * A0, nC1 = -k2b * uc, nB1 = B1 - k1b * C0 - k2b * ua;
 #pragma unroll
@@ -137,7 +144,7 @@ __device__ __forceinline__ void tri_group_solve(T (&a)[M], T (&b)[M], T (&c)[M],
     pcr_step<T, G, NR>(A0, B0, C0, F0, t, g);
     pcr_step<T, G, NR>(A1, B1, C1, F1, t, g);
   }
-  const T r0 = (T)1 / B0, r1 = (T)1 / B1;
+  const T r0 = rcpv(B0), r1 = rcpv(B1);
 #pragma unroll
   for (int r = 0; r < NR; ++r) {
     const C x0 = mk<C>(F0[r].x * r0, F0[r].y * r0);
@@ -216,12 +223,14 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 1) k_rhs2(cplx_t<T>*
     const int cb = (int)(n1 * sizeof(C));
     const bool v16 = (cb % 16) == 0;
     const int csz = v16 ? 16 : 8, nch = cb / csz;
-    for (int idx = gl; idx < 7 * nch; idx += G) {
-      const int col = idx / nch, part = idx - col * nch;
-      const C* src = (col < 3) ? gcru + col * n1 : (col == 3 ? gprs : gvel + (col - 4) * n1);
-      char* dst = reinterpret_cast<char*>(S + (col < 4 ? col : col + 1) * LD) + part * csz;
-      if (v16) cp_async16(dst, reinterpret_cast<const char*>(src) + part * csz);
-      else cp_async8(dst, reinterpret_cast<const char*>(src) + part * csz);
+#pragma unroll
+    for (int col = 0; col < 7; ++col) {
+      const char* src = reinterpret_cast<const char*>((col < 3) ? gcru + col * n1 : (col == 3 ? gprs : gvel + (col - 4) * n1));
+      char* dst = reinterpret_cast<char*>(S + (col < 4 ? col : col + 1) * LD);
+      for (int part = gl; part < nch; part += G) {
+        if (v16) cp_async16(dst + part * 16, src + part * 16);
+        else cp_async8(dst + part * 8, src + part * 8);
+      }
     }
   } else {
     for (int idx = gl; idx < 8 * LD; idx += G) S[idx] = czero<C>();
