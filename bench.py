@@ -306,7 +306,11 @@ def run_ours(args):
             "k_zfwd": t2 + 3 * nf * sc, "k_xflux": t1 + t2,
             "k_rhs": 14 * nf * sc,   # all wavenumbers (the ~50 FP64 ones run beside it)
         }
-        prof = mix["prof"] or {}
+        prof = dict(mix["prof"] or {})
+        if "k_zfwd_low" in prof and "k_zfwd" in prof:
+            # the z transform runs as two launches (low kx columns first)
+            lo, hi = prof.pop("k_zfwd_low"), prof["k_zfwd"]
+            prof["k_zfwd"] = (hi[0], hi[1] + lo[1])
         kp = mix["prof_steps"]
         tot_prof = sum(v[1] for k, v in prof.items() if k not in ("k_rhs_fp64", "k_rhs_mean")) or 1.0
         kernels = {}
