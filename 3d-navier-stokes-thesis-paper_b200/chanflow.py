@@ -54,6 +54,22 @@ class CfgGrid(C.Structure):
                                    "dy", "kx", "kz", "buffer", "target_inflow")]
 
 
+class CfgJet(C.Structure):
+    """cfg_jet (include/chanflow.h): index 0 of each pair is the bottom wall."""
+    _fields_ = [
+        ("mode", C.c_int),
+        ("xjet", C.c_double * 2), ("zjet", C.c_double * 2),
+        ("jetmag", C.c_double * 2), ("forcing", C.c_double * 2), ("for_freq", C.c_double * 2),
+        ("jet_diam", C.c_double),
+        ("width", C.c_double), ("freq", C.c_double),
+        ("frac_xbuff", C.c_double),
+        ("filter_jet_profile", C.c_int),
+        ("jet_forcing", C.c_double * 24),
+        ("jet_forcing_incr", C.c_double * 24),
+        ("seed", C.c_ulonglong),
+    ]
+
+
 class CfhRun(C.Structure):
     _fields_ = [
         ("re", C.c_double), ("ctrlu", C.c_double), ("ctrlw", C.c_double), ("lx", C.c_double),
@@ -104,6 +120,10 @@ SYMBOLS = {
     "cfg_small_r2c": (C.c_int, [_VP, _VP, _VP, C.c_int]),
     "cfg_small_c2r": (C.c_int, [_VP, _VP, _VP, C.c_int]),
     "cfg_l2_norm": (C.c_int, [_VP, _DP, _DP]),
+    "cfg_arnoldi_matvec": (C.c_int, [_VP, C.c_int, _VP, _VP]),
+    "cfg_set_jet": (C.c_int, [_VP, C.POINTER(CfgJet)]),
+    "cfg_jet_profile": (C.c_int, [_VP, C.c_double, C.c_double]),
+    "cfg_get_jet_forcing": (C.c_int, [_VP, _VP, _VP]),
     "cfg_remove_initial_divergence": (C.c_int, [_VP]),
     "cfg_compute_initial_pressure": (C.c_int, [_VP, C.c_int]),
     "cfg_diagnostics": (C.c_int, [_VP, _DP, _DP]),
@@ -331,6 +351,45 @@ class ChannelFlow:
         self._chk(self.L.cfg_xz_r2c(self.h, _p(d), _p(out)))
         return out
 
+    def small_fft_real_to_complex(self, data):
+        """small_fft_real_to_complex (PFC/transform.f90:950-1142): data
+        (nx, nz[, nplanes]) real -> (nz, nx/2+1[, nplanes]) complex, 1/(nx nz)."""
+        d = np.asfortranarray(data, dtype=np.float64)
+        npl = 1 if d.ndim == 2 else d.shape[2]
+        out = np.zeros((self.nz, self.nxh, npl), np.complex128, order="F")
+        self._chk(self.L.cfg_small_r2c(self.h, _p(d), _p(out), npl))
+        return out[:, :, 0] if d.ndim == 2 else out
+
+    def small_fft_complex_to_real(self, cdata):
+        cd = np.asfortranarray(cdata, dtype=np.complex128)
+        npl = 1 if cd.ndim == 2 else cd.shape[2]
+        out = np.zeros((self.nx, self.nz, npl), order="F")
+        self._chk(self.L.cfg_small_c2r(self.h, _p(cd), _p(out), npl))
+        return out[:, :, 0] if cd.ndim == 2 else out
+
+    def arnoldi_matvec(self, v, tend):
+        """compute_time_deriv (PFC/arnoldi.f90:485-567): w = Phi_T v for a
+        real vector of shape (nx, nz, ny+1, 3) (or its flat Fortran-order
+        ravel).  Overwrites the state."""
+        shape = (self.nx, self.nz, self.ny + 1, 3)
+        vv = np.asfortranarray(np.reshape(v, shape, order="F"), dtype=np.float64)
+        w = np.zeros(shape, order="F")
+        self._chk(self.L.cfg_arnoldi_matvec(self.h, int(tend), _p(vv), _p(w)))
+        return w if np.ndim(v) == 4 else w.ravel(order="F")
+
+    def set_jet(self, jet):
+        """crossflow = 1 with a CfgJet (jet_profile every substep), or None."""
+        self._chk(self.L.cfg_set_jet(self.h, C.byref(jet) if jet is not None else None))
+
+    def jet_profile(self, time, time_incr):
+        """pass2::jet_profile(time, time_incr, cbc_top(:,:,2), cbc_bot(:,:,2))."""
+        self._chk(self.L.cfg_jet_profile(self.h, time, time_incr))
+
+    def jet_forcing(self):
+        jf, inc = np.zeros(24), np.zeros(24)
+        self._chk(self.L.cfg_get_jet_forcing(self.h, _p(jf), _p(inc)))
+        return jf, inc
+
     def l2_norm(self):
         l2, drag = C.c_double(), C.c_double()
         self._chk(self.L.cfg_l2_norm(self.h, C.byref(l2), C.byref(drag)))
@@ -388,3 +447,21 @@ class ChannelFlow:
             self.set_scalars(0.0, sc["dt"], sc["p_grad"])
         self.remove_initial_divergence()
         self.compute_initial_pressure(0)
+
+
+def arnoldi_eigs(flow, tend, nev=12, ncv=25, tol=1e-8, maxiter=None, v0=None):
+    """Host driver of the Arnoldi stability solver (PFC/arnoldi.f90:150-330):
+    the largest-magnitude eigenvalues mu of the propagator Phi_T, T = tend*dt
+    (fixed dt), by implicitly restarted Arnoldi (ARPACK through
+    scipy.sparse.linalg.eigs, in place of the reference's PARPACK
+    pdnaupd/pdneupd) with ChannelFlow.arnoldi_matvec as the operator, and the
+    linearized eigenvalues cr = log(|mu| + eps)/T, ci = atan2(Im mu, Re mu)/T
+    (:803-806).  Returns (mu, cr + i*ci, eigenvectors (n, nev))."""
+    from scipy.sparse.linalg import LinearOperator, eigs
+    n = flow.nx * flow.nz * (flow.ny + 1) * 3
+    op = LinearOperator((n, n), matvec=lambda x: flow.arnoldi_matvec(np.real(np.ravel(x)), tend), dtype=np.float64)
+    mu, vec = eigs(op, k=nev, ncv=ncv, which="LM", tol=tol, maxiter=maxiter, v0=v0)
+    T = tend * flow.scalars()["dt"]
+    lam = (np.log(np.abs(mu) + np.finfo(np.float64).eps) + 1j * np.arctan2(mu.imag, mu.real)) / T
+    order = np.argsort(-np.abs(mu))
+    return mu[order], lam[order], vec[:, order]

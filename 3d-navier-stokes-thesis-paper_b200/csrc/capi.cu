@@ -14,6 +14,8 @@
 #include "pass1.cuh"
 #include "pass2.cuh"
 #include "pass1_fast.h"
+#include "arnoldi.cuh"
+#include "jet.cuh"
 #include "pass2v2.h"
 #include "planes.cuh"
 #include "regfft.cuh"
@@ -137,6 +139,10 @@ struct cfg_ctx {
   unsigned long long* divbits = nullptr;
   // lane-major grid coefficients of k_rhs2 (storage precision)
   void* rhs2_tbl = nullptr;
+  // crossflow jet (cfg_set_jet): parameters, device walk state
+  bool crossflow = false;
+  JetParams jp{};
+  JetState* jst = nullptr;
   int* plist = nullptr;
   // plane work buffers
   void *pw_H = nullptr, *pw_phys = nullptr, *pw_phys2 = nullptr, *pw_in = nullptr;
@@ -415,6 +421,11 @@ struct Impl {
   template <int MM>
   static int rhs_m(cfg_ctx* c, int rk, int mode) {
     const Geom& g = c->g;
+    // crossflow == 1: the wall jet of this substep (PFC/pass2.f90:41-43)
+    if (c->crossflow && mode == 0) {
+      const int r = jet(c, rk, 0.0, 0.0, 1);
+      if (r) return r;
+    }
     // fork: the FP64 low-|k| list and the mean mode on two side streams, one
     // warp per wavenumber so that they spread over many SMs beside the main
     // kernel
@@ -503,6 +514,57 @@ struct Impl {
     prof_begin(c, "k_pz_fwd");
     k_pz_fwd<T><<<dim3(g.nxh, np), 128, smz, c->st>>>((const C*)c->pw_H, out, osp, oskx, oskz, g.nxh, g.nz2, g.nz, 1,
                                                       scale, c->pz, (const C*)c->twz);
+    CKL();
+    return CFG_OK;
+  }
+
+  // small (nx x nz, no dealiasing) transforms of np planes,
+  // small_fft_real_to_complex / small_fft_complex_to_real
+  // (PFC/transform.f90:950-1142); H is a scratch of np*nxh*nz complex values
+  static int small_r2c(cfg_ctx* c, const T* phys, int np, C* out, size_t osp, size_t oskx, size_t oskz, C* H) {
+    const Geom& g = c->g;
+    const int smx = (int)(sizeof(C) * 3 * g.nx);
+    prof_begin(c, "k_px_fwd");
+    k_px_fwd<T><<<dim3((g.nz + 1) / 2, np), 128, smx, c->st>>>(phys, H, g.nxh, g.nz, g.nx, c->pxs, (const C*)c->twxs);
+    CKL();
+    const int smz = (int)(sizeof(C) * 3 * g.nz);
+    const T scale = (T)(1.0 / ((double)g.nx * (double)g.nz));
+    prof_begin(c, "k_pz_fwd");
+    k_pz_fwd<T><<<dim3(g.nxh, np), 128, smz, c->st>>>(H, out, osp, oskx, oskz, g.nxh, g.nz, g.nz, 0, scale, c->pzs,
+                                                      (const C*)c->twzs);
+    CKL();
+    return CFG_OK;
+  }
+  static int small_c2r(cfg_ctx* c, const C* in, PlaneIn L, int np, T* phys, C* H) {
+    const Geom& g = c->g;
+    const int smp = (int)(sizeof(C) * (g.nz + 2 * L.nc * g.nz));
+    prof_begin(c, "k_pz_inv");
+    k_pz_inv<T><<<dim3(g.nxh, np), 128, smp, c->st>>>(in, L, nullptr, np, H, g.nxh, g.nz, g.nz, 0, 0, c->pzs,
+                                                      (const C*)c->twzs);
+    CKL();
+    const int smx = (int)(sizeof(C) * 3 * g.nx);
+    prof_begin(c, "k_px_inv");
+    k_px_inv<T><<<dim3((g.nz + 1) / 2, np * L.nc), 128, smx, c->st>>>(H, phys, g.nxh, g.nz, g.nx, c->pxs,
+                                                                       (const C*)c->twxs);
+    CKL();
+    return CFG_OK;
+  }
+
+  // jet_profile (PFC/pass2.f90:423-673) into cbc(:,:,2): use_sc takes the
+  // end-of-substep time of substep rk from the device scalars
+  static int jet(cfg_ctx* c, int rk, double time, double incr, int use_sc) {
+    const Geom& g = c->g;
+    prof_begin(c, "k_jet_walk");
+    k_jet_walk<<<1, 32, 0, c->st>>>(c->jst, c->jp, c->sc, c->rkt, rk, time, incr, use_sc);
+    CKL();
+    prof_begin(c, "k_jet_field");
+    k_jet_field<T><<<dim3(g.nz, 3), 128, 0, c->st>>>((T*)c->pw_phys, c->jp, c->jst, g.nx, g.nz, c->p.lx, c->p.lz);
+    CKL();
+    int r = small_r2c(c, (const T*)c->pw_phys, 3, (C*)c->pw_in, (size_t)g.nw, g.nz, 1, (C*)c->pw_H);
+    if (r) return r;
+    prof_begin(c, "k_jet_combine");
+    k_jet_combine<T><<<(g.nw + 255) / 256, 256, 0, c->st>>>((const C*)c->pw_in, (C*)c->cbc, c->jp, c->gd, g.nx,
+                                                             g.nz, g.nxh, c->p.lx, c->p.lz);
     CKL();
     return CFG_OK;
   }
@@ -763,7 +825,7 @@ void cfg_destroy(cfg_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->dev);
   if (c->st) cudaStreamSynchronize(c->st);
-  void* bufs[] = {c->dgrid, c->fringe, c->vel, c->cru, c->prs, c->mvel64, c->mcru64, c->T1, c->T2, c->P, c->rhs2_tbl, c->cbc,
+  void* bufs[] = {c->dgrid, c->fringe, c->vel, c->cru, c->prs, c->mvel64, c->mcru64, c->T1, c->T2, c->P, c->rhs2_tbl, c->jst, c->cbc,
                   c->sc, c->d_um_dy, c->cflp, c->cflbits, c->l2acc, c->divbits, c->plist, c->pw_H,
                   c->pw_phys, c->pw_phys2, c->pw_in, c->stage, c->twx, c->twz, c->twxs, c->twzs,
                   c->wl_fast, c->wl_prec};
@@ -966,6 +1028,8 @@ static int timestep_impl(cfg_ctx* c, int nsteps, bool lin) {
 }
 
 int cfg_timestep(cfg_ctx* c, int nsteps) { return timestep_impl(c, nsteps, false); }
+
+
 int cfg_timestep_linearized(cfg_ctx* c, int nsteps) { return timestep_impl(c, nsteps, true); }
 
 int cfg_remove_initial_divergence(cfg_ctx* c) {
@@ -1050,13 +1114,125 @@ int cfg_xz_r2c(cfg_ctx* c, const double* data, double* cdata) {
   return CFG_OK;
 }
 
-int cfg_small_r2c(cfg_ctx* c, const double* data, double* cdata, int nplanes) {
-  (void)data; (void)cdata; (void)nplanes;
-  return fail(c, CFG_E_ARG, "cfg_small_r2c: not available");
+// the small transforms use the hybrid and flux work arrays as device scratch
+// (T1 holds the spectral planes; T2 the physical planes and, behind them, the
+// hybrid intermediate)
+static int small_capacity(cfg_ctx* c) {
+  const Geom& g = c->g;
+  const size_t t1 = (size_t)g.ny1 * 3 * g.nxh * g.nz2, t2 = (size_t)g.ny1 * 6 * g.nxh * g.nz2;
+  const size_t per_t2 = ((size_t)g.nx * g.nz + 1) / 2 + (size_t)g.nxh * g.nz + 1;
+  return (int)std::min<size_t>(std::min(t1 / g.nw, t2 / per_t2), 65535);
 }
+
+int cfg_small_r2c(cfg_ctx* c, const double* data, double* cdata, int nplanes) {
+  if (!c || !cdata || !data || nplanes < 1) return CFG_E_ARG;
+  if (nplanes > small_capacity(c)) return fail(c, CFG_E_ARG, "cfg_small_r2c: more than %d planes", small_capacity(c));
+  cudaSetDevice(c->dev);
+  const Geom& g = c->g;
+  const size_t nin = (size_t)g.nx * g.nz * nplanes, nout = (size_t)g.nw * nplanes;
+  int r = ensure_stage(c, std::max(nin, nout));
+  if (r) return r;
+  CK(cudaMemcpyAsync(c->stage, data, sizeof(double) * nin, cudaMemcpyHostToDevice, c->st));
+  if (c->mixed) {
+    k_real_in<float><<<grid1d(nin), 256, 0, c->st>>>((const double*)c->stage, (float*)c->T2, nin);
+    CKL();
+    r = Impl<float>::small_r2c(c, (const float*)c->T2, nplanes, (float2*)c->T1, (size_t)g.nw, g.nz, 1,
+                               (float2*)c->T2 + (nin + 1) / 2);
+    if (r) return r;
+    k_conv_out<float><<<grid1d(nout), 256, 0, c->st>>>((const float2*)c->T1, c->stage, nout, nullptr, 0);
+  } else {
+    k_real_in<double><<<grid1d(nin), 256, 0, c->st>>>((const double*)c->stage, (double*)c->T2, nin);
+    CKL();
+    r = Impl<double>::small_r2c(c, (const double*)c->T2, nplanes, (double2*)c->T1, (size_t)g.nw, g.nz, 1,
+                                (double2*)c->T2 + (nin + 1) / 2);
+    if (r) return r;
+    k_conv_out<double><<<grid1d(nout), 256, 0, c->st>>>((const double2*)c->T1, c->stage, nout, nullptr, 0);
+  }
+  CKL();
+  CK(cudaMemcpyAsync(cdata, c->stage, sizeof(double2) * nout, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return CFG_OK;
+}
+
 int cfg_small_c2r(cfg_ctx* c, const double* cdata, double* data, int nplanes) {
-  (void)data; (void)cdata; (void)nplanes;
-  return fail(c, CFG_E_ARG, "cfg_small_c2r: not available");
+  if (!c || !cdata || !data || nplanes < 1) return CFG_E_ARG;
+  if (nplanes > small_capacity(c)) return fail(c, CFG_E_ARG, "cfg_small_c2r: more than %d planes", small_capacity(c));
+  cudaSetDevice(c->dev);
+  const Geom& g = c->g;
+  const size_t nin = (size_t)g.nw * nplanes, nout = (size_t)g.nx * g.nz * nplanes;
+  int r = ensure_stage(c, std::max(nin, nout));
+  if (r) return r;
+  CK(cudaMemcpyAsync(c->stage, cdata, sizeof(double2) * nin, cudaMemcpyHostToDevice, c->st));
+  PlaneIn L{(size_t)g.nw, 0, (size_t)g.nz, 1, 1};
+  if (c->mixed) {
+    k_conv_in<float><<<grid1d(nin), 256, 0, c->st>>>(c->stage, (float2*)c->T1, nin, nullptr, 0);
+    CKL();
+    r = Impl<float>::small_c2r(c, (const float2*)c->T1, L, nplanes, (float*)c->T2, (float2*)c->T2 + (nout + 1) / 2);
+    if (r) return r;
+    k_real_out<float><<<grid1d(nout), 256, 0, c->st>>>((const float*)c->T2, (double*)c->stage, nout);
+  } else {
+    k_conv_in<double><<<grid1d(nin), 256, 0, c->st>>>(c->stage, (double2*)c->T1, nin, nullptr, 0);
+    CKL();
+    r = Impl<double>::small_c2r(c, (const double2*)c->T1, L, nplanes, (double*)c->T2,
+                                (double2*)c->T2 + (nout + 1) / 2);
+    if (r) return r;
+    k_real_out<double><<<grid1d(nout), 256, 0, c->st>>>((const double*)c->T2, (double*)c->stage, nout);
+  }
+  CKL();
+  CK(cudaMemcpyAsync(data, c->stage, sizeof(double) * nout, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return CFG_OK;
+}
+
+int cfg_set_jet(cfg_ctx* c, const cfg_jet* j) {
+  if (!c) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  if (!j || j->mode == 0) {
+    c->crossflow = false;
+    return CFG_OK;
+  }
+  if (j->mode != 1 && j->mode != 2) return fail(c, CFG_E_ARG, "cfg_set_jet: mode %d", j->mode);
+  if (j->filter_jet_profile < 0) return fail(c, CFG_E_ARG, "cfg_set_jet: filter_jet_profile < 0");
+  if (j->mode == 1 && !(j->jet_diam > 0.0)) return fail(c, CFG_E_ARG, "cfg_set_jet: jet_diam must be positive");
+  if (j->mode == 2 && !(j->width > 0.0)) return fail(c, CFG_E_ARG, "cfg_set_jet: width must be positive");
+  // define_suction_profile (PFC/pass2.f90:565-567)
+  const double frac_suct = 0.5 * j->frac_xbuff, xend = c->p.lx * (1.0 - j->frac_xbuff) + c->p.lx * frac_suct;
+  if (!(j->frac_xbuff > 0.0) || xend > c->p.lx) return fail(c, CFG_E_ARG, "Suction must end inside box.");
+  JetParams& p = c->jp;
+  p.mode = j->mode;
+  for (int w = 0; w < 2; ++w) {
+    p.xjet[w] = j->xjet[w]; p.zjet[w] = j->zjet[w]; p.jetmag[w] = j->jetmag[w];
+    p.forcing[w] = j->forcing[w]; p.for_freq[w] = j->for_freq[w];
+  }
+  p.jet_diam = j->jet_diam; p.width = j->width; p.freq = j->freq; p.frac_xbuff = j->frac_xbuff;
+  p.filter = j->filter_jet_profile; p.seed = j->seed;
+  if (!c->jst && cudaMalloc(&c->jst, sizeof(JetState)) != cudaSuccess) return fail(c, CFG_E_NOMEM, "jet state");
+  JetState h{};
+  memcpy(h.jf, j->jet_forcing, sizeof(h.jf));
+  memcpy(h.inc, j->jet_forcing_incr, sizeof(h.inc));
+  CK(cudaMemcpyAsync(c->jst, &h, sizeof(h), cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  c->crossflow = true;
+  return CFG_OK;
+}
+
+int cfg_jet_profile(cfg_ctx* c, double time, double time_incr) {
+  if (!c) return CFG_E_ARG;
+  if (!c->crossflow) return fail(c, CFG_E_STATE, "cfg_jet_profile: no jet set (cfg_set_jet)");
+  cudaSetDevice(c->dev);
+  return DISPATCH(c, jet(c, 0, time, time_incr, 0));
+}
+
+int cfg_get_jet_forcing(cfg_ctx* c, double* jet_forcing, double* jet_forcing_incr) {
+  if (!c) return CFG_E_ARG;
+  if (!c->jst) return fail(c, CFG_E_STATE, "cfg_get_jet_forcing: no jet set (cfg_set_jet)");
+  cudaSetDevice(c->dev);
+  JetState h{};
+  CK(cudaMemcpyAsync(&h, c->jst, sizeof(h), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (jet_forcing) memcpy(jet_forcing, h.jf, sizeof(h.jf));
+  if (jet_forcing_incr) memcpy(jet_forcing_incr, h.inc, sizeof(h.inc));
+  return CFG_OK;
 }
 
 int cfg_l2_norm(cfg_ctx* c, double* l2, double* drag) {
@@ -1147,3 +1323,75 @@ int cfg_synchronize(cfg_ctx* c) {
 }
 
 }  // extern "C"
+
+// compute_time_deriv (PFC/arnoldi.f90:485-567) on the device; see chanflow.h
+int cfg_arnoldi_matvec(cfg_ctx* c, int tend, const double* v, double* w) {
+  if (!c || !v || !w || tend < 0) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  const Geom& g = c->g;
+  const int np = 3 * g.ny1;
+  if (np > small_capacity(c)) return fail(c, CFG_E_ARG, "cfg_arnoldi_matvec: %d planes exceed the scratch", np);
+  const size_t nvec = (size_t)g.nx * g.nz * np, nf = (size_t)g.nw * np;
+  int r = ensure_stage(c, nvec);
+  if (r) return r;
+  CK(cudaMemcpyAsync(c->stage, v, sizeof(double) * nvec, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemsetAsync(c->divbits, 0, sizeof(unsigned long long), c->st));
+  k_absmax<<<std::min<size_t>(1184, (nvec + 255) / 256), 256, 0, c->st>>>((const double*)c->stage, nvec, c->divbits);
+  CKL();
+  unsigned long long mb = 0;
+  CK(cudaMemcpyAsync(&mb, c->divbits, sizeof(mb), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (mb == 0) return fail(c, CFG_E_ARG, "cfg_arnoldi_matvec: zero vector");
+  const double eps = 1.0e-8;   // PFC/arnoldi.f90:500
+  PlaneIn L{1, 0, (size_t)g.nz * np, (size_t)np, 1};
+  if (c->mixed) {
+    using C = float2;
+    k_real_in<float><<<grid1d(nvec), 256, 0, c->st>>>((const double*)c->stage, (float*)c->T2, nvec);
+    CKL();
+    r = Impl<float>::small_r2c(c, (const float*)c->T2, np, (C*)c->vel, 1, (size_t)g.nz * np, np, (C*)c->T1);
+    if (r) return r;
+    k_arnoldi_scale<float><<<grid1d(nf), 256, 0, c->st>>>((C*)c->vel, g, c->gd, c->divbits, eps, 0);
+    CKL();
+    k_mean_widen<float><<<1, 256, 0, c->st>>>((const C*)c->vel, c->mvel64, g.ny1);
+    CKL();
+    CK(cudaMemcpyAsync(c->mcru64, c->mvel64, sizeof(double2) * 3 * g.ny1, cudaMemcpyDeviceToDevice, c->st));
+  } else {
+    using C = double2;
+    k_real_in<double><<<grid1d(nvec), 256, 0, c->st>>>((const double*)c->stage, (double*)c->T2, nvec);
+    CKL();
+    r = Impl<double>::small_r2c(c, (const double*)c->T2, np, (C*)c->vel, 1, (size_t)g.nz * np, np, (C*)c->T1);
+    if (r) return r;
+    k_arnoldi_scale<double><<<grid1d(nf), 256, 0, c->st>>>((C*)c->vel, g, c->gd, c->divbits, eps, 0);
+    CKL();
+  }
+  c->mean64_valid = true;
+  // data2 = data1, p_grad = 0, d_um_dy = 0, initial pressure, t_total = 0
+  CK(cudaMemcpyAsync(c->cru, c->vel, csize(c) * nf, cudaMemcpyDeviceToDevice, c->st));
+  CK(cudaMemsetAsync(c->d_um_dy, 0, sizeof(double) * g.ny, c->st));
+  k_arnoldi_reset<<<1, 1, 0, c->st>>>(c->sc);
+  CKL();
+  r = cfg_compute_initial_pressure(c, 1);
+  if (r) return r;
+  c->step = 0;
+  r = timestep_impl(c, tend, true);
+  if (r) return r;
+  if (c->mixed) {
+    using C = float2;
+    k_arnoldi_scale<float><<<grid1d(nf), 256, 0, c->st>>>((C*)c->vel, g, c->gd, c->divbits, eps, 1);
+    CKL();
+    r = Impl<float>::small_c2r(c, (const C*)c->vel, L, np, (float*)c->T2, (C*)c->T1);
+    if (r) return r;
+    k_real_out<float><<<grid1d(nvec), 256, 0, c->st>>>((const float*)c->T2, (double*)c->stage, nvec);
+  } else {
+    using C = double2;
+    k_arnoldi_scale<double><<<grid1d(nf), 256, 0, c->st>>>((C*)c->vel, g, c->gd, c->divbits, eps, 1);
+    CKL();
+    r = Impl<double>::small_c2r(c, (const C*)c->vel, L, np, (double*)c->T2, (C*)c->T1);
+    if (r) return r;
+    k_real_out<double><<<grid1d(nvec), 256, 0, c->st>>>((const double*)c->T2, (double*)c->stage, nvec);
+  }
+  CKL();
+  CK(cudaMemcpyAsync(w, c->stage, sizeof(double) * nvec, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return cfg_status(c);
+}

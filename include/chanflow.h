@@ -130,6 +130,17 @@ int cfg_timestep(cfg_ctx *c, int nsteps);
 /* Same with nonlinear_linearized (the arnoldi.f90 matvec loop, :540-547). */
 int cfg_timestep_linearized(cfg_ctx *c, int nsteps);
 
+/* arnoldi::compute_time_deriv, PFC/arnoldi.f90:485-567: the propagator
+ * matvec w = Phi_T v of the Arnoldi stability solver (the OP*x step of the
+ * pdnaupd reverse-communication loop, :257-300).  v and w are host vectors
+ * (nx, nz, ny+1, 3) of physical velocity planes.  v is scaled by
+ * eps/max|v| (eps = 1e-8) and sqrt(dyh) (u, w) or sqrt(dy) (v) weights,
+ * transformed with small_fft_real_to_complex into data1 = data2, p_grad and
+ * d_um_dy are zeroed, the initial pressure is computed with the linearized
+ * term, tend linearized steps are taken from t_total = 0, and the result is
+ * unweighted and transformed back.  Overwrites the context's state. */
+int cfg_arnoldi_matvec(cfg_ctx *c, int tend, const double *v, double *w);
+
 /* transform::xz_fft_complex_to_real / xz_fft_real_to_complex,
  * PFC/transform.f90:195-227,258-409: one plane, host arrays
  * cdata (nz, nx/2+1) complex and data (nx2, nz2) real. */
@@ -137,9 +148,47 @@ int cfg_xz_c2r(cfg_ctx *c, const double *cdata, double *data);
 int cfg_xz_r2c(cfg_ctx *c, const double *data, double *cdata);
 /* transform::small_fft_real_to_complex / small_fft_complex_to_real,
  * PFC/transform.f90:950-1142: nx x nz grid, no dealiasing, nplanes planes
- * (data (nx, nz, nplanes), cdata (nz, nx/2+1, nplanes)). */
+ * (data (nx, nz, nplanes), cdata (nz, nx/2+1, nplanes)); forward scaled by
+ * 1/(nx*nz).  Computed in the context's precision.  Up to about 3*(ny+1)
+ * planes per call (CFG_E_ARG beyond). */
 int cfg_small_r2c(cfg_ctx *c, const double *data, double *cdata, int nplanes);
 int cfg_small_c2r(cfg_ctx *c, const double *cdata, double *data, int nplanes);
+
+/* Crossflow wall forcing, the cbc_top/cbc_bot(:,:,2) slot (jet_profile,
+ * PFC/pass2.f90:423-673, closed channel).  Index 0 of each pair is the
+ * bottom wall, 1 the top; a wall is forced when its jetmag is nonzero
+ * (:494,517).  Mode 1 is the reference's tanh jet with Freund forcing
+ * (define_jet_profile, :611-656); mode 2 a Gaussian spanwise slot at x = xjet,
+ * v = jetmag exp(-(d/width)^2) (1 + sin(2 pi freq t))/2, written to the same
+ * slot.  Both subtract the suction profile (define_suction_profile, :553-609)
+ * that balances the jet's mass flux.  The Freund parameters random-walk on
+ * every call (:454-477) with RANDOM_NUMBER replaced by the counter RNG of the
+ * initial field: draw n (0..23) of call k is u01(seed, k, 0, n, 7);
+ * seed 0 keeps them fixed. */
+typedef struct cfg_jet {
+  int mode;                        /* 0 off, 1 tanh jet, 2 Gaussian slot */
+  double xjet[2], zjet[2];         /* jet centre (absolute x, z) */
+  double jetmag[2];                /* jet velocity (mode 2: slot peak) */
+  double forcing[2], for_freq[2];  /* mode 1 amplitude modulation */
+  double jet_diam;                 /* mode 1 */
+  double width, freq;              /* mode 2 */
+  double frac_xbuff;               /* suction band (flow.dat frac_xbuff) */
+  int filter_jet_profile;          /* raised-cosine filter passes */
+  double jet_forcing[24];          /* (3,2,4) Freund A, St, phi, psi */
+  double jet_forcing_incr[24];     /* (3,2,4) their random-walk increments */
+  unsigned long long seed;         /* random-walk seed, 0: fixed parameters */
+} cfg_jet;
+/* crossflow = 1 (jet != NULL, mode != 0): every cfg_rhs_solve / cfg_timestep
+ * substep first calls jet_profile with the end-of-substep time
+ * t_total + dt*SUM(rkc(1:rk)+rkd(1:rk)) and increment dt*(rkc(rk)+rkd(rk))
+ * (PFC/pass2.f90:37-44), from the device-resident t_total and dt.  Resets
+ * the forcing parameters and the call counter.  NULL: crossflow = 0. */
+int cfg_set_jet(cfg_ctx *c, const cfg_jet *jet);
+/* pass2::jet_profile(time, time_incr, ctop, cbot) with host-given time:
+ * random walk, then cbc_top/cbc_bot(:,:,2).  Needs cfg_set_jet. */
+int cfg_jet_profile(cfg_ctx *c, double time, double time_incr);
+/* The current forcing parameters and increments (24 each; NULL skips). */
+int cfg_get_jet_forcing(cfg_ctx *c, double *jet_forcing, double *jet_forcing_incr);
 
 /* read_write::l2_norm, PFC/read_write.f90:1432-1462: perturbation L2 norm
  * about U=1-y^2 and the wall-shear difference d_um_dy(1)-d_um_dy(ny). */

@@ -182,6 +182,10 @@ struct orc_ctx {
   double t_total, dt, p_grad;
   int step, rk_step, status;
   fft_plan *px2, *pz2, *pxs, *pzs;
+  /* crossflow jet (PFC/pass2.f90:37-44, 423-673) */
+  int crossflow;
+  orc_jet jet;
+  long long jet_calls;
 };
 
 #define D1(c, z, x, j, q) (c)->data1[(z) + (size_t)(c)->p.nz * ((x) + (size_t)(c)->nxh * ((j) + (size_t)((c)->p.ny + 1) * (q)))]
@@ -892,6 +896,12 @@ static void rhs_one(orc_ctx *c, int x, int z) {
 
 void orc_rhs_solve(orc_ctx *c) {
   int nz = c->p.nz, nxh = c->nxh;
+  if (c->crossflow) {
+    /* end-of-substep time and increment, PFC/pass2.f90:37-38 */
+    double s = 0.0;
+    for (int r = 1; r <= c->rk_step; r++) s += RKC(r) + RKD(r);
+    orc_jet_profile(c, c->t_total + c->dt * s, c->dt * (RKC(c->rk_step) + RKD(c->rk_step)));
+  }
   rhs_one(c, 0, 0); /* mean mode first: it updates p_grad and d_um_dy */
 #pragma omp parallel for schedule(dynamic, 16)
   for (int t = 1; t < nz * nxh; t++) rhs_one(c, t / nz, t % nz);
@@ -1164,9 +1174,9 @@ double orc_max_divergence(orc_ctx *c) {
 }
 
 /* ------------------------------------------------------------------ */
-/* jet_profile, PFC/pass2.f90:423-673, with the forcing parameters given
- * (their random walk, :454-477, belongs to the caller) and bl_grid = 0.
- * Mode 2 is the Gaussian slot generator writing the same cbc(:,:,2) slot. */
+/* jet_profile, PFC/pass2.f90:423-673, with bl_grid = 0 (closed channel:
+ * the suction profile balances the jet's mass flux).  Mode 2 is the Gaussian
+ * slot generator writing the same cbc(:,:,2) slot. */
 static void filter_cosine(orc_ctx *c, cplx *cu) {
   int nz = c->p.nz, nxh = c->nxh;
   for (int x = 0; x < nxh; x++)
@@ -1176,10 +1186,44 @@ static void filter_cosine(orc_ctx *c, cplx *cu) {
           (1.0 + cos(c->pi * c->kz[z] / ((double)(nz / 2) * 2.0 * c->pi / c->p.lz)));
 }
 
-void orc_jet_profile(orc_ctx *c, const orc_jet *jt, double time) {
+void orc_set_jet(orc_ctx *c, const orc_jet *j) {
+  if (j) c->jet = *j;
+  c->crossflow = j != NULL && j->mode != 0;
+  c->jet_calls = 0;
+}
+
+void orc_get_jet_forcing(orc_ctx *c, double *jf, double *incr) {
+  if (jf) memcpy(jf, c->jet.jet_forcing, sizeof(double) * 24);
+  if (incr) memcpy(incr, c->jet.jet_forcing_incr, sizeof(double) * 24);
+}
+
+/* random walk of the Freund forcing parameters, PFC/pass2.f90:454-477 */
+static void jet_walk(orc_ctx *c, double time_incr) {
+  orc_jet *jt = &c->jet;
+  double *jf = jt->jet_forcing, *inc = jt->jet_forcing_incr;
+  for (int n = 0; n < 24; n++) {
+    double r = rng_u01(jt->seed, (int)c->jet_calls, 0, n, 7);
+    /* SIGN(1, r - 0.05) */
+    inc[n] = inc[n] * ((r - 0.05) >= 0.0 ? 1.0 : -1.0);
+  }
+  for (int n = 0; n < 24; n++) jf[n] = jf[n] + time_incr * inc[n];
+  for (int j = 0; j < 2; j++)
+    for (int i = 0; i < 3; i++) {
+      int a = i + 3 * j, b = i + 3 * j + 6;   /* (i,j,1), (i,j,2) */
+      if (jf[a] <= 0.01) { jf[a] = 0.01; inc[a] = fabs(inc[a]); }
+      else if (jf[a] >= 0.07) { jf[a] = 0.07; inc[a] = -fabs(inc[a]); }
+      if (jf[b] <= 0.1) { jf[b] = 0.1; inc[b] = fabs(inc[b]); }
+      else if (jf[b] >= 0.7) { jf[b] = 0.7; inc[b] = -fabs(inc[b]); }
+    }
+}
+
+void orc_jet_profile(orc_ctx *c, double time, double time_incr) {
+  const orc_jet *jt = &c->jet;
   int nx = c->p.nx, nz = c->p.nz, nxh = c->nxh;
   size_t cs = (size_t)nz * nxh, ns = (size_t)nx * nz;
   double lx = c->p.lx, lz = c->p.lz, pi = c->pi;
+  if (jt->seed != 0) jet_walk(c, time_incr);
+  c->jet_calls++;
   double *f = malloc(sizeof(double) * ns * 2), *vj = f + ns;
   cplx *cs_ = malloc(sizeof(cplx) * cs * 2), *cj = cs_ + cs;
   /* define_suction_profile, PFC/pass2.f90:553-609 */
@@ -1202,15 +1246,16 @@ void orc_jet_profile(orc_ctx *c, const orc_jet *jt, double time) {
   double sum_suction = creal(cs_[0]);
   for (int wall = 0; wall < 2; wall++) {
     cplx *dst = (wall == 0 ? c->cbc_bot : c->cbc_top) + cs;
-    if (!(jt->wall & (1 << wall)) || jt->mode == 0) { memset(dst, 0, sizeof(cplx) * cs); continue; }
+    if (jt->jetmag[wall] == 0.0 || jt->mode == 0) { memset(dst, 0, sizeof(cplx) * cs); continue; }
+    double jm = jt->jetmag[wall];
     if (jt->mode == 1) {
       /* define_jet_profile, PFC/pass2.f90:611-656 */
       const double fw[6] = {0, 1, 2, 0, 1, 2};
-      double v_ampl = jt->jetmag * (1.0 + jt->forcing * sin(2.0 * pi * time * jt->for_freq * jt->jetmag / jt->jet_diam));
+      double v_ampl = jm * (1.0 + jt->forcing[wall] * sin(2.0 * pi * time * jt->for_freq[wall] * jm / jt->jet_diam));
       for (int z = 1; z <= nz; z++)
         for (int x = 1; x <= nx; x++) {
-          double xd1 = F(c->xcoord, x) - jt->xjet, xd2 = F(c->xcoord, x) - (lx + jt->xjet);
-          double zd1 = F(c->zcoord, z) - jt->zjet, zd2 = F(c->zcoord, z) - (lz + jt->zjet);
+          double xd1 = F(c->xcoord, x) - jt->xjet[wall], xd2 = F(c->xcoord, x) - (lx + jt->xjet[wall]);
+          double zd1 = F(c->zcoord, z) - jt->zjet[wall], zd2 = F(c->zcoord, z) - (lz + jt->zjet[wall]);
           /* ABS(CMPLX(a,b)) without KIND is a default-real (single) complex */
           double r1 = (double)hypotf((float)xd1, (float)zd1) * 2.0 / jt->jet_diam;
           double r2 = (double)hypotf((float)xd2, (float)zd1) * 2.0 / jt->jet_diam;
@@ -1222,7 +1267,7 @@ void orc_jet_profile(orc_ctx *c, const orc_jet *jt, double time) {
           else {
             double phi = atan2(zd1, xd1), s = 0;
             for (int i = 0; i < 6; i++)
-              s += jt->jet_forcing[i] * cos(jt->jet_forcing[6 + i] * jt->jetmag * time / jt->jet_diam + jt->jet_forcing[12 + i]) *
+              s += jt->jet_forcing[i] * cos(jt->jet_forcing[6 + i] * jm * time / jt->jet_diam + jt->jet_forcing[12 + i]) *
                    cos(fw[i] * phi + jt->jet_forcing[18 + i]);
             double bjet = 5.0 + s;
             v = v_ampl * 0.5 * (1.0 - tanh(bjet * (r - 1.0 / r)));
@@ -1230,11 +1275,11 @@ void orc_jet_profile(orc_ctx *c, const orc_jet *jt, double time) {
           vj[(x - 1) + (size_t)nx * (z - 1)] = v;
         }
     } else {
-      /* Gaussian spanwise slot: v = peak exp(-(d/width)^2) (1+sin(2 pi f t))/2 */
-      double a = jt->peak * 0.5 * (1.0 + sin(2.0 * pi * jt->freq * time));
+      /* Gaussian spanwise slot at x = xjet */
+      double a = jm * 0.5 * (1.0 + sin(2.0 * pi * jt->freq * time));
       for (int z = 0; z < nz; z++)
         for (int x = 1; x <= nx; x++) {
-          double d = fabs(F(c->xcoord, x) - jt->xjet);
+          double d = fabs(F(c->xcoord, x) - jt->xjet[wall]);
           if (lx - d < d) d = lx - d;
           vj[(x - 1) + (size_t)nx * z] = a * exp(-(d / jt->width) * (d / jt->width));
         }

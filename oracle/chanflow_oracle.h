@@ -102,18 +102,30 @@ void orc_timestep(orc_ctx *c, int nsteps, int linearized);
 double orc_bulk_flux(orc_ctx *c);          /* Q, PFC/pass2.f90:106-108 */
 double orc_max_divergence(orc_ctx *c);     /* PFC/pass2.f90:380-419 */
 
-/* wall forcing (cbc(:,:,2)), PFC/pass2.f90:423-673 */
+/* wall forcing (cbc(:,:,2)), PFC/pass2.f90:423-673.  Index 0 is the bottom
+ * wall, 1 the top; a wall is forced when its jetmag is nonzero (:494,517). */
 typedef struct orc_jet {
   int mode;               /* 0 none, 1 reference tanh jet, 2 gaussian slot */
-  int wall;               /* bit0 bottom, bit1 top */
-  double xjet, zjet;      /* absolute positions */
-  double jetmag, forcing, for_freq, jet_diam;
-  double width, peak, freq; /* gaussian slot */
+  double xjet[2], zjet[2];        /* jet centre (absolute x, z) */
+  double jetmag[2];               /* jet velocity (mode 2: slot peak velocity) */
+  double forcing[2], for_freq[2]; /* amplitude modulation, mode 1 */
+  double jet_diam;                /* mode 1 */
+  double width, freq;             /* gaussian slot: v = jetmag exp(-(d/width)^2) (1+sin 2 pi freq t)/2 */
   double frac_xbuff;      /* suction region (PFC/pass2.f90:553-609) */
   int filter_jet_profile;
-  double jet_forcing[24]; /* (3,2,4) Freund forcing parameters, fixed */
+  double jet_forcing[24];       /* (3,2,4) Freund forcing parameters */
+  double jet_forcing_incr[24];  /* (3,2,4) their random-walk increments */
+  unsigned long long seed;      /* random walk RNG seed (0: parameters fixed) */
 } orc_jet;
-void orc_jet_profile(orc_ctx *c, const orc_jet *j, double time);
+/* crossflow == 1: rhs_solve calls jet_profile at every substep with the
+ * end-of-substep time (PFC/pass2.f90:37-44).  NULL switches it off. */
+void orc_set_jet(orc_ctx *c, const orc_jet *j);
+/* jet_profile(time, time_incr): random walk of the forcing parameters
+ * (:454-477, RANDOM_NUMBER replaced by the counter RNG, draw n of call k is
+ * orc_rng_u01(seed, k, 0, n, 7)), then the wall profile into cbc(:,:,2). */
+void orc_jet_profile(orc_ctx *c, double time, double time_incr);
+/* current forcing parameters and increments (24 each, may be NULL) */
+void orc_get_jet_forcing(orc_ctx *c, double *jet_forcing, double *jet_forcing_incr);
 
 /* Arnoldi propagator matvec, PFC/arnoldi.f90:485-567 */
 void orc_arnoldi_matvec(orc_ctx *c, int tend, const double *v, double *w);

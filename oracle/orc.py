@@ -28,15 +28,18 @@ class OrcParams(C.Structure):
 
 
 class OrcJet(C.Structure):
+    """orc_jet: index 0 of the per-wall pairs is the bottom wall, 1 the top."""
     _fields_ = [
-        ("mode", C.c_int), ("wall", C.c_int),
-        ("xjet", C.c_double), ("zjet", C.c_double),
-        ("jetmag", C.c_double), ("forcing", C.c_double), ("for_freq", C.c_double),
+        ("mode", C.c_int),
+        ("xjet", C.c_double * 2), ("zjet", C.c_double * 2),
+        ("jetmag", C.c_double * 2), ("forcing", C.c_double * 2), ("for_freq", C.c_double * 2),
         ("jet_diam", C.c_double),
-        ("width", C.c_double), ("peak", C.c_double), ("freq", C.c_double),
+        ("width", C.c_double), ("freq", C.c_double),
         ("frac_xbuff", C.c_double),
         ("filter_jet_profile", C.c_int),
         ("jet_forcing", C.c_double * 24),
+        ("jet_forcing_incr", C.c_double * 24),
+        ("seed", C.c_ulonglong),
     ]
 
 
@@ -87,7 +90,9 @@ def lib():
         L.orc_bulk_flux.restype = C.c_double
         L.orc_max_divergence.argtypes = [vp]
         L.orc_max_divergence.restype = C.c_double
-        L.orc_jet_profile.argtypes = [vp, C.POINTER(OrcJet), C.c_double]
+        L.orc_set_jet.argtypes = [vp, C.POINTER(OrcJet)]
+        L.orc_jet_profile.argtypes = [vp, C.c_double, C.c_double]
+        L.orc_get_jet_forcing.argtypes = [vp, vp, vp]
         L.orc_arnoldi_matvec.argtypes = [vp, C.c_int, vp, vp]
         _lib = L
     return _lib
@@ -275,8 +280,18 @@ class Oracle:
     def max_divergence(self):
         return self.L.orc_max_divergence(self.h)
 
-    def jet_profile(self, jet, time):
-        self.L.orc_jet_profile(self.h, C.byref(jet), time)
+    def set_jet(self, jet):
+        """Crossflow on (jet an OrcJet) or off (None)."""
+        self.L.orc_set_jet(self.h, C.byref(jet) if jet is not None else None)
+
+    def jet_profile(self, time, time_incr):
+        self.L.orc_jet_profile(self.h, time, time_incr)
+
+    def jet_forcing(self):
+        jf = np.zeros(24)
+        inc = np.zeros(24)
+        self.L.orc_get_jet_forcing(self.h, jf.ctypes.data, inc.ctypes.data)
+        return jf, inc
 
     def arnoldi_matvec(self, v, tend):
         v = np.asfortranarray(v, dtype=np.float64)

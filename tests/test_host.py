@@ -96,3 +96,39 @@ def test_flow_dat_reader_on_reference_file(cf):
     assert (run.nx, run.ny, run.nz, run.nx2, run.nz2) == (128, 200, 64, 192, 96)
     assert run.re == 7500.0 and run.which_test == 9 and run.l2_step == 20
     assert abs(run.lx - 6 * np.pi) < 1e-14 and abs(run.lz - 2 * np.pi) < 1e-14
+
+
+def test_arnoldi_driver_eigenvalues(cf):
+    """arnoldi_eigs on an operator of known spectrum: Phi_T = exp(L T) with
+    L diagonal; the driver must return mu = exp(lambda T) ordered by |mu| and
+    recover lambda = log|mu|/T + i atan2(Im mu, Re mu)/T (PFC/arnoldi.f90:803-806)."""
+    import numpy as np
+
+    class FakeFlow:
+        nx, ny, nz = 4, 3, 4
+
+        def __init__(self):
+            n = self.nx * self.nz * (self.ny + 1) * 3
+            rng = np.random.default_rng(0)
+            self.T = 0.5
+            lam = -rng.uniform(0.5, 4.0, n)
+            lam[:3] = [-0.01, -0.2, -0.35]
+            self.mu = np.exp(lam * self.T)
+            self.lam = lam
+            self.calls = 0
+
+        def arnoldi_matvec(self, v, tend):
+            assert tend == 10
+            self.calls += 1
+            return self.mu * v
+
+        def scalars(self):
+            return {"dt": 0.05}
+
+    f = FakeFlow()
+    mu, lam, vec = cf.chanflow.arnoldi_eigs(f, 10, nev=3, ncv=12, tol=1e-12,
+                                            v0=np.ones(f.mu.size))
+    np.testing.assert_allclose(mu.real, np.exp(np.array([-0.01, -0.2, -0.35]) * f.T), rtol=1e-10)
+    np.testing.assert_allclose(lam.real, [-0.01, -0.2, -0.35], rtol=1e-8)
+    assert np.abs(lam.imag).max() < 1e-12
+    assert vec.shape == (f.mu.size, 3)

@@ -116,3 +116,65 @@ def test_cfl_abort_flag(orc):
     o.timestep(1)
     assert o.status() == -1
     assert o.cfl[1:17].max() >= 1.15
+
+
+def test_jet_gaussian_slot_profile(orc):
+    """Mode 2 with no filter: the wall value transformed back to physical
+    space is the Gaussian slot minus the suction profile scaled to cancel its
+    mass flux (PFC/pass2.f90:493-537)."""
+    nx, nz = 32, 16
+    o = orc.Oracle(nx, 9, nz)
+    lx = 4 * np.pi
+    j = orc.OrcJet()
+    j.mode = 2
+    j.jetmag[0] = 0.1
+    j.xjet[0] = 0.3 * lx
+    j.width, j.freq, j.frac_xbuff = 0.2 * lx, 0.5, 0.2
+    o.set_jet(j)
+    t = 0.3
+    o.jet_profile(t, 0.1)
+    v = o.small_c2r(np.asfortranarray(o.cbc_bot[:, :, 1]))
+    x = np.arange(nx) * lx / nx
+    d = np.abs(x - j.xjet[0])
+    d = np.minimum(d, lx - d)
+    slot = 0.1 * 0.5 * (1 + np.sin(2 * np.pi * 0.5 * t)) * np.exp(-(d / j.width) ** 2)
+    # suction band: x in (0.8 lx, 0.9 lx), smooth rise/fall over 0.025 lx
+    xs, xe = 0.8 * lx, 0.9 * lx
+    xr, xf = xs + 0.025 * lx, xe - 0.025 * lx
+    f = np.zeros(nx)
+    for i, xc in enumerate(x):
+        if xs < xc < xe:
+            if xc < xr:
+                x2 = (xc - xs) / (xr - xs)
+                f[i] = 1 / (1 + np.exp(1 / x2 + 1 / (x2 - 1)))
+            elif xc > xf:
+                x2 = (xe - xc) / (xe - xf)
+                f[i] = 1 / (1 + np.exp(1 / x2 + 1 / (x2 - 1)))
+            else:
+                f[i] = 1.0
+    expect = slot - slot.mean() / f.mean() * f
+    np.testing.assert_allclose(v, np.repeat(expect[:, None], nz, axis=1), atol=1e-13)
+    # the top wall is not forced (jetmag 0)
+    assert np.abs(o.cbc_top[:, :, 1]).max() == 0.0
+
+
+def test_jet_random_walk_bounds(orc):
+    o = orc.Oracle(16, 9, 16)
+    j = orc.OrcJet()
+    j.mode, j.jetmag[0], j.jet_diam = 1, 0.1, 0.5
+    j.frac_xbuff, j.seed = 0.2, 99
+    for i in range(24):
+        j.jet_forcing[i] = [0.04, 0.4, 1.0, 1.0][i // 6]
+        j.jet_forcing_incr[i] = 0.3
+    o.set_jet(j)
+    flips = 0
+    prev = np.full(24, 0.3)
+    for k in range(400):
+        o.jet_profile(0.01 * k, 0.05)
+        jf, inc = o.jet_forcing()
+        assert jf[0:6].min() >= 0.01 and jf[0:6].max() <= 0.07
+        assert jf[6:12].min() >= 0.1 and jf[6:12].max() <= 0.7
+        flips += int(np.sum(np.sign(inc[12:]) != np.sign(prev[12:])))
+        prev = inc
+    # phases are not clamped: their increments flip with probability 0.05
+    assert 0.02 < flips / (400 * 12) < 0.09
