@@ -111,6 +111,67 @@ def run_reference(args):
 
 
 # --------------------------------------------------------------------------
+class Ranks:
+    """One process per GPU (torchrun env): barrier and max/sum over ranks of
+    host scalars.  Replicas only -- the step itself has no collective."""
+
+    def __init__(self, world, rank, local, backend):
+        import torch
+        self.world, self.rank, self.local, self.backend = world, rank, local, backend
+        self.device = "cpu"
+        if world > 1:
+            import datetime
+            import torch.distributed as dist
+            kw = {}
+            if backend == "nccl":
+                torch.cuda.set_device(local)
+                self.device = torch.device("cuda", local)
+                kw["device_id"] = self.device
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120), **kw)
+        elif backend == "nccl":
+            torch.cuda.set_device(0)
+
+    @classmethod
+    def from_env(cls, backend):
+        return cls(int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
+                   int(os.environ.get("LOCAL_RANK", "0")), backend)
+
+    def barrier(self):
+        if self.world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def _reduce(self, x, op):
+        if self.world == 1:
+            return x
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    def max(self, x):
+        import torch.distributed as dist
+        return self._reduce(x, dist.ReduceOp.MAX)
+
+    def sum(self, x):
+        import torch.distributed as dist
+        return self._reduce(x, dist.ReduceOp.SUM)
+
+    def close(self):
+        if self.world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+def throughput(world, units_per_rank, steps, ms_max):
+    """Whole-job Mpts*steps/s: every rank advanced its own domain `steps`
+    times; the job took the slowest rank's device time."""
+    return world * units_per_rank * steps / (ms_max / 1e3)
+
+
+# --------------------------------------------------------------------------
 class Clocks:
     """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
 
@@ -192,39 +253,13 @@ def timed_steps(torch, flow, steps, profile=False):
 
 def run_ours(args):
     import torch
-    import torch.distributed as dist
     import __graft_entry__
     cf = __graft_entry__.load_package()
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-    else:
-        torch.cuda.set_device(0)
+    rk = Ranks.from_env("nccl")
+    world, rank = rk.world, rk.rank
     dev = torch.cuda.current_device()
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def sum_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+    barrier, max_over_ranks, sum_over_ranks = rk.barrier, rk.max, rk.sum
 
     nx, ny, nz, K, W = args.nx, args.ny, args.nz, args.steps, args.warmup
     units = mpts(nx, ny, nz)
@@ -276,7 +311,7 @@ def run_ours(args):
             e1.synchronize()
             e2e_ms = max_over_ranks(e0.elapsed_time(e1))
             nbytes = sum(t.numel() * 8 for t in pin)
-            results["e2e"] = {"value": world * units * ke / (e2e_ms / 1e3), "unit": UNIT,
+            results["e2e"] = {"value": throughput(world, units, ke, e2e_ms), "unit": UNIT,
                               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes}
         flow.close()
         torch.cuda.synchronize()
@@ -290,7 +325,7 @@ def run_ours(args):
     if rank == 0:
         mix = results["mixed"]
         ms_step = mix["ms_total"] / K
-        value = world * units * K / (mix["ms_total"] / 1e3)
+        value = throughput(world, units, K, mix["ms_total"])
         pk, pk_kind = peaks()
         hbm = float(pk.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
         nxh, n1, nx2, nz2 = nx // 2 + 1, ny + 1, 3 * nx // 2, 3 * nz // 2
@@ -359,15 +394,13 @@ def run_ours(args):
         }
         if "fp64" in results:
             f = results["fp64"]
-            line["value_fp64"] = world * units * K / (f["ms_total"] / 1e3)
+            line["value_fp64"] = throughput(world, units, K, f["ms_total"])
             line["ms_per_step_fp64"] = f["ms_total"] / K
             line["fp64_roofline_step"] = {
                 "achieved": 3 * 20 * nf * 16 / (f["ms_total"] / K / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
                 "frac": 3 * 20 * nf * 16 / (f["ms_total"] / K / 1e3) / 1e9 / hbm}
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    rk.close()
     return 0
 
 
