@@ -320,26 +320,27 @@ struct Impl {
     c->fast_x = regfft_supported(g.nx2);
     if (c->fast_z) {
       const size_t zb = f32 ? 52 * 1024 : 108 * 1024;
+      // z inverse: three blocks per SM with the raw tile and the exchange
       c->fYB1 = 1;
-      for (int yb = 8; yb >= 1; --yb)
-        if (p1_fast_smem(0, g.nz2, f32, yb, g.nxh) <= zb) { c->fYB1 = yb; break; }
+      for (int yb = 4; yb >= 1; --yb)
+        if (p1_fast_smem(0, g.nz2, f32, yb, g.nxh, g.nz) <= 74 * 1024) { c->fYB1 = yb; break; }
       c->fYB3 = 1;
       for (int yb = 4; yb >= 1; --yb)
-        if (p1_fast_smem(2, g.nz2, f32, yb, g.nxh) <= zb) { c->fYB3 = yb; break; }
+        if (p1_fast_smem(2, g.nz2, f32, yb, g.nxh, g.nz) <= zb) { c->fYB3 = yb; break; }
     }
     if (c->fast_x) {
       c->fZR = 1;
       for (int zr : {4, 2})
-        if (g.nz2 % zr == 0 && p1_fast_smem(1, g.nx2, f32, zr, g.nxh) <= budget) { c->fZR = zr; break; }
-      if (p1_fast_smem(1, g.nx2, f32, c->fZR, g.nxh) > 220 * 1024) c->fast_x = false;
+        if (g.nz2 % zr == 0 && p1_fast_smem(1, g.nx2, f32, zr, g.nxh, g.nz) <= budget) { c->fZR = zr; break; }
+      if (p1_fast_smem(1, g.nx2, f32, c->fZR, g.nxh, g.nz) > 220 * 1024) c->fast_x = false;
     }
     if (getenv("CHANFLOW_GENERIC_FFT")) c->fast_x = c->fast_z = false;
     // split x stage: physical planes written once, fluxes read three of them
     c->flux_zr = getenv("CHANFLOW_FLUX_ZR") ? atoi(getenv("CHANFLOW_FLUX_ZR")) : 4;
     if (c->flux_zr != 2) c->flux_zr = 4;
     c->split_x = c->fast_x && !getenv("CHANFLOW_FUSED_XFLUX") && g.nz2 % (f32 ? 16 : 8) == 0 &&
-                 g.nz2 % c->flux_zr == 0 && p1_fast_smem(3, g.nx2, f32, 0, g.nxh) <= 200 * 1024 &&
-                 p1_fast_smem(4, g.nx2, f32, c->flux_zr, g.nxh) <= 200 * 1024;
+                 g.nz2 % c->flux_zr == 0 && p1_fast_smem(3, g.nx2, f32, 0, g.nxh, g.nz) <= 200 * 1024 &&
+                 p1_fast_smem(4, g.nx2, f32, c->flux_zr, g.nxh, g.nz) <= 200 * 1024;
     if (c->split_x &&
         cudaMalloc(&c->P, sizeof(T) * (size_t)(g.ny + 1) * 3 * g.nz2 * g.nx2) != cudaSuccess) {
       cudaGetLastError();

@@ -32,6 +32,6 @@ struct P1Launch {
 int p1_fast_launch(int which, int n, bool f32, const P1Launch& a);
 // shared memory bytes of kernel `which` at length n with its tile parameter
 // (YB for 0/2, ZR for 1 and 4, unused for 3); 0 when unsupported.
-size_t p1_fast_smem(int which, int n, bool f32, int param, int nxh);
+size_t p1_fast_smem(int which, int n, bool f32, int param, int nxh, int nz);
 
 }  // namespace cfd

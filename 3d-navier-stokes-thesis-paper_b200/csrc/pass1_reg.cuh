@@ -38,46 +38,74 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 // --------------------------------------------------------------------------
-// k_zinv_r: grid (nxh, ceil(ny1/YB)), block 256.  Inverse z transform of the
-// 3/2-padded columns (xz_fft_complex_to_real_parallel, PFC/transform.f90:345-368).
+// k_zinv_r: grid (nxh, ceil(ny1/YB)), block zinv_r_threads(N, YB) (one thread
+// per stage-1 task).  Inverse z transform of the 3/2-padded columns
+// (xz_fft_complex_to_real_parallel, PFC/transform.f90:345-368).  The block's
+// input -- YB consecutive planes of all kz and the three components of one kx,
+// contiguous YB-value runs of data1 -- is gathered with cp.async into a raw
+// tile first, so that all of its loads are in flight at once.
+template <int N> __host__ __device__ constexpr int zinv_r_threads(int YB) {
+  return ((3 * YB * Split<N>::N2 + 31) / 32) * 32;
+}
+template <typename T> struct ZRawPad {   // 32 bytes between component blocks
+  static constexpr int V = 32 / (int)sizeof(cplx_t<T>);
+};
+
 template <typename T, int NZ2>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_zinv_r(const cplx_t<T>* __restrict__ vel,
+__global__ void __launch_bounds__(288, sizeof(T) == 4 ? 3 : 1) k_zinv_r(const cplx_t<T>* __restrict__ vel,
                                                 cplx_t<T>* __restrict__ T1, Geom g,
                                                 const cplx_t<T>* __restrict__ twz, int YB) {
   using C = cplx_t<T>;
   constexpr int N1 = Split<NZ2>::N1, N2 = Split<NZ2>::N2, PITCH = N2 + 1, SEQ = SeqPitch<NZ2>::V;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* tw = reinterpret_cast<C*>(smem_raw);
-  C* Y = tw + NZ2;
   const int NZ = g.nz, NY1 = g.ny1, NXH = g.nxh;
+  const int RS = NZ * YB + ZRawPad<T>::V;   // raw stride per component
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  C* raw = tw + NZ2;                         // [c][kz][jj]
+  C* Y = raw + 3 * RS;
   const int kx = blockIdx.x;
   const int j0 = blockIdx.y * YB;
   const int nj = min(YB, NY1 - j0);
   const int nseq = 3 * YB;
+  const C* col = vel + (size_t)kx * NZ * 3 * NY1;
+  {
+    // gather: runs of nj planes at (kz, c), 16-byte pieces when aligned
+    const int rb = nj * (int)sizeof(C);
+    const bool v16 = (rb % 16) == 0 && ((size_t)NY1 * sizeof(C)) % 16 == 0 && ((size_t)j0 * sizeof(C)) % 16 == 0;
+    const int psz = v16 ? 16 : 8, np = rb / psz;
+    for (int idx = threadIdx.x; idx < 3 * NZ * np; idx += blockDim.x) {
+      const int part = idx % np, r = idx / np, kz = r % NZ, c = r / NZ;
+      const char* src = reinterpret_cast<const char*>(col + ((size_t)kz * 3 + c) * NY1 + j0) + part * psz;
+      char* dst = reinterpret_cast<char*>(raw + c * RS + kz * YB) + part * psz;
+      if (v16) cp_async16(dst, src);
+      else cp_async8(dst, src);
+    }
+    cp_async_commit();
+  }
   load_tw2<T, NZ2>(tw, twz);
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   __syncthreads();
   const T half = (T)0.5;
   const bool halve_x = (g.nx2 > g.nx) && (kx == NXH - 1) && (NZ2 > NZ);
-  const C* col = vel + (size_t)kx * NZ * 3 * NY1;
   // stage 1: consecutive threads take consecutive sequences (planes fastest)
   for (int t = threadIdx.x; t < nseq * N2; t += blockDim.x) {
     const int s = t % nseq, n2 = t / nseq;
     const int jj = s % YB, c = s / YB;
+    const C* rc = raw + c * RS + jj;
     C v[N1];
 #pragma unroll
     for (int n1 = 0; n1 < N1; ++n1) {
       const int m = N2 * n1 + n2;
       C x = czero<C>();
       if (jj < nj) {
-        const size_t base = (size_t)c * NY1 + j0 + jj;
         if (NZ2 > NZ) {
-          if (m < NZ / 2) x = col[(size_t)m * 3 * NY1 + base];
-          else if (m == NZ / 2) x = cscale(half, col[(size_t)(NZ / 2) * 3 * NY1 + base]);
-          else if (m == NZ2 - NZ / 2) x = cscale(half, cconj(col[(size_t)(NZ / 2) * 3 * NY1 + base]));
-          else if (m > NZ2 - NZ / 2) x = col[(size_t)(m - (NZ2 - NZ)) * 3 * NY1 + base];
+          if (m < NZ / 2) x = rc[m * YB];
+          else if (m == NZ / 2) x = cscale(half, rc[(NZ / 2) * YB]);
+          else if (m == NZ2 - NZ / 2) x = cscale(half, cconj(rc[(NZ / 2) * YB]));
+          else if (m > NZ2 - NZ / 2) x = rc[(m - (NZ2 - NZ)) * YB];
           if (halve_x) x = cscale(half, x);
         } else {
-          x = col[(size_t)m * 3 * NY1 + base];
+          x = rc[m * YB];
         }
       }
       v[n1] = x;
@@ -758,8 +786,8 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT
 }
 
 // smem sizes (bytes) of the three kernels
-template <typename T, int N> constexpr size_t zinv_r_smem(int YB) {
-  return sizeof(cplx_t<T>) * (N + (size_t)3 * YB * SeqPitch<N>::V);
+template <typename T, int N> size_t zinv_r_smem(int YB, int nz) {
+  return sizeof(cplx_t<T>) * (N + 3 * ((size_t)nz * YB + ZRawPad<T>::V) + (size_t)3 * YB * SeqPitch<N>::V);
 }
 template <typename T, int N> constexpr size_t zfwd_r_smem(int YB) {
   return sizeof(cplx_t<T>) * (N + (size_t)6 * YB * SeqPitch<N>::V);
