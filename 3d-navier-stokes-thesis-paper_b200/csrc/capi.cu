@@ -137,8 +137,10 @@ struct cfg_ctx {
   unsigned long long* cflbits = nullptr;
   double* l2acc = nullptr;
   unsigned long long* divbits = nullptr;
-  // lane-major grid coefficients of k_rhs2 (storage precision)
+  // lane-major grid coefficients of k_rhs2 (storage precision, rhs2_lanes
+  // lanes) and in FP64 for 32 lanes (the FP64 list and the mean mode)
   void* rhs2_tbl = nullptr;
+  void* rhs2_tbl64 = nullptr;
   // crossflow jet (cfg_set_jet): parameters, device walk state
   bool crossflow = false;
   JetParams jp{};
@@ -433,21 +435,42 @@ struct Impl {
     CK(cudaEventRecord(c->ev_fork, c->st));
     CK(cudaStreamWaitEvent(c->st2, c->ev_fork, 0));
     CK(cudaStreamWaitEvent(c->st3, c->ev_fork, 0));
+    const bool v2 = c->use_rhs2 && c->rhs2_tbl64 && mode == 0;
     if (c->n_prec > 0) {
       c->prof_stream = c->st2;
       prof_begin(c, "k_rhs_fp64");
-      k_rhs<double, T, MM><<<c->n_prec, 32, c->sm_rhs64 / 4, c->st2>>>((C*)c->vel, (C*)c->cru, (C*)c->prs,
-                                                                     (const C*)c->cbc + 3 * (size_t)g.nw,
-                                                                     (const C*)c->cbc, g, c->gd, c->sc, c->rkt, rk,
-                                                                     c->p.re, mode, c->wl_prec, c->n_prec);
+      if (v2 && sizeof(T) == 4) {
+        Rhs2Launch a{};
+        a.vel = c->vel; a.cru = c->cru; a.prs = c->prs;
+        a.cbc_top = (const C*)c->cbc + 3 * (size_t)g.nw; a.cbc_bot = c->cbc;
+        a.g = g; a.gd = c->gd; a.sc = c->sc; a.rkt = c->rkt; a.rk = rk; a.re = c->p.re;
+        a.wlist = c->wl_prec; a.nlist = c->n_prec; a.warps = 1; a.lanes = 32; a.tbl = c->rhs2_tbl64;
+        a.st = c->st2;
+        if (rhs2_launch_prec(a) != 0) return fail(c, CFG_E_CUDA, "k_rhs2 (FP64 list) launch");
+      } else {
+        k_rhs<double, T, MM><<<c->n_prec, 32, c->sm_rhs64 / 4, c->st2>>>((C*)c->vel, (C*)c->cru, (C*)c->prs,
+                                                                       (const C*)c->cbc + 3 * (size_t)g.nw,
+                                                                       (const C*)c->cbc, g, c->gd, c->sc, c->rkt, rk,
+                                                                       c->p.re, mode, c->wl_prec, c->n_prec);
+      }
       CKL();
     }
     if (mode == 0) c->mean64_valid = true;
     c->prof_stream = c->st3;
     prof_begin(c, "k_rhs_mean");
-    k_rhs_mean<T, MM><<<1, 32, 0, c->st3>>>((C*)c->vel, (C*)c->cru, (C*)c->prs, c->mvel64, c->mcru64,
-                                           (const C*)c->cbc + 3 * (size_t)g.nw, (const C*)c->cbc, g, c->gd, c->sc,
-                                           c->d_um_dy, c->rkt, rk, c->p.re, c->p.beta, c->p.fix_mass, mode);
+    if (v2) {
+      RhsMeanLaunch m{};
+      m.vel = c->vel; m.cru = c->cru; m.prs = c->prs; m.mvel64 = c->mvel64; m.mcru64 = c->mcru64;
+      m.cbc_top = (const C*)c->cbc + 3 * (size_t)g.nw; m.cbc_bot = c->cbc;
+      m.g = g; m.gd = c->gd; m.sc = c->sc; m.d_um_dy = c->d_um_dy; m.rkt = c->rkt; m.rk = rk;
+      m.re = c->p.re; m.beta = c->p.beta; m.fix_mass = c->p.fix_mass; m.tbl64 = (const double*)c->rhs2_tbl64;
+      m.st = c->st3;
+      if (rhs_mean2_launch(sizeof(T) == 4, m) != 0) return fail(c, CFG_E_CUDA, "k_rhs_mean2 launch");
+    } else {
+      k_rhs_mean<T, MM><<<1, 32, 0, c->st3>>>((C*)c->vel, (C*)c->cru, (C*)c->prs, c->mvel64, c->mcru64,
+                                             (const C*)c->cbc + 3 * (size_t)g.nw, (const C*)c->cbc, g, c->gd, c->sc,
+                                             c->d_um_dy, c->rkt, rk, c->p.re, c->p.beta, c->p.fix_mass, mode);
+    }
     CKL();
     c->prof_stream = nullptr;
     CK(cudaEventRecord(c->ev_join, c->st2));
@@ -816,6 +839,11 @@ int cfg_create(const cfg_params* p, const cfg_grid* gr, cfg_ctx** out) {
     rhs2_table(c->mixed, ny, c->rhs2_lanes, gr->dh, gr->dn, gr->d2h, gr->d2n, ht.data());
     if (cudaMalloc(&c->rhs2_tbl, tb) != cudaSuccess) return bad(CFG_E_NOMEM);
     cudaMemcpy(c->rhs2_tbl, ht.data(), tb, cudaMemcpyHostToDevice);
+    const size_t tb64 = rhs2_table_bytes(false, g.ny1, 32);
+    std::vector<unsigned char> h64(tb64);
+    rhs2_table(false, ny, 32, gr->dh, gr->dn, gr->d2h, gr->d2n, h64.data());
+    if (cudaMalloc(&c->rhs2_tbl64, tb64) != cudaSuccess) return bad(CFG_E_NOMEM);
+    cudaMemcpy(c->rhs2_tbl64, h64.data(), tb64, cudaMemcpyHostToDevice);
   }
   if (cudaDeviceSynchronize() != cudaSuccess) return bad(CFG_E_CUDA);
   *out = c;
@@ -826,7 +854,7 @@ void cfg_destroy(cfg_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->dev);
   if (c->st) cudaStreamSynchronize(c->st);
-  void* bufs[] = {c->dgrid, c->fringe, c->vel, c->cru, c->prs, c->mvel64, c->mcru64, c->T1, c->T2, c->P, c->rhs2_tbl, c->jst, c->cbc,
+  void* bufs[] = {c->dgrid, c->fringe, c->vel, c->cru, c->prs, c->mvel64, c->mcru64, c->T1, c->T2, c->P, c->rhs2_tbl, c->rhs2_tbl64, c->jst, c->cbc,
                   c->sc, c->d_um_dy, c->cflp, c->cflbits, c->l2acc, c->divbits, c->plist, c->pw_H,
                   c->pw_phys, c->pw_phys2, c->pw_in, c->stage, c->twx, c->twz, c->twxs, c->twzs,
                   c->wl_fast, c->wl_prec};

@@ -13,7 +13,7 @@ static int launch_m(const Rhs2Launch& a) {
   const size_t sm = rhs2_smem<T, M, G>(a.warps, a.g.ny1);
   static size_t cur = 48 * 1024;
   if (sm > cur) {
-    if (cudaFuncSetAttribute(k_rhs2<T, M, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) {
+    if (cudaFuncSetAttribute(k_rhs2<T, T, M, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) {
       cudaGetLastError();
       return -2;
     }
@@ -22,7 +22,7 @@ static int launch_m(const Rhs2Launch& a) {
   const int per_block = a.warps * (32 / G);
   dim3 gr((a.nlist + per_block - 1) / per_block);
   using C = cplx_t<T>;
-  k_rhs2<T, M, G><<<gr, 32 * a.warps, sm, a.st>>>((C*)a.vel, (C*)a.cru, (C*)a.prs, (const C*)a.cbc_top,
+  k_rhs2<T, T, M, G><<<gr, 32 * a.warps, sm, a.st>>>((C*)a.vel, (C*)a.cru, (C*)a.prs, (const C*)a.cbc_top,
                                                   (const C*)a.cbc_bot, a.g, a.gd, a.sc, a.rkt, a.rk, a.re, a.wlist,
                                                   a.nlist, (const T*)a.tbl);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
@@ -66,6 +66,60 @@ static int launch_g16(const Rhs2Launch& a) {
     default: return -1;
   }
 }
+
+// FP64 arithmetic over FP32 storage, one warp (one wavenumber) per block
+template <int M>
+static int launch_prec_m(const Rhs2Launch& a) {
+  const size_t sm = rhs2_smem<double, M, 32>(1, a.g.ny1);
+  if (sm > 48 * 1024) return -1;
+  k_rhs2<double, float, M, 32><<<a.nlist, 32, sm, a.st>>>((float2*)a.vel, (float2*)a.cru, (float2*)a.prs,
+                                                         (const float2*)a.cbc_top, (const float2*)a.cbc_bot, a.g, a.gd,
+                                                         a.sc, a.rkt, a.rk, a.re, a.wlist, a.nlist,
+                                                         (const double*)a.tbl);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int rhs2_launch_prec(const Rhs2Launch& a) {
+  const int M = (a.g.ny1 + 31) / 32;
+  switch (M < 2 ? 2 : M) {
+    case 2: return launch_prec_m<2>(a);
+    case 3: return launch_prec_m<3>(a);
+    case 4: return launch_prec_m<4>(a);
+    case 5: return launch_prec_m<5>(a);
+    case 6: return launch_prec_m<6>(a);
+    case 7: return launch_prec_m<7>(a);
+    case 8: return launch_prec_m<8>(a);
+    default: return -1;
+  }
+}
+
+template <typename S, int M>
+static int launch_mean_m(const RhsMeanLaunch& a) {
+  using CS = cplx_t<S>;
+  const size_t sm = rhs_mean2_smem<M>(a.g.ny1);
+  if (sm > 48 * 1024) return -1;
+  k_rhs_mean2<S, M><<<1, 32, sm, a.st>>>((CS*)a.vel, (CS*)a.cru, (CS*)a.prs, a.mvel64, a.mcru64,
+                                         (const CS*)a.cbc_top, (const CS*)a.cbc_bot, a.g, a.gd, a.sc, a.d_um_dy,
+                                         a.rkt, a.rk, a.re, a.beta, a.fix_mass, a.tbl64);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+template <typename S>
+static int launch_mean_t(const RhsMeanLaunch& a) {
+  const int M = (a.g.ny1 + 31) / 32;
+  switch (M < 2 ? 2 : M) {
+    case 2: return launch_mean_m<S, 2>(a);
+    case 3: return launch_mean_m<S, 3>(a);
+    case 4: return launch_mean_m<S, 4>(a);
+    case 5: return launch_mean_m<S, 5>(a);
+    case 6: return launch_mean_m<S, 6>(a);
+    case 7: return launch_mean_m<S, 7>(a);
+    case 8: return launch_mean_m<S, 8>(a);
+    default: return -1;
+  }
+}
+
+int rhs_mean2_launch(bool f32, const RhsMeanLaunch& a) { return f32 ? launch_mean_t<float>(a) : launch_mean_t<double>(a); }
 
 int rhs2_launch(bool f32, const Rhs2Launch& a) {
   if (f32 && a.lanes == 16) return launch_g16(a);

@@ -187,15 +187,18 @@ __host__ __device__ __forceinline__ int rhs2_ld(int n1) { return (n1 + 1) & ~1; 
 // Shared memory per wavenumber: eight columns
 //   0-2 cru (u,v,w), overwritten by the new velocity cv;  3 pressure;
 //   4 pressure correction;  5-7 nonlinear term, overwritten by the next cru.
-template <typename T, int M, int G>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 1) k_rhs2(cplx_t<T>* __restrict__ vel, cplx_t<T>* __restrict__ cru,
-                                              cplx_t<T>* __restrict__ prs,
-                                              const cplx_t<T>* __restrict__ cbc_top,
-                                              const cplx_t<T>* __restrict__ cbc_bot, Geom g,
+// T is the arithmetic precision, S the storage precision of the state (the
+// mixed path runs its |k| < 4 list with T = double over S = float).
+template <typename T, typename S, int M, int G>
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 1) k_rhs2(cplx_t<S>* __restrict__ vel, cplx_t<S>* __restrict__ cru,
+                                              cplx_t<S>* __restrict__ prs,
+                                              const cplx_t<S>* __restrict__ cbc_top,
+                                              const cplx_t<S>* __restrict__ cbc_bot, Geom g,
                                               GridDev gd, const DevScalars* __restrict__ sc, RkTab rkt,
                                               int rk, double re, const int* __restrict__ wlist,
                                               int nlist, const T* __restrict__ tbl) {
   using C = cplx_t<T>;
+  using CS = cplx_t<S>;
   constexpr int GPW = 32 / G;                 // lane groups (wavenumbers) per warp
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -209,31 +212,39 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 1) k_rhs2(cplx_t<T>*
   const int kxi = w / NZ, kzi = w % NZ;
   const T kx = (T)gd.kx[kxi], kz = (T)gd.kz[kzi];
   const T k2 = valid ? (T)(gd.kx[kxi] * gd.kx[kxi] + gd.kz[kzi] * gd.kz[kzi]) : (T)1;
-  C* S = reinterpret_cast<C*>(smem_raw) + (size_t)(warp * GPW + grp) * 8 * LD;
-  C* sV = S;             // 3 columns: cru, then the new velocity cv
-  C* sP = S + 3 * LD;    // pressure
-  C* sH = S + 4 * LD;    // pressure correction
-  C* sN = S + 5 * LD;    // 3 columns: nonlinear term, then the next cru
-  C* gvel = vel + (size_t)w * 3 * n1;
-  C* gcru = cru + (size_t)w * 3 * n1;
-  C* gprs = prs + (size_t)w * n1;
+  C* S_ = reinterpret_cast<C*>(smem_raw) + (size_t)(warp * GPW + grp) * 8 * LD;
+  C* sV = S_;             // 3 columns: cru, then the new velocity cv
+  C* sP = S_ + 3 * LD;    // pressure
+  C* sH = S_ + 4 * LD;    // pressure correction
+  C* sN = S_ + 5 * LD;    // 3 columns: nonlinear term, then the next cru
+  CS* gvel = vel + (size_t)w * 3 * n1;
+  CS* gcru = cru + (size_t)w * 3 * n1;
+  CS* gprs = prs + (size_t)w * n1;
 
   // ---- asynchronous staging of the seven input columns: cru (u,v,w), p, NL (u,v,w)
-  if (valid) {
+  if (valid && sizeof(S) != sizeof(T)) {
+    // widening copy (mixed storage, FP64 arithmetic)
+#pragma unroll
+    for (int col = 0; col < 7; ++col) {
+      const CS* src = (col < 3) ? gcru + col * n1 : (col == 3 ? gprs : gvel + (col - 4) * n1);
+      C* dst = S_ + (col < 4 ? col : col + 1) * LD;
+      for (int j = gl; j < n1; j += G) dst[j] = cvt<C>(src[j]);
+    }
+  } else if (valid) {
     const int cb = (int)(n1 * sizeof(C));
     const bool v16 = (cb % 16) == 0;
     const int csz = v16 ? 16 : 8, nch = cb / csz;
 #pragma unroll
     for (int col = 0; col < 7; ++col) {
       const char* src = reinterpret_cast<const char*>((col < 3) ? gcru + col * n1 : (col == 3 ? gprs : gvel + (col - 4) * n1));
-      char* dst = reinterpret_cast<char*>(S + (col < 4 ? col : col + 1) * LD);
+      char* dst = reinterpret_cast<char*>(S_ + (col < 4 ? col : col + 1) * LD);
       for (int part = gl; part < nch; part += G) {
         if (v16) cp_async16(dst + part * 16, src + part * 16);
         else cp_async8(dst + part * 8, src + part * 8);
       }
     }
   } else {
-    for (int idx = gl; idx < 8 * LD; idx += G) S[idx] = czero<C>();
+    for (int idx = gl; idx < 8 * LD; idx += G) S_[idx] = czero<C>();
   }
   cp_async_commit();
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
@@ -287,10 +298,10 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 1) k_rhs2(cplx_t<T>*
         const int j = gl * M + i;
         if (j == 0) {
           a[i] = 0; b[i] = 1; c[i] = 0;
-          f[0][i] = cbc_bot[w]; f[1][i] = cbc_bot[2 * nw + w];
+          f[0][i] = cvt<C>(cbc_bot[w]); f[1][i] = cvt<C>(cbc_bot[2 * nw + w]);
         } else if (j == n1 - 1) {
           a[i] = 0; b[i] = 1; c[i] = 0;
-          f[0][i] = cbc_top[w]; f[1][i] = cbc_top[2 * nw + w];
+          f[0][i] = cvt<C>(cbc_top[w]); f[1][i] = cvt<C>(cbc_top[2 * nw + w]);
         } else if (j < n1 - 1) {
           a[i] = -vis_imp * rc<T, M, G>(tbl, RC_D2H, i, gl);
           b[i] = -vis_imp * rc<T, M, G>(tbl, RC_D2H + 1, i, gl) + alpha;
@@ -314,8 +325,8 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 1) k_rhs2(cplx_t<T>*
 #pragma unroll
       for (int i = 0; i < M; ++i) {
         const int j = gl * M + i;
-        if (j == 0) { a[i] = 0; b[i] = 1; c[i] = 0; f[0][i] = cbc_bot[nw + w]; }
-        else if (j == ny - 1) { a[i] = 0; b[i] = 1; c[i] = 0; f[0][i] = cbc_top[nw + w]; }
+        if (j == 0) { a[i] = 0; b[i] = 1; c[i] = 0; f[0][i] = cvt<C>(cbc_bot[nw + w]); }
+        else if (j == ny - 1) { a[i] = 0; b[i] = 1; c[i] = 0; f[0][i] = cvt<C>(cbc_top[nw + w]); }
         else if (j < ny - 1) {
           a[i] = -vis_imp * rc<T, M, G>(tbl, RC_D2N, i, gl);
           b[i] = -vis_imp * rc<T, M, G>(tbl, RC_D2N + 1, i, gl) + alpha;
@@ -435,12 +446,151 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 1) k_rhs2(cplx_t<T>*
     const C* acc = (rk < 3) ? sN : sV;
     for (int q = 0; q < 3; ++q)
       for (int j = gl; j < n1; j += G) {
-        gvel[q * n1 + j] = sV[q * LD + j];
-        gcru[q * n1 + j] = acc[q * LD + j];
+        gvel[q * n1 + j] = cvt<CS>(sV[q * LD + j]);
+        gcru[q * n1 + j] = cvt<CS>(acc[q * LD + j]);
       }
-    for (int j = gl; j < n1; j += G) gprs[j] = sP[j];
+    for (int j = gl; j < n1; j += G) gprs[j] = cvt<CS>(sP[j]);
   }
 }
+
+// Mean mode (kx = kz = 0) of the substep with the constant-mass-flux pressure
+// gradient (PFC/pass2.f90:217-263, 356-375), FP64 arithmetic, one warp of 32
+// lanes: the cru and NL columns are staged in shared memory, u and w share
+// one solve (alpha = 1), v takes the wall value.  In mixed precision the FP64
+// mean columns live in mvel64/mcru64 beside the FP32 state.
+template <typename S, int M>
+__global__ void __launch_bounds__(32) k_rhs_mean2(cplx_t<S>* __restrict__ vel, cplx_t<S>* __restrict__ cru,
+                                                  cplx_t<S>* __restrict__ prs, double2* __restrict__ mvel64,
+                                                  double2* __restrict__ mcru64,
+                                                  const cplx_t<S>* __restrict__ cbc_top,
+                                                  const cplx_t<S>* __restrict__ cbc_bot, Geom g, GridDev gd,
+                                                  DevScalars* __restrict__ sc, double* __restrict__ d_um_dy,
+                                                  RkTab rkt, int rk, double re, double beta, int fix_mass,
+                                                  const double* __restrict__ tbl) {
+  using C = double2;
+  using CS = cplx_t<S>;
+  constexpr int G = 32;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x;
+  const int ny = g.ny, n1 = g.ny1, LD = rhs2_ld(n1);
+  const size_t nw = (size_t)g.nw;
+  C* sC = reinterpret_cast<C*>(smem_raw);   // 3 columns: cru
+  C* sN = sC + 3 * LD;                      // 3 columns: nonlinear term
+  C* sV = sN + 3 * LD;                      // 3 columns: new velocity
+  const bool side = (mcru64 != nullptr);
+  for (int q = 0; q < 3; ++q)
+    for (int j = lane; j < n1; j += G) {
+      sC[q * LD + j] = side ? mcru64[q * n1 + j] : cvt<C>(cru[q * n1 + j]);
+      sN[q * LD + j] = cvt<C>(vel[q * n1 + j]);
+    }
+  __syncwarp();
+  const double dt = sc->dt;
+  const double coef = rkt.B(rk) * dt;
+  const double vis_imp = rkt.D(rk) * (dt / re);
+  const double rk_press = (rkt.Cc(rk) + rkt.D(rk)) * dt;
+  const double vis_exp = rkt.Cc(rk) * (dt / re);
+  // cv = cru + coef*cu (+ explicit viscous term on rk1; k = 0)
+  C r[3][M];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const int kd = (q == 1) ? RC_D2N : RC_D2H;
+    const int nq = (q == 1) ? ny : n1;
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      const int j = lane * M + i;
+      C v = make_double2(0.0, 0.0);
+      if (j < n1) {
+        const C cr = sC[q * LD + j], nl = sN[q * LD + j];
+        v = make_double2(cr.x - coef * nl.x, cr.y - coef * nl.y);
+        if (rk == 1 && j < nq) v = cadd(v, cscale(vis_exp, d2c_t<double, M, G>(sC + q * LD, tbl, kd, i, lane, j, nq)));
+      }
+      r[q][i] = v;
+    }
+  }
+  // constant mass flux pressure gradient (cu = -NL)
+  double pg = sc->p_grad;
+  if (fix_mass == 1) {
+    double part = 0;
+    for (int j = 1 + lane; j <= ny - 1; j += G) part += gd.dyh[j] * (-sN[j].x);
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+    pg = -part + 0.5 * (d_um_dy[ny - 1] - d_um_dy[0]) / re;
+  }
+  const double cb = cos(beta) * rk_press * pg, sb = sin(beta) * rk_press * pg;
+  {
+    double a[M], b[M], c[M];
+    C f[2][M];
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      const int j = lane * M + i;
+      if (j == 0) {
+        a[i] = 0; b[i] = 1; c[i] = 0;
+        f[0][i] = cvt<C>(cbc_bot[0]); f[1][i] = cvt<C>(cbc_bot[2 * nw]);
+      } else if (j == n1 - 1) {
+        a[i] = 0; b[i] = 1; c[i] = 0;
+        f[0][i] = cvt<C>(cbc_top[0]); f[1][i] = cvt<C>(cbc_top[2 * nw]);
+      } else if (j < n1 - 1) {
+        a[i] = -vis_imp * rc<double, M, G>(tbl, RC_D2H, i, lane);
+        b[i] = -vis_imp * rc<double, M, G>(tbl, RC_D2H + 1, i, lane) + 1.0;
+        c[i] = -vis_imp * rc<double, M, G>(tbl, RC_D2H + 2, i, lane);
+        f[0][i] = make_double2(r[0][i].x - cb, r[0][i].y);
+        f[1][i] = make_double2(r[2][i].x - sb, r[2][i].y);
+      } else {
+        a[i] = 0; b[i] = 1; c[i] = 0;
+        f[0][i] = make_double2(0.0, 0.0); f[1][i] = make_double2(0.0, 0.0);
+      }
+    }
+    tri_group_solve<double, M, G, 2>(a, b, c, f, lane);
+    const C vb = cvt<C>(cbc_bot[nw]);
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      const int j = lane * M + i;
+      if (j < n1) {
+        sV[j] = f[0][i];
+        sV[2 * LD + j] = f[1][i];
+        sV[LD + j] = (j < ny) ? vb : make_double2(0.0, 0.0);
+      }
+    }
+  }
+  __syncwarp();
+  // next-substep accumulator (PFC/pass2.f90:312-333) and the stores
+  const double coef2 = (rk < 3) ? dt * rkt.A(rk + 1) : 0.0;
+  const double vis_exp2 = (rk < 3) ? (dt / re) * rkt.Cc(rk + 1) : 0.0;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const int kd = (q == 1) ? RC_D2N : RC_D2H;
+    const int nq = (q == 1) ? ny : n1;
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      const int j = lane * M + i;
+      if (j >= n1) continue;
+      const C cv = sV[q * LD + j];
+      C v = cv;
+      if (rk < 3) {
+        const C nl = sN[q * LD + j];
+        v = make_double2(cv.x - coef2 * nl.x, cv.y - coef2 * nl.y);
+        if (j < nq) v = cadd(v, cscale(vis_exp2, d2c_t<double, M, G>(sV + q * LD, tbl, kd, i, lane, j, nq)));
+      }
+      cru[q * n1 + j] = cvt<CS>(v);
+      if (side) mcru64[q * n1 + j] = v;
+    }
+  }
+  for (int q = 0; q < 3; ++q)
+    for (int j = lane; j < n1; j += G) {
+      const C v = sV[q * LD + j];
+      vel[q * n1 + j] = cvt<CS>(v);
+      if (side) mvel64[q * n1 + j] = v;
+    }
+  for (int j = lane; j < n1; j += G) prs[j] = cvt<CS>(make_double2(0.0, 0.0));
+  if (lane == 0) {
+    sc->p_grad = pg;
+    const double* dm = gd.dm;
+    d_um_dy[0] = dm[0] * sV[0].x + dm[1] * sV[1].x + dm[2] * sV[2].x;
+    d_um_dy[ny - 1] = dm[3] * sV[ny - 2].x + dm[4] * sV[ny - 1].x + dm[5] * sV[ny].x;
+  }
+  for (int j = 1 + lane; j <= ny - 2; j += G) d_um_dy[j] = gd.dn[j] * (sV[j + 1].x - sV[j].x);
+}
+
+template <int M> size_t rhs_mean2_smem(int n1) { return sizeof(double2) * 9 * (size_t)rhs2_ld(n1); }
 
 template <typename T, int M, int G>
 size_t rhs2_smem(int warps, int n1) {

@@ -26,6 +26,27 @@ struct Rhs2Launch {
 
 // 0 on success, -1 unsupported size, -2 launch error
 int rhs2_launch(bool f32, const Rhs2Launch& a);
+// the mixed path's |k| < 4 list: FP64 arithmetic over FP32 storage, tbl the
+// FP64 table for 32 lanes
+int rhs2_launch_prec(const Rhs2Launch& a);
+
+// the mean mode (k_rhs_mean2)
+struct RhsMeanLaunch {
+  void *vel, *cru, *prs;
+  double2 *mvel64, *mcru64;   // FP64 mean columns (mixed), or null
+  const void *cbc_top, *cbc_bot;
+  Geom g;
+  GridDev gd;
+  DevScalars* sc;
+  double* d_um_dy;
+  RkTab rkt;
+  int rk;
+  double re, beta;
+  int fix_mass;
+  const double* tbl64;        // FP64 coefficient table for 32 lanes
+  cudaStream_t st;
+};
+int rhs_mean2_launch(bool f32, const RhsMeanLaunch& a);
 bool rhs2_supported(int ny1);
 // the lane-major grid-coefficient table the kernel reads (host side)
 size_t rhs2_table_bytes(bool f32, int ny1, int lanes);
