@@ -2,4 +2,5 @@
 nonlinear products and per-wavenumber implicit y-solves of the reference
 Fortran solver, behind the C ABI of include/chanflow.h."""
 from .chanflow import (FP64, MIXED, CfgJet, ChanflowError, ChannelFlow, Grid, initial_field,  # noqa: F401
-                       load_library, read_flow_dat, LIB_PATH, SYMBOLS)
+                       load_library, read_flow_dat, read_velocity_file, save_velocity_file, LIB_PATH,
+                       SYMBOLS)

@@ -121,6 +121,10 @@ SYMBOLS = {
     "cfg_small_c2r": (C.c_int, [_VP, _VP, _VP, C.c_int]),
     "cfg_l2_norm": (C.c_int, [_VP, _DP, _DP]),
     "cfg_arnoldi_matvec": (C.c_int, [_VP, C.c_int, _VP, _VP]),
+    "cfg_save_velocity": (C.c_int, [_VP, C.c_char_p]),
+    "cfg_read_velocity": (C.c_int, [_VP, C.c_char_p]),
+    "cfg_write_vtk": (C.c_int, [_VP, C.c_char_p]),
+    "cfg_wait_io": (C.c_int, [_VP]),
     "cfg_set_jet": (C.c_int, [_VP, C.POINTER(CfgJet)]),
     "cfg_jet_profile": (C.c_int, [_VP, C.c_double, C.c_double]),
     "cfg_get_jet_forcing": (C.c_int, [_VP, _VP, _VP]),
@@ -142,6 +146,10 @@ SYMBOLS = {
     "cfh_initial_field": (C.c_int, [C.POINTER(CfhGrid), C.c_int, C.c_ulonglong, C.c_double,
                                     C.c_double, _VP]),
     "cfh_rng_u01": (C.c_double, [C.c_ulonglong, C.c_int, C.c_int, C.c_int, C.c_int]),
+    "cfh_save_velocity": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                    C.c_double, C.c_double, _VP, C.c_char_p, C.c_int]),
+    "cfh_read_velocity": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                    _DP, _DP, _VP, C.c_char_p, C.c_int]),
 }
 
 _lib = None
@@ -238,6 +246,33 @@ def read_flow_dat(path):
     if r != 0:
         raise ChanflowError(err.value.decode())
     return run
+
+
+def save_velocity_file(path, data1, lx, lz, re, dt, t_total):
+    """Write a host data1 (nz, nx/2+1, ny+1, 3) as the reference's restart
+    file (read_write::save_velocity, PFC/read_write.f90:211-292)."""
+    L = load_library()
+    d = np.asfortranarray(data1, dtype=np.complex128)
+    nz, nxh, n1, _ = d.shape
+    err = C.create_string_buffer(256)
+    r = L.cfh_save_velocity(os.fsencode(path), 2 * (nxh - 1), n1 - 1, nz, lx, lz, re, dt, t_total,
+                            d.ctypes.data, err, 256)
+    if r != 0:
+        raise ChanflowError(err.value.decode())
+
+
+def read_velocity_file(path, nx, ny, nz, lx, lz, re):
+    """Read a restart file with read_velocity's checks; returns
+    (data1, dt, t_total)."""
+    L = load_library()
+    d = np.zeros((nz, nx // 2 + 1, ny + 1, 3), np.complex128, order="F")
+    dt, t = C.c_double(), C.c_double()
+    err = C.create_string_buffer(256)
+    r = L.cfh_read_velocity(os.fsencode(path), nx, ny, nz, lx, lz, re, C.byref(dt), C.byref(t), d.ctypes.data,
+                            err, 256)
+    if r != 0:
+        raise ChanflowError(err.value.decode())
+    return d, dt.value, t.value
 
 
 class ChannelFlow:
@@ -376,6 +411,26 @@ class ChannelFlow:
         w = np.zeros(shape, order="F")
         self._chk(self.L.cfg_arnoldi_matvec(self.h, int(tend), _p(vv), _p(w)))
         return w if np.ndim(v) == 4 else w.ravel(order="F")
+
+    def save_velocity(self, path, wait=False):
+        """read_write::save_velocity: the restart file of the current data1,
+        written in the background (wait_io() or the next output waits)."""
+        self._chk(self.L.cfg_save_velocity(self.h, os.fsencode(path)))
+        if wait:
+            self.wait_io()
+
+    def read_velocity(self, path):
+        """read_write::read_velocity: data1, t_total (and dt if dt_flag)."""
+        self._chk(self.L.cfg_read_velocity(self.h, os.fsencode(path)))
+
+    def write_vtk(self, path, wait=False):
+        """The VTK velocity snapshot of output_hdf_dfsd (background write)."""
+        self._chk(self.L.cfg_write_vtk(self.h, os.fsencode(path)))
+        if wait:
+            self.wait_io()
+
+    def wait_io(self):
+        self._chk(self.L.cfg_wait_io(self.h))
 
     def set_jet(self, jet):
         """crossflow = 1 with a CfgJet (jet_profile every substep), or None."""

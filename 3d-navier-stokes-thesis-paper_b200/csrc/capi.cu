@@ -8,6 +8,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "chanflow.h"
@@ -15,9 +16,11 @@
 #include "pass2.cuh"
 #include "pass1_fast.h"
 #include "arnoldi.cuh"
+#include "io.cuh"
 #include "jet.cuh"
 #include "pass2v2.h"
 #include "planes.cuh"
+#include "restart.h"
 #include "regfft.cuh"
 
 using namespace cfd;
@@ -113,6 +116,20 @@ struct cfg_ctx {
   // main per-wavenumber kernel; joined back with events
   cudaStream_t st2 = nullptr, st3 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join3 = nullptr;
+  // background file output (restart file, VTK snapshot): the layout kernel
+  // runs on st, the copy to pinned host memory on st_io, the file write on
+  // io_thread
+  cudaStream_t st_io = nullptr;
+  cudaEvent_t ev_io_start = nullptr, ev_io_done = nullptr;
+  void* io_dev = nullptr;
+  void* io_host = nullptr;
+  size_t io_bytes = 0;
+  DevScalars* sc_snap = nullptr;   // device copy of the scalars at the snapshot
+  DevScalars* sc_host = nullptr;   // pinned
+  std::thread io_thread;
+  int io_status = 0;
+  std::string io_err;
+  std::vector<double> hyh;
   cudaStream_t prof_stream = nullptr;
   std::string err;
   long long launches = 0;
@@ -755,6 +772,7 @@ int cfg_create(const cfg_params* p, const cfg_grid* gr, cfg_ctx** out) {
   }
   memcpy(c->hdm, gr->dm, sizeof(double) * 12);
   c->hdy.assign(gr->dy, gr->dy + n1);
+  c->hyh.assign(gr->yh, gr->yh + n1);
   // state and work buffers
   const size_t cs = csize(c), nf = (size_t)g.nw * 3 * n1;
   const size_t t1 = (size_t)n1 * 3 * g.nxh * g.nz2, t2 = (size_t)n1 * 6 * g.nxh * g.nz2;
@@ -853,7 +871,16 @@ int cfg_create(const cfg_params* p, const cfg_grid* gr, cfg_ctx** out) {
 void cfg_destroy(cfg_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->dev);
+  if (c->io_thread.joinable()) c->io_thread.join();
   if (c->st) cudaStreamSynchronize(c->st);
+  if (c->st_io) cudaStreamSynchronize(c->st_io);
+  if (c->io_dev) cudaFree(c->io_dev);
+  if (c->sc_snap) cudaFree(c->sc_snap);
+  if (c->io_host) cudaFreeHost(c->io_host);
+  if (c->sc_host) cudaFreeHost(c->sc_host);
+  if (c->ev_io_start) cudaEventDestroy(c->ev_io_start);
+  if (c->ev_io_done) cudaEventDestroy(c->ev_io_done);
+  if (c->st_io) cudaStreamDestroy(c->st_io);
   void* bufs[] = {c->dgrid, c->fringe, c->vel, c->cru, c->prs, c->mvel64, c->mcru64, c->T1, c->T2, c->P, c->rhs2_tbl, c->rhs2_tbl64, c->jst, c->cbc,
                   c->sc, c->d_um_dy, c->cflp, c->cflbits, c->l2acc, c->divbits, c->plist, c->pw_H,
                   c->pw_phys, c->pw_phys2, c->pw_in, c->stage, c->twx, c->twz, c->twxs, c->twzs,
@@ -1424,3 +1451,162 @@ int cfg_arnoldi_matvec(cfg_ctx* c, int tend, const double* v, double* w) {
   CK(cudaStreamSynchronize(c->st));
   return cfg_status(c);
 }
+
+// ---------------------------------------------------------------------------
+// Restart file and VTK snapshot (PFC/read_write.f90:21-292, 296-500)
+
+int cfg_wait_io(cfg_ctx* c) {
+  if (!c) return CFG_E_ARG;
+  if (c->io_thread.joinable()) c->io_thread.join();
+  const int r = c->io_status;
+  c->io_status = 0;
+  if (r) {
+    c->err = c->io_err;
+    fprintf(stderr, "chanflow: %s\n", c->io_err.c_str());
+  }
+  return r;
+}
+
+// device and pinned host buffers of the background output, grown on demand
+static int ensure_io(cfg_ctx* c, size_t bytes) {
+  if (!c->st_io) {
+    CK(cudaStreamCreateWithFlags(&c->st_io, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&c->ev_io_start, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->ev_io_done, cudaEventDisableTiming));
+    CK(cudaMalloc(&c->sc_snap, sizeof(DevScalars)));
+    CK(cudaMallocHost(&c->sc_host, sizeof(DevScalars)));
+  }
+  if (c->io_bytes >= bytes) return CFG_OK;
+  CK(cudaStreamSynchronize(c->st_io));
+  if (c->io_dev) cudaFree(c->io_dev);
+  if (c->io_host) cudaFreeHost(c->io_host);
+  c->io_dev = c->io_host = nullptr;
+  c->io_bytes = 0;
+  if (cudaMalloc(&c->io_dev, bytes) != cudaSuccess || cudaMallocHost(&c->io_host, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(c, CFG_E_NOMEM, "output buffers of %zu bytes", bytes);
+  }
+  c->io_bytes = bytes;
+  return CFG_OK;
+}
+
+// after the layout kernel on st: snapshot the scalars, copy the io buffer to
+// the host on st_io and start the file writer, which waits for that copy
+template <typename F>
+static int start_io(cfg_ctx* c, size_t bytes, F write) {
+  CK(cudaMemcpyAsync(c->sc_snap, c->sc, sizeof(DevScalars), cudaMemcpyDeviceToDevice, c->st));
+  CK(cudaEventRecord(c->ev_io_start, c->st));
+  CK(cudaStreamWaitEvent(c->st_io, c->ev_io_start, 0));
+  CK(cudaMemcpyAsync(c->io_host, c->io_dev, bytes, cudaMemcpyDeviceToHost, c->st_io));
+  CK(cudaMemcpyAsync(c->sc_host, c->sc_snap, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->st_io));
+  CK(cudaEventRecord(c->ev_io_done, c->st_io));
+  const int dev = c->dev;
+  c->io_thread = std::thread([c, dev, write]() {
+    cudaSetDevice(dev);
+    if (cudaEventSynchronize(c->ev_io_done) != cudaSuccess) {
+      c->io_status = CFG_E_CUDA;
+      c->io_err = "output copy failed";
+      return;
+    }
+    std::string why;
+    c->io_status = write(why);
+    c->io_err = why;
+  });
+  return CFG_OK;
+}
+
+int cfg_save_velocity(cfg_ctx* c, const char* path) {
+  if (!c || !path) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  int r = cfg_wait_io(c);
+  if (r) return r;
+  const Geom& g = c->g;
+  const size_t nf = (size_t)g.nw * 3 * g.ny1, bytes = nf * sizeof(double2);
+  r = ensure_io(c, bytes);
+  if (r) return r;
+  if (c->mixed)
+    k_restart_out<float><<<grid1d(nf), 256, 0, c->st>>>((const float2*)c->vel, c->mean64_valid ? c->mvel64 : nullptr,
+                                                        (double2*)c->io_dev, g);
+  else
+    k_restart_out<double><<<grid1d(nf), 256, 0, c->st>>>((const double2*)c->vel, nullptr, (double2*)c->io_dev, g);
+  CKL();
+  const std::string p(path);
+  const cfg_params prm = c->p;
+  return start_io(c, bytes, [c, p, prm](std::string& why) {
+    return cfd_io::write_restart_slabs(p.c_str(), prm.nx, prm.ny, prm.nz, prm.lx, prm.lz, prm.re, c->sc_host->dt,
+                                       c->sc_host->t_total, (const double*)c->io_host, why);
+  });
+}
+
+int cfg_read_velocity(cfg_ctx* c, const char* path) {
+  if (!c || !path) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  int r = cfg_wait_io(c);
+  if (r) return r;
+  const Geom& g = c->g;
+  const size_t nf = (size_t)g.nw * 3 * g.ny1, bytes = nf * sizeof(double2);
+  r = ensure_io(c, bytes);
+  if (r) return r;
+  CK(cudaStreamSynchronize(c->st_io));
+  double dt = 0, t_total = 0;
+  std::string why;
+  r = cfd_io::read_restart_slabs(path, c->p.nx, c->p.ny, c->p.nz, c->p.lx, c->p.lz, c->p.re, &dt, &t_total,
+                                 (double*)c->io_host, why);
+  if (r) return fail(c, r, "%s", why.c_str());
+  CK(cudaMemcpyAsync(c->io_dev, c->io_host, bytes, cudaMemcpyHostToDevice, c->st));
+  if (c->mixed)
+    k_restart_in<float><<<grid1d(nf), 256, 0, c->st>>>((const double2*)c->io_dev, (float2*)c->vel, c->mvel64, g);
+  else
+    k_restart_in<double><<<grid1d(nf), 256, 0, c->st>>>((const double2*)c->io_dev, (double2*)c->vel, nullptr, g);
+  CKL();
+  c->mean64_valid = true;
+  // t_total from the file; dt too when dt_flag (PFC/read_write.f90:75-79)
+  DevScalars h;
+  CK(cudaMemcpyAsync(&h, c->sc, sizeof(h), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  h.t_total = t_total;
+  if (c->p.dt_flag == 1) h.dt = dt;
+  CK(cudaMemcpyAsync(c->sc, &h, sizeof(h), cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return CFG_OK;
+}
+
+int cfg_write_vtk(cfg_ctx* c, const char* path) {
+  if (!c || !path) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  int r = cfg_wait_io(c);
+  if (r) return r;
+  const Geom& g = c->g;
+  const int np = 3 * g.ny1;
+  const size_t nvec = (size_t)g.nx * g.ny1 * g.nz * 3, bytes = nvec * 4;
+  const size_t nspec = (size_t)g.nw * np, nh = (size_t)np * g.nxh * g.nz;
+  r = ensure_io(c, bytes);
+  if (r) return r;
+  PlaneIn L{(size_t)g.nw, 0, (size_t)g.nz, 1, 1};
+  if (c->mixed) {
+    using C = float2;
+    k_vtk_planes<float><<<grid1d(nspec), 256, 0, c->st>>>((const C*)c->vel, c->mean64_valid ? c->mvel64 : nullptr,
+                                                          (C*)c->T1, g);
+    CKL();
+    float* phys = (float*)((C*)c->T2 + nh);
+    r = Impl<float>::small_c2r(c, (const C*)c->T1, L, np, phys, (C*)c->T2);
+    if (r) return r;
+    k_vtk_pack<float><<<grid1d(nvec), 256, 0, c->st>>>(phys, (uint32_t*)c->io_dev, g.nx, g.ny1, g.nz);
+  } else {
+    using C = double2;
+    k_vtk_planes<double><<<grid1d(nspec), 256, 0, c->st>>>((const C*)c->vel, nullptr, (C*)c->T1, g);
+    CKL();
+    double* phys = (double*)((C*)c->T2 + nh);
+    r = Impl<double>::small_c2r(c, (const C*)c->T1, L, np, phys, (C*)c->T2);
+    if (r) return r;
+    k_vtk_pack<double><<<grid1d(nvec), 256, 0, c->st>>>(phys, (uint32_t*)c->io_dev, g.nx, g.ny1, g.nz);
+  }
+  CKL();
+  const std::string p(path);
+  const cfg_params prm = c->p;
+  return start_io(c, bytes, [c, p, prm](std::string& why) {
+    return cfd_io::write_vtk(p.c_str(), prm.nx, prm.ny, prm.nz, prm.lx, prm.lz, c->hyh.data(),
+                             (const unsigned char*)c->io_host, why);
+  });
+}
+

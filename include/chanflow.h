@@ -201,6 +201,32 @@ int cfg_remove_initial_divergence(cfg_ctx *c);
  * selects nonlinear_linearized as in arnoldi.f90:528-535. */
 int cfg_compute_initial_pressure(cfg_ctx *c, int linearized);
 
+/* Output that does not stall the step.  Each call converts the device state
+ * to the file's order with one kernel on the context stream, copies it to
+ * pinned host memory on a second stream and writes the file on a host thread;
+ * it returns at once and later steps may be issued meanwhile.  At most one
+ * write is in flight: the next output call (or cfg_wait_io) waits for it.
+ * cfg_wait_io returns that write's status (CFG_E_ARG with the message in
+ * cfg_last_error on an I/O failure).  cfg_destroy waits too.
+ *
+ * read_write::save_velocity (PFC/read_write.f90:211-292): the restart file
+ * (Fortran unformatted sequential: header NX, NY, NZ, LX, LZ, RE, DT,
+ * T_TOTAL; one record per kx with data1(1:nz, kx, 1:ny+1, 1:3); a closing
+ * record 0, 0), DT and T_TOTAL taken at the call. */
+int cfg_save_velocity(cfg_ctx *c, const char *path);
+/* read_write::output_hdf_dfsd's VTK snapshot (PFC/read_write.f90:296-500,
+ * xskip = yskip = zskip = 1): u, v, w on the nx x (ny+1) x nz grid of
+ * (x, yh, z) points -- v averaged onto yh, small_fft_complex_to_real per
+ * plane -- as a legacy binary big-endian float32 rectilinear grid. */
+int cfg_write_vtk(cfg_ctx *c, const char *path);
+int cfg_wait_io(cfg_ctx *c);
+/* read_write::read_velocity (PFC/read_write.f90:21-209): checks NX, NY, NZ,
+ * LX, LZ against the context (CFG_E_ARG with the reference's message),
+ * reports a changed RE on stderr, uploads data1 and sets t_total (and dt
+ * when dt_flag).  The caller then removes the divergence and computes the
+ * initial pressure as define_initial_field does.  Synchronous. */
+int cfg_read_velocity(cfg_ctx *c, const char *path);
+
 /* Bulk flux Q = sum dyh*Re(u_mean) (PFC/pass2.f90:106-108) and the maximum
  * |divergence| over all wavenumbers (check_divergence, :380-419). */
 int cfg_diagnostics(cfg_ctx *c, double *bulk_flux, double *max_divergence);

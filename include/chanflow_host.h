@@ -62,6 +62,21 @@ int cfh_define_grid(cfh_grid *g, double lx, double lz, double stretch, int unifo
 int cfh_initial_field(const cfh_grid *g, int which_test, unsigned long long seed,
                       double ampl, double beta, double *data1);
 
+/* read_write::save_velocity / read_velocity (PFC/read_write.f90:21-292) on
+ * host arrays in data1 layout (nz, nx/2+1, ny+1, 3): the reference's restart
+ * file, Fortran unformatted sequential (4-byte record markers, native byte
+ * order): a header record NX, NY, NZ, LX, LZ, RE, DT, T_TOTAL, one record
+ * per kx holding data1(1:nz, kx, 1:ny+1, 1:3), and a closing record 0, 0
+ * (no dynamic SGS coefficients).  cfh_read_velocity applies read_velocity's
+ * checks (NX, NY, NZ equal; LX, LZ within EPSILON) and returns CFG_E_ARG
+ * with the reference's message in err otherwise; a changed RE is reported
+ * on stderr and accepted, as the reference does.  It returns the file's DT
+ * and T_TOTAL (the caller keeps its own dt unless dt_flag, :75-78). */
+int cfh_save_velocity(const char *path, int nx, int ny, int nz, double lx, double lz, double re,
+                      double dt, double t_total, const double *data1, char *err, int errlen);
+int cfh_read_velocity(const char *path, int nx, int ny, int nz, double lx, double lz, double re,
+                      double *dt, double *t_total, double *data1, char *err, int errlen);
+
 /* The seeded counter-based generator replacing RANDOM_NUMBER. */
 double cfh_rng_u01(unsigned long long seed, int x, int z, int j, int col);
 
