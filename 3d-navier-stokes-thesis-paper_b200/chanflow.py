@@ -125,6 +125,8 @@ SYMBOLS = {
     "cfg_read_velocity": (C.c_int, [_VP, C.c_char_p]),
     "cfg_write_vtk": (C.c_int, [_VP, C.c_char_p]),
     "cfg_wait_io": (C.c_int, [_VP]),
+    "cfg_write_vtk_derived": (C.c_int, [_VP, C.c_char_p]),
+    "cfg_plane_statistics": (C.c_int, [_VP, _VP]),
     "cfg_set_jet": (C.c_int, [_VP, C.POINTER(CfgJet)]),
     "cfg_jet_profile": (C.c_int, [_VP, C.c_double, C.c_double]),
     "cfg_get_jet_forcing": (C.c_int, [_VP, _VP, _VP]),
@@ -428,6 +430,19 @@ class ChannelFlow:
         self._chk(self.L.cfg_write_vtk(self.h, os.fsencode(path)))
         if wait:
             self.wait_io()
+
+    def write_vtk_derived(self, path, wait=False):
+        """The snapshot plus vorticity, Q-criterion and discriminant."""
+        self._chk(self.L.cfg_write_vtk_derived(self.h, os.fsencode(path)))
+        if wait:
+            self.wait_io()
+
+    def plane_statistics(self):
+        """(ny+1, 27) per-plane moments of velocity and vorticity (see
+        include/chanflow.h, cfg_plane_statistics)."""
+        out = np.zeros((self.ny + 1, 27), order="F")
+        self._chk(self.L.cfg_plane_statistics(self.h, _p(out)))
+        return out
 
     def wait_io(self):
         self._chk(self.L.cfg_wait_io(self.h))

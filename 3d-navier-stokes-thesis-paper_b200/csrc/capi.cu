@@ -130,6 +130,10 @@ struct cfg_ctx {
   int io_status = 0;
   std::string io_err;
   std::vector<double> hyh;
+  // post-processing: y-derivative weights/stencils on yh, per-plane sums
+  double* pp_wy = nullptr;
+  int* pp_sy = nullptr;
+  double* pp_acc = nullptr;
   cudaStream_t prof_stream = nullptr;
   std::string err;
   long long launches = 0;
@@ -881,7 +885,7 @@ void cfg_destroy(cfg_ctx* c) {
   if (c->ev_io_start) cudaEventDestroy(c->ev_io_start);
   if (c->ev_io_done) cudaEventDestroy(c->ev_io_done);
   if (c->st_io) cudaStreamDestroy(c->st_io);
-  void* bufs[] = {c->dgrid, c->fringe, c->vel, c->cru, c->prs, c->mvel64, c->mcru64, c->T1, c->T2, c->P, c->rhs2_tbl, c->rhs2_tbl64, c->jst, c->cbc,
+  void* bufs[] = {c->dgrid, c->fringe, c->vel, c->cru, c->prs, c->mvel64, c->mcru64, c->T1, c->T2, c->P, c->rhs2_tbl, c->rhs2_tbl64, c->jst, c->pp_wy, c->pp_sy, c->pp_acc, c->cbc,
                   c->sc, c->d_um_dy, c->cflp, c->cflbits, c->l2acc, c->divbits, c->plist, c->pw_H,
                   c->pw_phys, c->pw_phys2, c->pw_in, c->stage, c->twx, c->twz, c->twxs, c->twzs,
                   c->wl_fast, c->wl_prec};
@@ -1606,7 +1610,131 @@ int cfg_write_vtk(cfg_ctx* c, const char* path) {
   const cfg_params prm = c->p;
   return start_io(c, bytes, [c, p, prm](std::string& why) {
     return cfd_io::write_vtk(p.c_str(), prm.nx, prm.ny, prm.nz, prm.lx, prm.lz, c->hyh.data(),
-                             (const unsigned char*)c->io_host, why);
+                             (const unsigned char*)c->io_host, 0, why);
   });
+}
+
+// ---------------------------------------------------------------------------
+// Post-processing: velocity-gradient tensor, vorticity, Q-criterion and
+// discriminant on the snapshot grid, and per-plane moments (the arithmetic of
+// ParaView-Code/DiscriminantFilter.cpd:17 and PFC/stats.f90:120-251)
+
+// 3-point Lagrange first-derivative weights on yh (stats.f90's setup_diff
+// stencils: planes j-1, j, j+1; one-sided at the ends)
+static int ensure_postproc(cfg_ctx* c) {
+  if (c->pp_wy) return CFG_OK;
+  const int n1 = c->g.ny1;
+  std::vector<double> w(3 * n1);
+  std::vector<int> sidx(3 * n1);
+  const std::vector<double>& y = c->hyh;
+  for (int j = 0; j < n1; ++j) {
+    const int a = (j == 0) ? 0 : (j == n1 - 1 ? n1 - 3 : j - 1);
+    const int nd[3] = {a, a + 1, a + 2};
+    const double x0 = y[j];
+    for (int q = 0; q < 3; ++q) {
+      const double xq = y[nd[q]], xr = y[nd[(q + 1) % 3]], xs = y[nd[(q + 2) % 3]];
+      w[3 * j + q] = ((x0 - xr) + (x0 - xs)) / ((xq - xr) * (xq - xs));
+      sidx[3 * j + q] = nd[q];
+    }
+  }
+  CK(cudaMalloc(&c->pp_wy, sizeof(double) * 3 * n1));
+  CK(cudaMalloc(&c->pp_sy, sizeof(int) * 3 * n1));
+  CK(cudaMalloc(&c->pp_acc, sizeof(double) * 30 * n1));
+  CK(cudaMemcpy(c->pp_wy, w.data(), sizeof(double) * 3 * n1, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->pp_sy, sidx.data(), sizeof(int) * 3 * n1, cudaMemcpyHostToDevice));
+  return CFG_OK;
+}
+
+template <typename T>
+static int postproc(cfg_ctx* c, uint32_t* out) {
+  using C = cplx_t<T>;
+  const Geom& g = c->g;
+  const int n1 = g.ny1;
+  const size_t nw = (size_t)g.nw;
+  const double2* m64 = (c->mixed && c->mean64_valid) ? c->mvel64 : nullptr;
+  double* accV = c->pp_acc;
+  double* accW = c->pp_acc + 15 * (size_t)n1;
+  CK(cudaMemsetAsync(c->pp_acc, 0, sizeof(double) * 30 * n1, c->st));
+  // velocity on the yh planes
+  const int np3 = 3 * n1;
+  PlaneIn L{nw, 0, (size_t)g.nz, 1, 1};
+  k_vtk_planes<T><<<grid1d(nw * np3), 256, 0, c->st>>>((const C*)c->vel, m64, (C*)c->T1, g);
+  CKL();
+  T* physU = (T*)((C*)c->T2 + (size_t)np3 * g.nxh * g.nz);
+  int r = Impl<T>::small_c2r(c, (const C*)c->T1, L, np3, physU, (C*)c->T2);
+  if (r) return r;
+  if (out) {
+    k_vtk_pack<T><<<grid1d((size_t)g.nx * n1 * g.nz * 3), 256, 0, c->st>>>(physU, out, g.nx, n1, g.nz);
+    CKL();
+  }
+  k_stats_vel<T><<<dim3(g.nz, n1), 128, 0, c->st>>>(physU, (const C*)c->T1, g.nx, g.nz, n1, nw, accV);
+  CKL();
+  // the gradient tensor in chunks of planes that fit the work arrays
+  const int NP = std::max(1, std::min(32, (int)((size_t)n1 * g.nz2 / (3 * (size_t)g.nz))));
+  for (int p0 = 0; p0 < n1; p0 += NP) {
+    const int np = std::min(NP, n1 - p0);
+    k_grad_spec<T><<<grid1d(nw * 3 * np), 256, 0, c->st>>>((const C*)c->vel, m64, (C*)c->T1, g, c->gd, c->pp_wy,
+                                                           c->pp_sy, p0, np);
+    CKL();
+    T* physA = (T*)((C*)c->T2 + (size_t)9 * np * g.nxh * g.nz);
+    r = Impl<T>::small_c2r(c, (const C*)c->T1, L, 9 * np, physA, (C*)c->T2);
+    if (r) return r;
+    k_derived<T><<<dim3(g.nz, np), 128, 0, c->st>>>(physA, (const C*)c->T1, g.nx, g.nz, n1, nw, p0, out, accW);
+    CKL();
+  }
+  return CFG_OK;
+}
+
+int cfg_write_vtk_derived(cfg_ctx* c, const char* path) {
+  if (!c || !path) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  int r = cfg_wait_io(c);
+  if (r) return r;
+  r = ensure_postproc(c);
+  if (r) return r;
+  const Geom& g = c->g;
+  const size_t npts = (size_t)g.nx * g.ny1 * g.nz, bytes = npts * 8 * 4;
+  r = ensure_io(c, bytes);
+  if (r) return r;
+  r = c->mixed ? postproc<float>(c, (uint32_t*)c->io_dev) : postproc<double>(c, (uint32_t*)c->io_dev);
+  if (r) return r;
+  const std::string p(path);
+  const cfg_params prm = c->p;
+  return start_io(c, bytes, [c, p, prm](std::string& why) {
+    return cfd_io::write_vtk(p.c_str(), prm.nx, prm.ny, prm.nz, prm.lx, prm.lz, c->hyh.data(),
+                             (const unsigned char*)c->io_host, 1, why);
+  });
+}
+
+int cfg_plane_statistics(cfg_ctx* c, double* stats) {
+  if (!c || !stats) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  int r = ensure_postproc(c);
+  if (r) return r;
+  r = c->mixed ? postproc<float>(c, nullptr) : postproc<double>(c, nullptr);
+  if (r) return r;
+  const int n1 = c->g.ny1;
+  std::vector<double> acc(30 * (size_t)n1);
+  CK(cudaMemcpyAsync(acc.data(), c->pp_acc, sizeof(double) * acc.size(), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  const double scale = 1.0 / ((double)c->g.nx * (double)c->g.nz), eps = 2.220446049250313e-16;
+  auto col = [&](int k) { return stats + (size_t)k * n1; };
+  for (int j = 0; j < n1; ++j) {
+    const double* v = &acc[(size_t)j * 15];
+    const double* w = &acc[(size_t)(n1 + j) * 15];
+    for (int q = 0; q < 3; ++q) {
+      const double var = scale * v[q], var_w = scale * w[q];
+      col(q)[j] = v[12 + q];
+      col(3 + q)[j] = var;
+      col(6 + q)[j] = scale * v[3 + q] / (std::pow(var, 1.5) + eps);
+      col(9 + q)[j] = scale * v[6 + q] / (var * var + eps);
+      col(12 + q)[j] = scale * v[9 + q];
+      col(15 + q)[j] = w[12 + q];
+      col(18 + q)[j] = var_w;
+      col(21 + q)[j] = scale * w[3 + q] / (std::pow(var_w, 1.5) + eps);
+      col(24 + q)[j] = scale * w[6 + q] / (var_w * var_w + eps);
+    }
+  }
+  return CFG_OK;
 }
 

@@ -180,7 +180,7 @@ int read_restart_slabs(const char* path, int nx, int ny, int nz, double lx, doub
 }
 
 int write_vtk(const char* path, int nx, int ny, int nz, double lx, double lz, const double* yh,
-              const unsigned char* vec_be, std::string& why) {
+              const unsigned char* vec_be, int derived, std::string& why) {
   FILE* f = std::fopen(path, "wb");
   if (!f) {
     why = std::string("cannot open ") + path + ": " + std::strerror(errno);
@@ -220,6 +220,20 @@ int write_vtk(const char* path, int nx, int ny, int nz, double lx, double lz, co
   ok = ok && std::fwrite(pd.data(), 1, pd.size(), f) == pd.size() &&
        std::fwrite(vec, 1, std::strlen(vec), f) == std::strlen(vec) &&
        std::fwrite(vec_be, 1, npts * 12, f) == npts * 12 && std::fputc('\n', f) != EOF;
+  if (derived) {
+    // vorticity, Q-criterion and discriminant behind the velocity, same
+    // point order (the reference snapshot stops after flowvec)
+    const unsigned char* d = vec_be + npts * 12;
+    const char* vor = "VECTORS vorticity float\n";
+    const char* qh = "SCALARS Q float 1\nLOOKUP_TABLE default\n";
+    const char* dh = "SCALARS D float 1\nLOOKUP_TABLE default\n";
+    ok = ok && std::fwrite(vor, 1, std::strlen(vor), f) == std::strlen(vor) &&
+         std::fwrite(d, 1, npts * 12, f) == npts * 12 && std::fputc('\n', f) != EOF &&
+         std::fwrite(qh, 1, std::strlen(qh), f) == std::strlen(qh) &&
+         std::fwrite(d + npts * 12, 1, npts * 4, f) == npts * 4 && std::fputc('\n', f) != EOF &&
+         std::fwrite(dh, 1, std::strlen(dh), f) == std::strlen(dh) &&
+         std::fwrite(d + npts * 16, 1, npts * 4, f) == npts * 4 && std::fputc('\n', f) != EOF;
+  }
   ok = (std::fclose(f) == 0) && ok;
   if (!ok) {
     why = std::string("write error on ") + path;

@@ -11,8 +11,9 @@ int write_restart_slabs(const char* path, int nx, int ny, int nz, double lx, dou
 int read_restart_slabs(const char* path, int nx, int ny, int nz, double lx, double lz, double re, double* dt,
                        double* t_total, double* slabs, std::string& why);
 // vec_be: nx*(ny+1)*nz*3 big-endian float32 values, (u,v,w) fastest, then x,
-// the plane, z
+// the plane, z; with `derived`, followed by the vorticity (3 per point), Q
+// and D (1 per point) in the same order
 int write_vtk(const char* path, int nx, int ny, int nz, double lx, double lz, const double* yh,
-              const unsigned char* vec_be, std::string& why);
+              const unsigned char* vec_be, int derived, std::string& why);
 
 }  // namespace cfd_io

@@ -219,6 +219,22 @@ int cfg_save_velocity(cfg_ctx *c, const char *path);
  * (x, yh, z) points -- v averaged onto yh, small_fft_complex_to_real per
  * plane -- as a legacy binary big-endian float32 rectilinear grid. */
 int cfg_write_vtk(cfg_ctx *c, const char *path);
+/* Post-processing on the same grid (x, yh, z): the velocity-gradient tensor
+ * A_ij = du_i/dx_j (x and z derivatives spectral, y by 3-point Lagrange
+ * differences on yh -- the stencils of PFC/stats.f90's setup_diff), the
+ * vorticity, the Q-criterion -tr(A^2)/2 and the discriminant
+ * D = (6 (tr A^3)^2 - (tr A^2)^3)/8 of the ParaView Calculator in
+ * ParaView-Code/DiscriminantFilter.cpd:17, computed on the device and
+ * written behind the velocity as VECTORS vorticity, SCALARS Q and SCALARS D
+ * (background write, as cfg_write_vtk). */
+int cfg_write_vtk_derived(cfg_ctx *c, const char *path);
+/* Per-plane moments of one snapshot (compute_velocity_moments and
+ * compute_vorticity_moments, PFC/stats.f90:423-456, with weight 1): stats is
+ * (ny+1, 27) column-major: mean u, v, w; variance; skewness m3/(m2^1.5+eps);
+ * flatness m4/(m2^2+eps); the fluxes <u'v'>, <v'v'>, <w'v'>; then mean,
+ * variance, skewness and flatness of the three vorticity components, on the
+ * planes yh(1..ny+1).  Synchronous. */
+int cfg_plane_statistics(cfg_ctx *c, double *stats);
 int cfg_wait_io(cfg_ctx *c);
 /* read_write::read_velocity (PFC/read_write.f90:21-209): checks NX, NY, NZ,
  * LX, LZ against the context (CFG_E_ARG with the reference's message),

@@ -68,8 +68,25 @@ def parse_vtk(path):
     npts = nx * n1 * nz
     v = np.frombuffer(b, ">f4", 3 * npts, i).astype(np.float32)
     i += 12 * npts
-    assert b[i:] == b"\n"
+    assert b[i:i + 1] == b"\n"
+    i += 1
     # (c, x, plane, z) with c fastest
     out["vel"] = v.reshape((3, nx, n1, nz), order="F").transpose(1, 2, 3, 0)
     out["dims"] = dims
+    # optional further sections: VECTORS name float / SCALARS name float 1
+    while i < len(b):
+        kind, name = line().split()[:2]
+        if kind == "SCALARS":
+            line()   # LOOKUP_TABLE default
+            n = npts
+        else:
+            n = 3 * npts
+        a = np.frombuffer(b, ">f4", n, i).astype(np.float32)
+        i += 4 * n
+        assert b[i:i + 1] == b"\n"
+        i += 1
+        if kind == "SCALARS":
+            out[name] = a.reshape((nx, n1, nz), order="F")
+        else:
+            out[name] = a.reshape((3, nx, n1, nz), order="F").transpose(1, 2, 3, 0)
     return out
