@@ -70,6 +70,15 @@ class CfgJet(C.Structure):
     ]
 
 
+class CfgFringe(C.Structure):
+    """cfg_fringe (include/chanflow.h): init_buffer's parameters."""
+    _fields_ = [
+        ("fringe_gain", C.c_double), ("xfringe", C.c_int), ("zfringe", C.c_int),
+        ("frac_xbuff", C.c_double), ("buff_xrise", C.c_double), ("buff_xfall", C.c_double),
+        ("frac_zbuff", C.c_double),
+    ]
+
+
 class CfhRun(C.Structure):
     _fields_ = [
         ("re", C.c_double), ("ctrlu", C.c_double), ("ctrlw", C.c_double), ("lx", C.c_double),
@@ -87,6 +96,8 @@ class CfhRun(C.Structure):
         ("stretch", C.c_double), ("dt", C.c_double), ("seed", C.c_ulonglong),
         ("precision", C.c_int), ("uniform_grid", C.c_int), ("jet_mode", C.c_int),
         ("jet_width", C.c_double), ("jet_peak", C.c_double), ("jet_freq", C.c_double),
+        ("fringe_gain", C.c_double), ("buff_xrise", C.c_double), ("buff_xfall", C.c_double),
+        ("frac_zbuff", C.c_double), ("buff_zrise", C.c_double), ("buff_zfall", C.c_double),
     ]
 
 
@@ -125,6 +136,8 @@ SYMBOLS = {
     "cfg_read_velocity": (C.c_int, [_VP, C.c_char_p]),
     "cfg_write_vtk": (C.c_int, [_VP, C.c_char_p]),
     "cfg_wait_io": (C.c_int, [_VP]),
+    "cfg_init_buffer": (C.c_int, [_VP, C.POINTER(CfgFringe)]),
+    "cfg_get_buffer": (C.c_int, [_VP, _VP, _VP]),
     "cfg_write_vtk_derived": (C.c_int, [_VP, C.c_char_p]),
     "cfg_plane_statistics": (C.c_int, [_VP, _VP]),
     "cfg_set_jet": (C.c_int, [_VP, C.POINTER(CfgJet)]),
@@ -443,6 +456,19 @@ class ChannelFlow:
         out = np.zeros((self.ny + 1, 27), order="F")
         self._chk(self.L.cfg_plane_statistics(self.h, _p(out)))
         return out
+
+    def init_buffer(self, fringe_gain, xfringe=1, zfringe=0, frac_xbuff=0.1, buff_xrise=0.03,
+                    buff_xfall=0.02, frac_zbuff=0.1):
+        """init_buffer (PFC/init_jet_buffer.f90:358-483) on the device."""
+        f = CfgFringe(fringe_gain, xfringe, zfringe, frac_xbuff, buff_xrise, buff_xfall, frac_zbuff)
+        self._chk(self.L.cfg_init_buffer(self.h, C.byref(f)))
+
+    def buffer(self):
+        """(buffer (nx2, nz2), target_inflow (ny+1, 3)) on the device."""
+        b = np.zeros((self.nx2, self.nz2), order="F")
+        t = np.zeros((self.ny + 1, 3), order="F")
+        self._chk(self.L.cfg_get_buffer(self.h, _p(b), _p(t)))
+        return b, t
 
     def wait_io(self):
         self._chk(self.L.cfg_wait_io(self.h))

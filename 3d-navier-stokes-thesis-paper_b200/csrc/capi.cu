@@ -1738,3 +1738,78 @@ int cfg_plane_statistics(cfg_ctx* c, double* stats) {
   return CFG_OK;
 }
 
+// ---------------------------------------------------------------------------
+// init_buffer (PFC/init_jet_buffer.f90:358-483) on the device
+int cfg_init_buffer(cfg_ctx* c, const cfg_fringe* f) {
+  if (!c || !f) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  const Geom& g = c->g;
+  if (f->xfringe == 0 && f->zfringe == 0) {
+    c->has_fringe = 0;
+    return CFG_OK;
+  }
+  if (!c->fringe && cudaMalloc(&c->fringe, rsize(c) * g.nx2 * g.nz2) != cudaSuccess)
+    return fail(c, CFG_E_NOMEM, "fringe buffer");
+  FringeParams fp{f->xfringe, f->zfringe, f->frac_xbuff, f->buff_xrise, f->buff_xfall, f->frac_zbuff};
+  const size_t np = (size_t)g.nx2 * g.nz2;
+  PlaneIn L{0, 0, (size_t)g.nz, 1, 1};
+  int r;
+  if (c->mixed) {
+    using T = float;
+    using C = float2;
+    k_fringe_profile<T><<<g.nz, 128, 0, c->st>>>((T*)c->pw_phys, fp, g.nx, g.nz, c->p.lx, c->p.lz);
+    CKL();
+    r = Impl<T>::small_r2c(c, (const T*)c->pw_phys, 1, (C*)c->pw_in, 0, g.nz, 1, (C*)c->pw_H);
+    if (r) return r;
+    r = Impl<T>::planes_c2r(c, (const C*)c->pw_in, L, nullptr, 1, (T*)c->pw_phys2);
+    if (r) return r;
+    k_scale_real<T><<<grid1d(np), 256, 0, c->st>>>((const T*)c->pw_phys2, (T*)c->fringe, np, f->fringe_gain);
+  } else {
+    using T = double;
+    using C = double2;
+    k_fringe_profile<T><<<g.nz, 128, 0, c->st>>>((T*)c->pw_phys, fp, g.nx, g.nz, c->p.lx, c->p.lz);
+    CKL();
+    r = Impl<T>::small_r2c(c, (const T*)c->pw_phys, 1, (C*)c->pw_in, 0, g.nz, 1, (C*)c->pw_H);
+    if (r) return r;
+    r = Impl<T>::planes_c2r(c, (const C*)c->pw_in, L, nullptr, 1, (T*)c->pw_phys2);
+    if (r) return r;
+    k_scale_real<T><<<grid1d(np), 256, 0, c->st>>>((const T*)c->pw_phys2, (T*)c->fringe, np, f->fringe_gain);
+  }
+  CKL();
+  // target_inflow for the closed channel: 0.75 (1 - yh^8) (cos beta, 0, sin beta)
+  const int n1 = g.ny1;
+  std::vector<double> tgt(3 * (size_t)n1, 0.0);
+  for (int j = 0; j < n1; ++j) {
+    const double p = 0.75 * (1.0 - std::pow(c->hyh[j], 8));
+    tgt[j] = p * std::cos(c->p.beta);
+    tgt[2 * (size_t)n1 + j] = p * std::sin(c->p.beta);
+  }
+  CK(cudaMemcpyAsync((void*)c->gd.target, tgt.data(), sizeof(double) * tgt.size(), cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  c->has_fringe = 1;
+  return CFG_OK;
+}
+
+int cfg_get_buffer(cfg_ctx* c, double* buffer, double* target_inflow) {
+  if (!c) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  const Geom& g = c->g;
+  const size_t np = (size_t)g.nx2 * g.nz2;
+  if (buffer) {
+    if (!c->has_fringe || !c->fringe) {
+      memset(buffer, 0, sizeof(double) * np);
+    } else if (c->mixed) {
+      std::vector<float> h(np);
+      CK(cudaMemcpyAsync(h.data(), c->fringe, sizeof(float) * np, cudaMemcpyDeviceToHost, c->st));
+      CK(cudaStreamSynchronize(c->st));
+      for (size_t i = 0; i < np; ++i) buffer[i] = h[i];
+    } else {
+      CK(cudaMemcpyAsync(buffer, c->fringe, sizeof(double) * np, cudaMemcpyDeviceToHost, c->st));
+    }
+  }
+  if (target_inflow)
+    CK(cudaMemcpyAsync(target_inflow, c->gd.target, sizeof(double) * 3 * g.ny1, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return CFG_OK;
+}
+

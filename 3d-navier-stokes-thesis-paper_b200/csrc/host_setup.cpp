@@ -88,8 +88,9 @@ int cfh_read_flow_dat(const char* path, cfh_run* r, char* err, int errlen) {
   skip(1); rdi(&r->crossflow); rdi(&r->filter_jet_profile); skip(1); rd(&r->jet_diam); rd(&tmp);
   skip(2); rd(&r->xjet_top); rd(&r->zjet_top); rd(&r->jetmag_top); rd(&r->forcing_top); rd(&r->for_freq_top); rd(&tmp);
   skip(1); rd(&r->xjet_bot); rd(&r->zjet_bot); rd(&r->jetmag_bot); rd(&r->forcing_bot); rd(&r->for_freq_bot); rd(&tmp);
-  skip(1); rd(&tmp); skip(1); rdi(&r->xfringe); rd(&r->frac_xbuff); rd(&tmp); rd(&tmp);
-  skip(1); rdi(&r->zfringe); rd(&tmp); rd(&tmp); rd(&tmp);
+  skip(1); rd(&r->fringe_gain); skip(1); rdi(&r->xfringe); rd(&r->frac_xbuff); rd(&r->buff_xrise);
+  rd(&r->buff_xfall);
+  skip(1); rdi(&r->zfringe); rd(&r->frac_zbuff); rd(&r->buff_zrise); rd(&r->buff_zfall);
   if (!ok) return seterr("flow.dat: missing or malformed value before line 96");
   const double pi = atan2(0.0, -1.0);
   r->beta = r->beta * asin(1.0);

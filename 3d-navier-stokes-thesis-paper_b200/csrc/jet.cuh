@@ -186,4 +186,71 @@ __global__ void k_jet_combine(const cplx_t<T>* __restrict__ spec, cplx_t<T>* __r
   }
 }
 
+// ---------------------------------------------------------------------------
+// init_buffer (PFC/init_jet_buffer.f90:358-483): the fringe profile on the
+// nx x nz grid.  Each direction's band rises and falls with
+// 1/(1+exp(1/t + 1/(t-1))) (define_fringe_region, :453-482); where the x and
+// z bands overlap the two ramps combine through sqrt(tx^2 + tz^2).
+struct FringeParams {
+  int xfringe, zfringe;
+  double frac_xbuff, buff_xrise, buff_xfall, frac_zbuff;
+};
+
+__device__ __forceinline__ void fringe_region(double t, double ts, double tr, double tf, double te, double& f,
+                                              double& f2) {
+  f = 0.0;
+  f2 = 0.0;
+  if (t > ts) {
+    if (t < tr) {
+      const double t2 = (t - ts) / (tr - ts);
+      f = 1.0 / (1.0 + exp(1.0 / t2 + 1.0 / (t2 - 1.0)));
+      f2 = t2;
+    } else if (t > tf && t < te) {
+      const double t2 = (te - t) / (te - tf);
+      f = 1.0 / (1.0 + exp(1.0 / t2 + 1.0 / (t2 - 1.0)));
+      f2 = t2;
+    } else if (t >= te) {
+      f = 0.0;
+    } else {
+      f = 1.0;
+    }
+  }
+}
+
+template <typename T>
+__global__ void k_fringe_profile(T* __restrict__ out, FringeParams fp, int nx, int nz, double lx, double lz) {
+  const int z = blockIdx.x;
+  const double tz = (double)z * lz / (double)nz;
+  double fz = 0.0, fz2 = 0.0;
+  if (fp.zfringe == 1) {
+    double fa, fa2, fb, fb2;
+    fringe_region(tz, -1.0, -1.0, 0.0, fp.frac_zbuff * lz, fa, fa2);
+    fringe_region(tz, lz - fp.frac_zbuff * lz, lz, lz + 1.0, lz + 1.0, fb, fb2);
+    fz = fa + fb;
+    fz2 = fa2 + fb2;
+  }
+  for (int x = threadIdx.x; x < nx; x += blockDim.x) {
+    const double tx = (double)x * lx / (double)nx;
+    double fx = 0.0, fx2 = 0.0;
+    if (fp.xfringe == 1) {
+      const double xs = lx * (1.0 - fp.frac_xbuff);
+      fringe_region(tx, xs, xs + lx * fp.buff_xrise, lx - lx * fp.buff_xfall, lx, fx, fx2);
+    }
+    double v;
+    if (fx < 1.0 && fz < 1.0 && fx * fz > 0.0) {
+      const double t = sqrt(fx2 * fx2 + fz2 * fz2);
+      v = (t < 1.0) ? 1.0 / (1.0 + exp(1.0 / t + 1.0 / (t - 1.0))) : 1.0;
+    } else {
+      v = fmax(fx, fz);
+    }
+    out[(size_t)z * nx + x] = (T)v;
+  }
+}
+
+template <typename T>
+__global__ void k_scale_real(const T* __restrict__ in, T* __restrict__ out, size_t n, double s) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = (T)(s * (double)in[i]);
+}
+
 }  // namespace cfd

@@ -190,6 +190,24 @@ int cfg_jet_profile(cfg_ctx *c, double time, double time_incr);
 /* The current forcing parameters and increments (24 each; NULL skips). */
 int cfg_get_jet_forcing(cfg_ctx *c, double *jet_forcing, double *jet_forcing_incr);
 
+/* Fringe (buffer) region, init_buffer (PFC/init_jet_buffer.f90:358-483),
+ * computed on the device: the nx x nz profile (define_fringe_region ramps
+ * in x and, with zfringe, at both z ends), transformed with
+ * small_fft_real_to_complex and interpolated onto the dealiased nx2 x nz2
+ * grid with xz_fft_complex_to_real, times fringe_gain; target_inflow
+ * (ny+1, 3) = 0.75 (1 - yh^8) (cos beta, 0, sin beta) of the closed
+ * channel.  The nonlinear step then adds buffer*(u - target) (pass1.f90).
+ * xfringe = zfringe = 0 switches the fringe off. */
+typedef struct cfg_fringe {
+  double fringe_gain;
+  int xfringe, zfringe;
+  double frac_xbuff, buff_xrise, buff_xfall;   /* x band: last frac_xbuff of lx */
+  double frac_zbuff;                           /* z bands at both ends */
+} cfg_fringe;
+int cfg_init_buffer(cfg_ctx *c, const cfg_fringe *f);
+/* The device's buffer (nx2, nz2) and target_inflow (ny+1, 3); NULL skips. */
+int cfg_get_buffer(cfg_ctx *c, double *buffer, double *target_inflow);
+
 /* read_write::l2_norm, PFC/read_write.f90:1432-1462: perturbation L2 norm
  * about U=1-y^2 and the wall-shear difference d_um_dy(1)-d_um_dy(ny). */
 int cfg_l2_norm(cfg_ctx *c, double *l2, double *drag);

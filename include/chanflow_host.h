@@ -34,6 +34,8 @@ typedef struct cfh_run {
   int uniform_grid;       /* which_test 6 grid */
   int jet_mode;           /* 0 none, 1 reference tanh jet, 2 gaussian slot */
   double jet_width, jet_peak, jet_freq;
+  /* fringe parameters, flow.dat lines 88-95 */
+  double fringe_gain, buff_xrise, buff_xfall, frac_zbuff, buff_zrise, buff_zfall;
 } cfh_run;
 
 /* Grid operators in reference layout, owned by the caller (sizes as in
