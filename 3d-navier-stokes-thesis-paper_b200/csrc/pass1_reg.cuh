@@ -3,6 +3,7 @@
 // hot-path lengths (48 ... 576).  See pass1.cuh for what each kernel computes
 // and which reference routine it replaces.
 #pragma once
+#include <type_traits>
 #include "cfd_common.cuh"
 #include "pass1.cuh"
 #include "regfft.cuh"
@@ -620,10 +621,12 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT
   C* tw = reinterpret_cast<C*>(smem_raw);   // tw2[q*N2 + n2]
   C* FP = tw + N;                           // [NSEQ][SEQ] padded sequences
   __shared__ T red[3][NW];
+  __shared__ T skx[NX2 / 2 + 2];             // kx of the retained columns (nx/2+1 <= nx2/2+1)
   const int NXH = g.nxh, NZ2 = g.nz2, ny = g.ny;
   const int z0 = blockIdx.x * ZR;
   const int k = 2 + blockIdx.y;
   load_tw2<T, N>(tw, twx);
+  for (int i = threadIdx.x; i < g.nxh; i += NT) skx[i] = (T)gd.kx[i];
   auto px = [](int x) { return (x / N2) * PITCH + (x % N2); };
   const T half = (T)0.5, two = (T)2.0;
   const T dhk = (T)gd.dh[k - 1];
@@ -649,71 +652,83 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT
   const T* Pp = P0 + pstride;
   const size_t cs = (size_t)NZ2 * N;
   T ma = 0, mb = 0, mc = 0;
-  constexpr int IT = (ZR * N + NT - 1) / NT;
-#pragma unroll
-  for (int it = 0; it < IT; ++it) {
-    const int idx = it * NT + (int)threadIdx.x;
-    if ((ZR * N) % NT != 0 && idx >= ZR * N) break;
-    const int x = idx % N, r = idx / N;
-    const size_t o = (size_t)r * N + x;
-    const T U = __ldg(P0 + o), V = __ldg(P0 + cs + o), W = __ldg(P0 + 2 * cs + o);
-    const T Up = __ldg(Pp + o), Wp = __ldg(Pp + 2 * cs + o);
-    const T Vp = (k < ny) ? __ldg(Pp + cs + o) : V;
-    const T Um = __ldg(Pm + o), Vm = __ldg(Pm + cs + o), Wm = __ldg(Pm + 2 * cs + o);
-    const T fr = has_fringe ? fringe[(size_t)(z0 + r) * N + x] : (T)0;
-    T fpu0, fpw0, fpu, fpw, xfu, zfu, xfw, zfw;
-    if (!LIN) {
-      if (k == 2) { fpu0 = Vm * Um; fpw0 = Vm * Wm; }
-      else { fpu0 = Vm * half * (Um + U); fpw0 = Vm * half * (Wm + W); }
-      if (k < ny) { fpu = V * half * (U + Up); fpw = V * half * (W + Wp); }
-      else { fpu = V * Up; fpw = V * Wp; }
-      xfu = U * U; zfu = W * U; xfw = U * W; zfw = W * W;
+  // fluxes of one point (r, x) into the packed sequences
+  auto point = [&](T U, T V, T W, T Up, T Vp, T Wp, T Um, T Vm, T Wm, T fr, int r, int x) {
+  T fpu0, fpw0, fpu, fpw, xfu, zfu, xfw, zfw;
+  if (!LIN) {
+    if (k == 2) { fpu0 = Vm * Um; fpw0 = Vm * Wm; }
+    else { fpu0 = Vm * half * (Um + U); fpw0 = Vm * half * (Wm + W); }
+    if (k < ny) { fpu = V * half * (U + Up); fpw = V * half * (W + Wp); }
+    else { fpu = V * Up; fpw = V * Wp; }
+    xfu = U * U; zfu = W * U; xfw = U * W; zfw = W * W;
+  } else {
+    if (k == 2) { fpu0 = Bm[1] * Um + Vm * Bm[0]; fpw0 = Bm[1] * Wm + Vm * Bm[2]; }
+    else {
+      fpu0 = Bm[1] * half * (Um + U) + Vm * half * (Bm[0] + B0[0]);
+      fpw0 = Bm[1] * half * (Wm + W) + Vm * half * (Bm[2] + B0[2]);
+    }
+    if (k < ny) {
+      fpu = B0[1] * half * (U + Up) + V * half * (B0[0] + Bp[0]);
+      fpw = B0[1] * half * (W + Wp) + V * half * (B0[2] + Bp[2]);
     } else {
-      if (k == 2) { fpu0 = Bm[1] * Um + Vm * Bm[0]; fpw0 = Bm[1] * Wm + Vm * Bm[2]; }
-      else {
-        fpu0 = Bm[1] * half * (Um + U) + Vm * half * (Bm[0] + B0[0]);
-        fpw0 = Bm[1] * half * (Wm + W) + Vm * half * (Bm[2] + B0[2]);
-      }
-      if (k < ny) {
-        fpu = B0[1] * half * (U + Up) + V * half * (B0[0] + Bp[0]);
-        fpw = B0[1] * half * (W + Wp) + V * half * (B0[2] + Bp[2]);
-      } else {
-        fpu = B0[1] * Up + V * Bp[0];
-        fpw = B0[1] * Wp + V * Bp[2];
-      }
-      xfu = two * B0[0] * U; zfu = B0[2] * U + W * B0[0];
-      xfw = B0[2] * U + W * B0[0]; zfw = two * B0[2] * W;
+      fpu = B0[1] * Up + V * Bp[0];
+      fpw = B0[1] * Wp + V * Bp[2];
     }
-    const T dyu = dhk * (fpu - fpu0) + fr * (U - tu);
-    const T dyw = dhk * (fpw - fpw0) + fr * (W - tw_);
-    T xfv = 0, dyv = 0, zfv = 0;
-    if (veq) {
-      T fp0, fp;
-      if (!LIN) {
-        const T t0 = half * (Vm + V), t1 = half * (V + Vp);
-        fp0 = t0 * t0; fp = t1 * t1;
-        xfv = V * (iu1 * U + iu2 * Up);
-        zfv = V * (iu1 * W + iu2 * Wp);
-      } else {
-        const T t0 = half * (Vm + V), b0v = half * (Bm[1] + B0[1]);
-        const T t1 = half * (V + Vp), b1v = half * (B0[1] + Bp[1]);
-        fp0 = two * t0 * b0v; fp = two * t1 * b1v;
-        xfv = B0[1] * (iu1 * U + iu2 * Up) + V * (iu1 * B0[0] + iu2 * Bp[0]);
-        zfv = B0[1] * (iu1 * W + iu2 * Wp) + V * (iu1 * B0[2] + iu2 * Bp[2]);
-      }
-      dyv = dnk * (fp - fp0) + fr * (V - tv);
+    xfu = two * B0[0] * U; zfu = B0[2] * U + W * B0[0];
+    xfw = B0[2] * U + W * B0[0]; zfw = two * B0[2] * W;
+  }
+  const T dyu = dhk * (fpu - fpu0) + fr * (U - tu);
+  const T dyw = dhk * (fpw - fpw0) + fr * (W - tw_);
+  T xfv = 0, dyv = 0, zfv = 0;
+  if (veq) {
+    T fp0, fp;
+    if (!LIN) {
+      const T t0 = half * (Vm + V), t1 = half * (V + Vp);
+      fp0 = t0 * t0; fp = t1 * t1;
+      xfv = V * (iu1 * U + iu2 * Up);
+      zfv = V * (iu1 * W + iu2 * Wp);
+    } else {
+      const T t0 = half * (Vm + V), b0v = half * (Bm[1] + B0[1]);
+      const T t1 = half * (V + Vp), b1v = half * (B0[1] + Bp[1]);
+      fp0 = two * t0 * b0v; fp = two * t1 * b1v;
+      xfv = B0[1] * (iu1 * U + iu2 * Up) + V * (iu1 * B0[0] + iu2 * Bp[0]);
+      zfv = B0[1] * (iu1 * W + iu2 * Wp) + V * (iu1 * B0[2] + iu2 * Bp[2]);
     }
-    const int pxx = px(x);
-    (void)zfu;
-    FP[(4 * r + 0) * SEQ + pxx] = mk<C>(xfu, dyu);
-    FP[(4 * r + 1) * SEQ + pxx] = mk<C>(xfw, dyw);
-    FP[(4 * r + 2) * SEQ + pxx] = mk<C>(xfv, dyv);
-    FP[(4 * r + 3) * SEQ + pxx] = mk<C>(zfw, zfv);
+    dyv = dnk * (fp - fp0) + fr * (V - tv);
+  }
+  const int pxx = px(x);
+  (void)zfu;
+  FP[(4 * r + 0) * SEQ + pxx] = mk<C>(xfu, dyu);
+  FP[(4 * r + 1) * SEQ + pxx] = mk<C>(xfw, dyw);
+  FP[(4 * r + 2) * SEQ + pxx] = mk<C>(xfv, dyv);
+  FP[(4 * r + 3) * SEQ + pxx] = mk<C>(zfw, zfv);
     if (do_cfl) {
       ma = fmax(ma, fabs(U + Up));
       mb = fmax(mb, fabs(V));
       mc = fmax(mc, fabs(W + Wp));
     }
+  };
+  // two neighbouring x per thread and 8- or 16-byte loads (x even, rows of
+  // even length)
+  using V2 = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
+  static_assert(N % 2 == 0, "even rows");
+  constexpr int IT = (ZR * N / 2 + NT - 1) / NT;
+#pragma unroll
+  for (int it = 0; it < IT; ++it) {
+    const int idx = it * NT + (int)threadIdx.x;
+    if ((ZR * N / 2) % NT != 0 && idx >= ZR * N / 2) break;
+    const int x = 2 * (idx % (N / 2)), r = idx / (N / 2);
+    const size_t o = (size_t)r * N + x;
+    auto ld2 = [&](const T* b) { return __ldg(reinterpret_cast<const V2*>(b + o)); };
+    const V2 U = ld2(P0), V = ld2(P0 + cs), W = ld2(P0 + 2 * cs);
+    const V2 Up = ld2(Pp), Wp = ld2(Pp + 2 * cs);
+    const V2 Vp = (k < ny) ? ld2(Pp + cs) : V;
+    const V2 Um = ld2(Pm), Vm = ld2(Pm + cs), Wm = ld2(Pm + 2 * cs);
+    V2 fr;
+    if (has_fringe) fr = __ldg(reinterpret_cast<const V2*>(fringe + (size_t)(z0 + r) * N + x));
+    else { fr.x = (T)0; fr.y = (T)0; }
+    point(U.x, V.x, W.x, Up.x, Vp.x, Wp.x, Um.x, Vm.x, Wm.x, fr.x, r, x);
+    point(U.y, V.y, W.y, Up.y, Vp.y, Wp.y, Um.y, Vm.y, Wm.y, fr.y, r, x + 1);
   }
   if (do_cfl) {
 #pragma unroll
@@ -763,7 +778,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT
   const size_t base = (size_t)(k - 1) * 6;
   for (int idx = threadIdx.x; idx < NXH * ZR; idx += NT) {
     const int r = idx % ZR, kx = idx / ZR;
-    const T kxv = (T)gd.kx[kx];
+    const T kxv = skx[kx];
     const int km = (kx == 0) ? 0 : N - kx;
 #define OUT(e, part) T2[((base + (e) * 2 + (part)) * NXH + kx) * NZ2 + z0 + r]
 #pragma unroll
