@@ -158,7 +158,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_zfwd_r(const cp
   const int NZ = g.nz, NY1 = g.ny1, NXH = g.nxh, ny = g.ny;
   const int kx = blockIdx.x;
   const int j0 = 1 + blockIdx.y * YB;   // 1-based first plane
+  __shared__ T skz[NZ2];                 // kz of the retained rows (nz <= nz2)
   load_tw2<T, NZ2>(tw, twz);
+  for (int i = threadIdx.x; i < NZ; i += blockDim.x) skz[i] = (T)gd.kz[i];
   __syncthreads();
   for (int t = threadIdx.x; t < nseq * N2; t += blockDim.x) {
     const int s = t / N2, n2 = t - s * N2;
@@ -224,7 +226,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_zfwd_r(const cp
         fz = cadd(Zc[NZ / 2], cconj(Zc[off + NZ / 2]));
       } else { fa = A[off + kz]; fz = Zc[off + kz]; }
       const C tz = cscale(wsc, fz);
-      out = cadd(cimul<C>((T)gd.kz[kz], tz), cscale(wsc, fa));
+      out = cadd(cimul<C>(skz[kz], tz), cscale(wsc, fa));
     }
     vel[((size_t)(kx * NZ + kz) * 3 + e) * NY1 + (j - 1)] = out;
   }
