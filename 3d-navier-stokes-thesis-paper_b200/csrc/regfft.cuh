@@ -85,6 +85,21 @@ __host__ __device__ __forceinline__ C mul_i(C a) {   // (SIGN * i) * a
   return SIGN > 0 ? mk<C>(-a.y, a.x) : mk<C>(a.y, -a.x);
 }
 
+// x * W_N^m for a twiddle known at compile time after unrolling: the
+// quarter turns are sign changes and swaps (IEEE multiplication by an exact
+// 0 or 1 is not folded by the compiler), the rest a complex multiply
+template <typename T, int N, int SIGN>
+__host__ __device__ __forceinline__ cplx_t<T> twmul(cplx_t<T> x, int m) {
+  using C = cplx_t<T>;
+  const int q = (m % N) * (48 / N);
+  if (q == 0) return x;
+  if (q == 24) return mk<C>(-x.x, -x.y);
+  // W = cos(2 pi q/48) + i SIGN sin(2 pi q/48): SIGN i at q = 12, -SIGN i at 36
+  if (q == 12) return mul_i<C, SIGN>(x);
+  if (q == 36) return mul_i<C, -SIGN>(x);
+  return cmul(x, wconst<T, N, SIGN>(m));
+}
+
 template <typename T, int N, int SIGN> struct SmallFFT;
 
 template <typename T, int SIGN> struct SmallFFT<T, 1, SIGN> {
@@ -141,9 +156,7 @@ template <typename T, int P, int Q, int SIGN> struct Composite {
     for (int k2 = 0; k2 < Q; ++k2) {
 #pragma unroll
       for (int p = 0; p < P; ++p) {
-        C x = v[(p + P * k2) * S];
-        if (p * k2 != 0) x = cmul(x, wconst<T, N, SIGN>(p * k2));
-        t[k2 * P + p] = x;
+        t[k2 * P + p] = twmul<T, N, SIGN>(v[(p + P * k2) * S], p * k2);
       }
       SmallFFT<T, P, SIGN>::template run<1>(t + k2 * P);
     }
