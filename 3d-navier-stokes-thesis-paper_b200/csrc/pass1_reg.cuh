@@ -524,16 +524,22 @@ __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_g
 // row pitch (complex values) of the gathered hybrid rows: 16 bytes of padding
 // keeps the 16-byte cp.async destinations aligned and the stage-1 reads
 // (consecutive threads on consecutive kx) free of bank conflicts
+template <int N, int ZB> __host__ __device__ constexpr int xinv_threads() {
+  return ((ZB / 2) * Split<N>::N2 + 31) / 32 * 32 < 128 ? 128
+       : (((ZB / 2) * Split<N>::N2 + 31) / 32 * 32 > 256 ? 256 : ((ZB / 2) * Split<N>::N2 + 31) / 32 * 32);
+}
+
 template <typename T, int ZB> struct RawPitch {
   static constexpr int V = ZB + 16 / (int)sizeof(cplx_t<T>);
 };
 
-// k_xinv_r: grid (nz2/ZB, 3, ny+1), block 128.  Inverse x transform of ZB
+// k_xinv_r: grid (nz2/ZB, 3, ny+1), block xinv_threads (one thread per
+// stage-1 task, at least 128).  Inverse x transform of ZB
 // hybrid rows (one plane, one component) into physical rows, two real rows per
 // complex FFT (the x part of xz_fft_complex_to_real_parallel,
 // PFC/transform.f90:345-368).  v of plane ny+1 is not formed: no flux reads it.
 template <typename T, int NX2, int ZB>
-__global__ void __launch_bounds__(128) k_xinv_r(const cplx_t<T>* __restrict__ T1, T* __restrict__ P, Geom g,
+__global__ void __launch_bounds__(256) k_xinv_r(const cplx_t<T>* __restrict__ T1, T* __restrict__ P, Geom g,
                                                 const cplx_t<T>* __restrict__ twx) {
   using C = cplx_t<T>;
   constexpr int N1 = Split<NX2>::N1, N2 = Split<NX2>::N2, PITCH = N2 + 1, SEQ = SeqPitch<NX2>::V;
