@@ -153,6 +153,13 @@ SYMBOLS = {
     "cfg_xz_c2r_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _VP, _VP, _VP]),
     "cfg_profile_enable": (C.c_int, [_VP, C.c_int]),
     "cfg_profile_read": (C.c_int, [_VP, C.c_int, C.c_char_p, C.c_int, C.POINTER(C.c_int), _DP]),
+    "cfg_partition": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "cfg_group_create": (C.c_int, [C.POINTER(CfgParams), C.POINTER(CfgGrid), C.c_int, _VP, C.POINTER(_VP)]),
+    "cfg_group_size": (C.c_int, [_VP]),
+    "cfg_group_rank": (_VP, [_VP, C.c_int]),
+    "cfg_group_timestep": (C.c_int, [_VP, C.c_int]),
+    "cfg_group_synchronize": (C.c_int, [_VP]),
+    "cfg_group_destroy": (None, [_VP]),
     "cfh_run_defaults": (None, [C.POINTER(CfhRun)]),
     "cfh_read_flow_dat": (C.c_int, [C.c_char_p, C.POINTER(CfhRun), C.c_char_p, C.c_int]),
     "cfh_grid_alloc": (C.POINTER(CfhGrid), [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
@@ -318,7 +325,8 @@ class ChannelFlow:
 
     def close(self):
         if getattr(self, "h", None):
-            self.L.cfg_destroy(self.h)
+            if getattr(self, "_owned", True):
+                self.L.cfg_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -561,3 +569,107 @@ def arnoldi_eigs(flow, tend, nev=12, ncv=25, tol=1e-8, maxiter=None, v0=None):
     lam = (np.log(np.abs(mu) + np.finfo(np.float64).eps) + 1j * np.arctan2(mu.imag, mu.real)) / T
     order = np.argsort(-np.abs(mu))
     return mu[order], lam[order], vec[:, order]
+
+
+PARTITION_KEYS = ("nx_proc", "x_start", "nz_proc", "z_start", "nz_small_proc", "z_small_start")
+
+
+def partition(nx, nz, nz2, nproc):
+    """distribute_data (PFC/setup.f90:298-437): the split of the nx/2+1
+    Fourier columns, the nz2 physical z rows and the nz undealiased z rows
+    among nproc ranks, as a dict of int arrays (keys PARTITION_KEYS)."""
+    L = load_library()
+    arrs = [np.zeros(nproc, np.int32) for _ in PARTITION_KEYS]
+    r = L.cfg_partition(nx, nz, nz2, nproc, *[_p(a) for a in arrs])
+    if r != 0:
+        raise ChanflowError(f"cfg_partition failed ({ERRORS.get(r, r)})")
+    return dict(zip(PARTITION_KEYS, arrs))
+
+
+class Group:
+    """cfg_group: nranks contexts that advance one field together, rank i
+    holding the Fourier columns [x_start[i], x_start[i] + nx_proc[i]) of the
+    state and the z2 rows [z_start[i], ...) of the physical planes -- the
+    reference's MPI decomposition (PFC/setup.f90:298-437) with the transposes
+    of the x-z transforms as stores into the owning rank's buffers.
+    devices: one GPU per rank (default: all ranks on `device`)."""
+
+    def __init__(self, grid, nranks, devices=None, re=2500.0, dt=0.005, beta=0.0, cfl_max=0.95, fix_mass=1,
+                 dt_flag=0, precision=FP64, device=0):
+        self.L = load_library()
+        self.grid = grid
+        self.nranks = nranks
+        self.params = CfgParams(grid.nx, grid.ny, grid.nz, grid.nx2, grid.nz2, re, grid.lx, grid.lz,
+                                beta, dt, cfl_max, fix_mass, dt_flag, 0.0, 0.0, precision, device)
+        g, keep = grid.cfg_grid()
+        devs = None if devices is None else np.ascontiguousarray(devices, dtype=np.int32)
+        h = C.c_void_p()
+        r = self.L.cfg_group_create(C.byref(self.params), C.byref(g), nranks, _p(devs), C.byref(h))
+        if r != 0:
+            raise ChanflowError(f"cfg_group_create failed ({ERRORS.get(r, r)})")
+        self.h = h
+        self.part = partition(grid.nx, grid.nz, grid.nz2, nranks)
+        self.ranks = []
+        for i in range(nranks):
+            f = ChannelFlow.__new__(ChannelFlow)
+            f.L, f.grid, f.precision, f.params = self.L, grid, precision, self.params
+            f.nx, f.ny, f.nz, f.nx2, f.nz2 = grid.nx, grid.ny, grid.nz, grid.nx2, grid.nz2
+            f.nxh = int(self.part["nx_proc"][i])
+            f.h = C.c_void_p(self.L.cfg_group_rank(self.h, i))
+            f._owned = False
+            f.step = 0
+            self.ranks.append(f)
+
+    def _chk(self, r, rank=0):
+        if r != 0:
+            msg = self.L.cfg_last_error(self.ranks[rank].h)
+            raise ChanflowError(f"{ERRORS.get(r, r)}: {msg.decode() if msg else ''}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            for f in self.ranks:
+                f.h = None
+            self.L.cfg_group_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _slab(self, i):
+        x0 = int(self.part["x_start"][i])
+        return slice(x0, x0 + int(self.part["nx_proc"][i]))
+
+    def upload_state(self, data1=None, data2=None, data4=None):
+        """Whole-field arrays in the reference's layouts, split by kx slab."""
+        for i, f in enumerate(self.ranks):
+            sl = self._slab(i)
+            f.upload_state(None if data1 is None else data1[:, sl],
+                           None if data2 is None else data2[..., sl],
+                           None if data4 is None else data4[..., sl])
+
+    def download_state(self):
+        parts = [f.download_state() for f in self.ranks]
+        d1 = np.concatenate([p[0] for p in parts], axis=1)
+        d2 = np.concatenate([p[1] for p in parts], axis=3)
+        d4 = np.concatenate([p[2] for p in parts], axis=2)
+        return np.asfortranarray(d1), np.asfortranarray(d2), np.asfortranarray(d4)
+
+    def set_scalars(self, t_total, dt, p_grad, d_um_dy=None):
+        for f in self.ranks:
+            f.set_scalars(t_total, dt, p_grad, d_um_dy)
+
+    def scalars(self, rank=0):
+        return self.ranks[rank].scalars()
+
+    def timestep(self, n=1):
+        self._chk(self.L.cfg_group_timestep(self.h, n))
+
+    def synchronize(self):
+        self._chk(self.L.cfg_group_synchronize(self.h))
+
+    def status(self):
+        return [f.status() for f in self.ranks]
+

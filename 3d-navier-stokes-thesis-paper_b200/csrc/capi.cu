@@ -204,6 +204,21 @@ struct cfg_ctx {
   std::vector<Rec> recs;
   const char* cur_name = nullptr;
   cudaEvent_t cur_a = nullptr;
+  // rank of a multi-rank run (cfg_group): kx slab [g.kx0, g.kx0 + g.nxh) in
+  // Fourier space, z2 slab [z0s, z0s + gP.nz2) in physical space
+  // (distribute_data, PFC/setup.f90:298-437)
+  int rank = 0, nranks = 1, z0s = 0;
+  Geom gP{};              // geometry of the x stage: all kx, this rank's z2 rows
+  GridDev gd_all{};       // grid operators with the global kx table
+  Scatter scat{};         // transpose targets (n == 0: one rank)
+  void* scat_tab = nullptr;
+  unsigned long long** cfl_peers = nullptr;   // the other ranks' cflbits
+  int n_cfl_peers = 0;
+};
+
+// slab of one rank (cfg_group_create); one rank: the whole grid
+struct SlabPart {
+  int rank, nranks, x0, nxl, z0, nzl;
 };
 
 static cudaEvent_t prof_event(cfg_ctx* c) {
@@ -287,6 +302,22 @@ static dim3 grid1d(size_t n, int bs = 256) {
 }
 
 // ----------------------------------------------------------------------------
+// global CFL maxima of a multi-rank run: each rank folds the other ranks'
+// per-plane maxima (peer memory) into its own before k_cfl_finalize, so that
+// every rank takes the same dt (the MPI_ALLREDUCE of check_cfl,
+// PFC/pass1.f90:202-250).  Values are non-negative doubles as bit patterns.
+__global__ void k_cfl_merge(unsigned long long* __restrict__ own, unsigned long long* const* __restrict__ peers,
+                            int npeers, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    unsigned long long m = own[i];
+    for (int r = 0; r < npeers; ++r) {
+      const unsigned long long v = *((volatile const unsigned long long*)peers[r] + i);
+      m = v > m ? v : m;
+    }
+    own[i] = m;
+  }
+}
+
 template <typename T>
 struct Impl {
   using C = cplx_t<T>;
@@ -361,11 +392,13 @@ struct Impl {
     // split x stage: physical planes written once, fluxes read three of them
     c->flux_zr = getenv("CHANFLOW_FLUX_ZR") ? atoi(getenv("CHANFLOW_FLUX_ZR")) : 4;
     if (c->flux_zr != 2) c->flux_zr = 4;
-    c->split_x = c->fast_x && !getenv("CHANFLOW_FUSED_XFLUX") && g.nz2 % (f32 ? 16 : 8) == 0 &&
-                 g.nz2 % c->flux_zr == 0 && p1_fast_smem(3, g.nx2, f32, 0, g.nxh, g.nz) <= 200 * 1024 &&
-                 p1_fast_smem(4, g.nx2, f32, c->flux_zr, g.nxh, g.nz) <= 200 * 1024;
+    // (gP: the x stage's geometry, all kx and this rank's z2 rows)
+    const Geom& gp = c->gP;
+    c->split_x = c->fast_x && (!getenv("CHANFLOW_FUSED_XFLUX") || c->nranks > 1) && gp.nz2 % 8 == 0 &&
+                 gp.nz2 % c->flux_zr == 0 && p1_fast_smem(3, g.nx2, f32, gp.nz2, gp.nxh, g.nz) <= 200 * 1024 &&
+                 p1_fast_smem(4, g.nx2, f32, c->flux_zr, gp.nxh, g.nz) <= 200 * 1024;
     if (c->split_x &&
-        cudaMalloc(&c->P, sizeof(T) * (size_t)(g.ny + 1) * 3 * g.nz2 * g.nx2) != cudaSuccess) {
+        cudaMalloc(&c->P, sizeof(T) * (size_t)(g.ny + 1) * 3 * gp.nz2 * g.nx2) != cudaSuccess) {
       cudaGetLastError();
       c->split_x = false;
     }
@@ -380,48 +413,76 @@ struct Impl {
   }
 
   static int nonlinear(cfg_ctx* c, int step, int rk, bool lin) {
+    for (int ph = 1; ph <= 3; ++ph) {
+      const int r = nl_phase(c, step, rk, lin, ph);
+      if (r) return r;
+    }
+    return CFG_OK;
+  }
+
+  // nonlinear (PFC/pass1.f90:26-124) in three phases; a multi-rank run puts
+  // a barrier between them: 1 the inverse z transform, scattered to the z2
+  // slabs; 2 the x stage (inverse x, fluxes, forward x), scattered to the kx
+  // slabs; 3 the forward z transform and the CFL / dt update
+  static int nl_phase(cfg_ctx* c, int step, int rk, bool lin, int phase) {
     const Geom& g = c->g;
-    c->mean64_valid = false;
     const int do_cfl = (rk == 1);
-    if (do_cfl) CK(cudaMemsetAsync(c->cflbits, 0, sizeof(unsigned long long) * 3 * g.ny1, c->st));
+    const bool f32 = sizeof(T) == 4;
     P1Launch a{};
     a.vel = c->vel; a.T1 = c->T1; a.T2 = c->T2; a.velout = c->vel; a.g = g; a.twx = c->twx; a.twz = c->twz;
     a.gd = c->gd; a.fringe = c->fringe; a.has_fringe = c->has_fringe; a.YB1 = c->fYB1; a.YB3 = c->fYB3;
     a.ZR = c->fZR; a.cflbits = c->cflbits; a.do_cfl = do_cfl; a.lin = lin ? 1 : 0; a.st = c->st;
     a.KC = (int)std::max(2L, std::min(16L, (long)(g.ny - 1) * (g.nz2 / c->fZR) / 592));
-    const bool f32 = sizeof(T) == 4;
-    dim3 g1(g.nxh, (g.ny1 + c->YB1 - 1) / c->YB1);
-    prof_begin(c, "k_zinv");
-    if (c->fast_z) {
-      if (p1_fast_launch(0, g.nz2, f32, a) != 0) return fail(c, CFG_E_CUDA, "k_zinv_r launch");
-    } else
-      k_zinv<T><<<g1, 256, c->sm_zinv, c->st>>>((const C*)c->vel, (C*)c->T1, g, c->pz, (const C*)c->twz,
-                                                 c->YB1, 0, g.ny1);
-    CKL();
-    dim3 g2(g.nz2 / c->ZR, (g.ny - 1 + c->KC - 1) / c->KC);
     a.P = c->P;
     a.FZR = c->flux_zr;
-    if (c->split_x) {
-      prof_begin(c, "k_xinv");
-      if (p1_fast_launch(3, g.nx2, f32, a) != 0) return fail(c, CFG_E_CUDA, "k_xinv_r launch");
+    a.sc = c->scat;
+    if (phase == 1) {
+      c->mean64_valid = false;
+      if (do_cfl) CK(cudaMemsetAsync(c->cflbits, 0, sizeof(unsigned long long) * 3 * g.ny1, c->st));
+      dim3 g1(g.nxh, (g.ny1 + c->YB1 - 1) / c->YB1);
+      prof_begin(c, "k_zinv");
+      if (c->fast_z) {
+        if (p1_fast_launch(0, g.nz2, f32, a) != 0) return fail(c, CFG_E_CUDA, "k_zinv_r launch");
+      } else
+        k_zinv<T><<<g1, 256, c->sm_zinv, c->st>>>((const C*)c->vel, (C*)c->T1, g, c->pz, (const C*)c->twz,
+                                                   c->YB1, 0, g.ny1);
       CKL();
-      prof_begin(c, "k_flux");
-      if (p1_fast_launch(4, g.nx2, f32, a) != 0) return fail(c, CFG_E_CUDA, "k_flux_r launch");
-    } else if (c->fast_x) {
-      prof_begin(c, "k_xflux");
-      if (p1_fast_launch(1, g.nx2, f32, a) != 0) return fail(c, CFG_E_CUDA, "k_xflux_r launch");
-    } else if (lin) {
-      prof_begin(c, "k_xflux");
-      k_xflux<T, true><<<g2, 256, c->sm_xflux, c->st>>>((const C*)c->T1, (C*)c->T2, g, c->px, (const C*)c->twx,
-                                                         c->gd, (const T*)c->fringe, c->has_fringe, c->ZR, c->KC,
-                                                         c->cflbits, do_cfl);
-    } else {
-      prof_begin(c, "k_xflux");
-      k_xflux<T, false><<<g2, 256, c->sm_xflux, c->st>>>((const C*)c->T1, (C*)c->T2, g, c->px, (const C*)c->twx,
-                                                          c->gd, (const T*)c->fringe, c->has_fringe, c->ZR, c->KC,
-                                                          c->cflbits, do_cfl);
+      return CFG_OK;
     }
-    CKL();
+    if (phase == 2) {
+      dim3 g2(g.nz2 / c->ZR, (g.ny - 1 + c->KC - 1) / c->KC);
+      if (c->split_x) {
+        // x stage on this rank's z2 rows, all kx
+        a.g = c->gP;
+        a.gd = c->gd_all;
+        if (c->fringe) a.fringe = (const T*)c->fringe + (size_t)c->z0s * g.nx2;
+        prof_begin(c, "k_xinv");
+        if (p1_fast_launch(3, g.nx2, f32, a) != 0) return fail(c, CFG_E_CUDA, "k_xinv_r launch");
+        CKL();
+        prof_begin(c, "k_flux");
+        if (p1_fast_launch(4, g.nx2, f32, a) != 0) return fail(c, CFG_E_CUDA, "k_flux_r launch");
+      } else if (c->fast_x) {
+        prof_begin(c, "k_xflux");
+        if (p1_fast_launch(1, g.nx2, f32, a) != 0) return fail(c, CFG_E_CUDA, "k_xflux_r launch");
+      } else if (lin) {
+        prof_begin(c, "k_xflux");
+        k_xflux<T, true><<<g2, 256, c->sm_xflux, c->st>>>((const C*)c->T1, (C*)c->T2, g, c->px, (const C*)c->twx,
+                                                           c->gd, (const T*)c->fringe, c->has_fringe, c->ZR, c->KC,
+                                                           c->cflbits, do_cfl);
+      } else {
+        prof_begin(c, "k_xflux");
+        k_xflux<T, false><<<g2, 256, c->sm_xflux, c->st>>>((const C*)c->T1, (C*)c->T2, g, c->px, (const C*)c->twx,
+                                                            c->gd, (const T*)c->fringe, c->has_fringe, c->ZR, c->KC,
+                                                            c->cflbits, do_cfl);
+      }
+      CKL();
+      return CFG_OK;
+    }
+    if (do_cfl && c->n_cfl_peers > 0) {
+      prof_begin(c, "k_cfl_merge");
+      k_cfl_merge<<<1, 256, 0, c->st>>>(c->cflbits, c->cfl_peers, c->n_cfl_peers, 3 * g.ny1);
+      CKL();
+    }
     dim3 g3(g.nxh, (g.ny1 + c->YB3 - 1) / c->YB3);
     prof_begin(c, "k_zfwd");
     if (c->fast_z) {
@@ -479,7 +540,9 @@ struct Impl {
     if (mode == 0) c->mean64_valid = true;
     c->prof_stream = c->st3;
     prof_begin(c, "k_rhs_mean");
-    if (v2) {
+    if (g.kx0 != 0) {
+      // the mean mode lives on the rank that holds kx = 0
+    } else if (v2) {
       RhsMeanLaunch m{};
       m.vel = c->vel; m.cru = c->cru; m.prs = c->prs; m.mvel64 = c->mvel64; m.mcru64 = c->mcru64;
       m.cbc_top = (const C*)c->cbc + 3 * (size_t)g.nw; m.cbc_bot = c->cbc;
@@ -680,6 +743,14 @@ static int ensure_stage(cfg_ctx* c, size_t elems) {
   return CFG_OK;
 }
 
+// the FP64 side copy of the mean column, on the rank that holds kx = 0
+static double2* mean_side(const cfg_ctx* c, double2* p) { return c->g.kx0 == 0 ? p : nullptr; }
+
+// entry points that need the whole grid on one context
+static int single_only(cfg_ctx* c, const char* what) {
+  return fail(c, CFG_E_ARG, "%s: not available on one rank of a multi-rank group", what);
+}
+
 static int check_status(cfg_ctx* c) {
   DevScalars h;
   CK(cudaMemcpyAsync(&h, c->sc, sizeof(h), cudaMemcpyDeviceToHost, c->st));
@@ -695,7 +766,8 @@ const char* cfg_last_error(const cfg_ctx* c) { return c ? c->err.c_str() : "null
 long long cfg_launch_count(const cfg_ctx* c) { return c ? c->launches : 0; }
 void* cfg_stream(cfg_ctx* c) { return c ? (void*)c->st : nullptr; }
 
-int cfg_create(const cfg_params* p, const cfg_grid* gr, cfg_ctx** out) {
+// one context: the whole grid (sp == nullptr) or one rank's slabs of it
+static int create_impl(const cfg_params* p, const cfg_grid* gr, const SlabPart* sp, cfg_ctx** out) {
   if (!p || !gr || !out) return CFG_E_ARG;
   *out = nullptr;
   cfg_ctx* c = new cfg_ctx();
@@ -711,9 +783,21 @@ int cfg_create(const cfg_params* p, const cfg_grid* gr, cfg_ctx** out) {
   c->mixed = (p->precision == CFG_MIXED);
   Geom& g = c->g;
   g.nx = p->nx; g.ny = p->ny; g.nz = p->nz; g.nx2 = p->nx2; g.nz2 = p->nz2;
-  g.nxh = p->nx / 2 + 1;
+  g.nxh_all = p->nx / 2 + 1;
+  g.nxh = sp ? sp->nxl : g.nxh_all;
+  g.kx0 = sp ? sp->x0 : 0;
   g.ny1 = p->ny + 1;
   g.nw = g.nz * g.nxh;
+  c->gP = g;
+  c->gP.nxh = g.nxh_all;
+  c->gP.kx0 = 0;
+  c->gP.nz2 = sp ? sp->nzl : g.nz2;
+  c->gP.nw = g.nz * g.nxh_all;
+  if (sp) {
+    c->rank = sp->rank;
+    c->nranks = sp->nranks;
+    c->z0s = sp->z0;
+  }
   if (!make_plan(g.nx2, c->px) || !make_plan(g.nz2, c->pz) || !make_plan(g.nx, c->pxs) || !make_plan(g.nz, c->pzs)) {
     fprintf(stderr, "cfg_create: transform lengths must be 2^a 3^b\n");
     delete c;
@@ -746,7 +830,7 @@ int cfg_create(const cfg_params* p, const cfg_grid* gr, cfg_ctx** out) {
                   {gr->dn, (size_t)ny, &c->gd.dn},     {gr->iu, (size_t)2 * ny, &c->gd.iu},
                   {gr->dm, 12, &c->gd.dm},             {gr->d2h, (size_t)3 * n1, &c->gd.d2h},
                   {gr->d2n, (size_t)3 * ny, &c->gd.d2n}, {gr->dyh, (size_t)n1, &c->gd.dyh},
-                  {gr->dy, (size_t)n1, &c->gd.dy},     {gr->kx, (size_t)g.nxh, &c->gd.kx},
+                  {gr->dy, (size_t)n1, &c->gd.dy},     {gr->kx, (size_t)g.nxh_all, &c->gd.kx},
                   {gr->kz, (size_t)g.nz, &c->gd.kz},   {tgt, (size_t)3 * n1, &c->gd.target},
                   {zeros3.data(), (size_t)3 * n1, &c->gd.baseflow}};
   size_t tot = 0;
@@ -774,12 +858,19 @@ int cfg_create(const cfg_params* p, const cfg_grid* gr, cfg_ctx** out) {
     }
     cudaMemcpy(c->dgrid, h.data(), sizeof(double) * tot, cudaMemcpyHostToDevice);
   }
+  // the x stage reads the global kx table; the Fourier-space kernels this
+  // rank's slab of it
+  c->gd_all = c->gd;
+  c->gd.kx = c->gd_all.kx + g.kx0;
   memcpy(c->hdm, gr->dm, sizeof(double) * 12);
   c->hdy.assign(gr->dy, gr->dy + n1);
   c->hyh.assign(gr->yh, gr->yh + n1);
   // state and work buffers
   const size_t cs = csize(c), nf = (size_t)g.nw * 3 * n1;
-  const size_t t1 = (size_t)n1 * 3 * g.nxh * g.nz2, t2 = (size_t)n1 * 6 * g.nxh * g.nz2;
+  // T1: hybrid rows of this rank's z2 slab for all kx (the z transform's
+  // scatter target); T2: x-transformed fluxes of this rank's kx slab for all
+  // z2 (the flux kernel's scatter target)
+  const size_t t1 = (size_t)n1 * 3 * g.nxh_all * c->gP.nz2, t2 = (size_t)n1 * 6 * g.nxh * g.nz2;
   bool ok = cudaMalloc(&c->vel, cs * nf) == cudaSuccess && cudaMalloc(&c->cru, cs * nf) == cudaSuccess &&
             cudaMalloc(&c->prs, cs * (size_t)g.nw * n1) == cudaSuccess && cudaMalloc(&c->T1, cs * t1) == cudaSuccess &&
             cudaMalloc(&c->T2, cs * t2) == cudaSuccess && cudaMalloc(&c->cbc, cs * 6 * (size_t)g.nw) == cudaSuccess &&
@@ -821,8 +912,8 @@ int cfg_create(const cfg_params* p, const cfg_grid* gr, cfg_ctx** out) {
     // the wavenumbers with |k| < 4 (ill-conditioned pressure solves on the
     // stretched grid) run with FP64 arithmetic
     std::vector<int> fast, prec;
-    for (int w = 1; w < g.nw; ++w) {
-      const double kx = gr->kx[w / g.nz], kz = gr->kz[w % g.nz];
+    for (int w = (g.kx0 == 0 ? 1 : 0); w < g.nw; ++w) {
+      const double kx = gr->kx[g.kx0 + w / g.nz], kz = gr->kz[w % g.nz];
       const double k2 = kx * kx + kz * kz;
       if (c->mixed && k2 < 16.0) prec.push_back(w);
       else fast.push_back(w);
@@ -872,6 +963,8 @@ int cfg_create(const cfg_params* p, const cfg_grid* gr, cfg_ctx** out) {
   return CFG_OK;
 }
 
+int cfg_create(const cfg_params* p, const cfg_grid* gr, cfg_ctx** out) { return create_impl(p, gr, nullptr, out); }
+
 void cfg_destroy(cfg_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->dev);
@@ -888,7 +981,7 @@ void cfg_destroy(cfg_ctx* c) {
   void* bufs[] = {c->dgrid, c->fringe, c->vel, c->cru, c->prs, c->mvel64, c->mcru64, c->T1, c->T2, c->P, c->rhs2_tbl, c->rhs2_tbl64, c->jst, c->pp_wy, c->pp_sy, c->pp_acc, c->cbc,
                   c->sc, c->d_um_dy, c->cflp, c->cflbits, c->l2acc, c->divbits, c->plist, c->pw_H,
                   c->pw_phys, c->pw_phys2, c->pw_in, c->stage, c->twx, c->twz, c->twxs, c->twzs,
-                  c->wl_fast, c->wl_prec};
+                  c->wl_fast, c->wl_prec, c->scat_tab, c->cfl_peers};
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
@@ -911,13 +1004,13 @@ int cfg_upload_state(cfg_ctx* c, const double* d1, const double* d2, const doubl
   if (d1) {
     CK(cudaMemcpyAsync(c->stage, d1, sizeof(double2) * nf, cudaMemcpyHostToDevice, c->st));
     c->mean64_valid = true;
-    if (c->mixed) k_data1_in<float><<<grid1d(nf), 256, 0, c->st>>>(c->stage, (float2*)c->vel, c->mvel64, g);
+    if (c->mixed) k_data1_in<float><<<grid1d(nf), 256, 0, c->st>>>(c->stage, (float2*)c->vel, mean_side(c, c->mvel64), g);
     else k_data1_in<double><<<grid1d(nf), 256, 0, c->st>>>(c->stage, (double2*)c->vel, nullptr, g);
     CKL();
   }
   if (d2) {
     CK(cudaMemcpyAsync(c->stage, d2, sizeof(double2) * nf, cudaMemcpyHostToDevice, c->st));
-    if (c->mixed) k_conv_in<float><<<grid1d(nf), 256, 0, c->st>>>(c->stage, (float2*)c->cru, nf, c->mcru64, 3 * (size_t)g.ny1);
+    if (c->mixed) k_conv_in<float><<<grid1d(nf), 256, 0, c->st>>>(c->stage, (float2*)c->cru, nf, mean_side(c, c->mcru64), 3 * (size_t)g.ny1);
     else k_conv_in<double><<<grid1d(nf), 256, 0, c->st>>>(c->stage, (double2*)c->cru, nf, nullptr, 0);
     CKL();
   }
@@ -940,14 +1033,14 @@ int cfg_download_state(cfg_ctx* c, double* d1, double* d2, double* d4) {
   int r = ensure_stage(c, nf);
   if (r) return r;
   if (d1) {
-    if (c->mixed) k_data1_out<float><<<grid1d(nf), 256, 0, c->st>>>((const float2*)c->vel, c->mean64_valid ? c->mvel64 : nullptr, c->stage, g);
+    if (c->mixed) k_data1_out<float><<<grid1d(nf), 256, 0, c->st>>>((const float2*)c->vel, c->mean64_valid ? mean_side(c, c->mvel64) : nullptr, c->stage, g);
     else k_data1_out<double><<<grid1d(nf), 256, 0, c->st>>>((const double2*)c->vel, nullptr, c->stage, g);
     CKL();
     CK(cudaMemcpyAsync(d1, c->stage, sizeof(double2) * nf, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
   }
   if (d2) {
-    if (c->mixed) k_conv_out<float><<<grid1d(nf), 256, 0, c->st>>>((const float2*)c->cru, c->stage, nf, c->mcru64, 3 * (size_t)g.ny1);
+    if (c->mixed) k_conv_out<float><<<grid1d(nf), 256, 0, c->st>>>((const float2*)c->cru, c->stage, nf, mean_side(c, c->mcru64), 3 * (size_t)g.ny1);
     else k_conv_out<double><<<grid1d(nf), 256, 0, c->st>>>((const double2*)c->cru, c->stage, nf, nullptr, 0);
     CKL();
     CK(cudaMemcpyAsync(d2, c->stage, sizeof(double2) * nf, cudaMemcpyDeviceToHost, c->st));
@@ -1045,6 +1138,7 @@ int cfg_boundary(cfg_ctx* c) {
 
 int cfg_nonlinear(cfg_ctx* c, int step, int rk_step) {
   if (!c || rk_step < 1 || rk_step > 3) return CFG_E_ARG;
+  if (c->nranks > 1) return single_only(c, "cfg_nonlinear");
   cudaSetDevice(c->dev);
   c->step = step;
   return DISPATCH(c, nonlinear(c, step, rk_step, false));
@@ -1052,6 +1146,7 @@ int cfg_nonlinear(cfg_ctx* c, int step, int rk_step) {
 
 int cfg_nonlinear_linearized(cfg_ctx* c, int step, int rk_step) {
   if (!c || rk_step < 1 || rk_step > 3) return CFG_E_ARG;
+  if (c->nranks > 1) return single_only(c, "cfg_nonlinear_linearized");
   cudaSetDevice(c->dev);
   c->step = step;
   return DISPATCH(c, nonlinear(c, step, rk_step, true));
@@ -1066,6 +1161,7 @@ int cfg_rhs_solve(cfg_ctx* c, int step, int rk_step) {
 
 static int timestep_impl(cfg_ctx* c, int nsteps, bool lin) {
   if (!c || nsteps < 0) return CFG_E_ARG;
+  if (c->nranks > 1) return single_only(c, "cfg_timestep");
   cudaSetDevice(c->dev);
   for (int s = 0; s < nsteps; ++s) {
     c->step = c->step < 0 ? 1 : c->step + 1;
@@ -1104,6 +1200,7 @@ int cfg_remove_initial_divergence(cfg_ctx* c) {
 
 int cfg_compute_initial_pressure(cfg_ctx* c, int linearized) {
   if (!c) return CFG_E_ARG;
+  if (c->nranks > 1) return single_only(c, "cfg_compute_initial_pressure");
   cudaSetDevice(c->dev);
   // step = -1, rk_step = 3 (PFC/init_vel.f90:444-445): no CFL, no dt change
   int r = DISPATCH(c, nonlinear(c, -1, 3, linearized != 0));
@@ -1121,6 +1218,7 @@ int cfg_compute_initial_pressure(cfg_ctx* c, int linearized) {
 
 int cfg_xz_c2r(cfg_ctx* c, const double* cdata, double* data) {
   if (!c || !cdata || !data) return CFG_E_ARG;
+  if (c->nranks > 1) return single_only(c, "cfg_xz_c2r");
   cudaSetDevice(c->dev);
   const Geom& g = c->g;
   const size_t nin = (size_t)g.nw, nout = (size_t)g.nx2 * g.nz2;
@@ -1149,6 +1247,7 @@ int cfg_xz_c2r(cfg_ctx* c, const double* cdata, double* data) {
 
 int cfg_xz_r2c(cfg_ctx* c, const double* data, double* cdata) {
   if (!c || !cdata || !data) return CFG_E_ARG;
+  if (c->nranks > 1) return single_only(c, "cfg_xz_r2c");
   cudaSetDevice(c->dev);
   const Geom& g = c->g;
   const size_t nin = (size_t)g.nx2 * g.nz2, nout = (size_t)g.nw;
@@ -1186,6 +1285,7 @@ static int small_capacity(cfg_ctx* c) {
 
 int cfg_small_r2c(cfg_ctx* c, const double* data, double* cdata, int nplanes) {
   if (!c || !cdata || !data || nplanes < 1) return CFG_E_ARG;
+  if (c->nranks > 1) return single_only(c, "cfg_small_r2c");
   if (nplanes > small_capacity(c)) return fail(c, CFG_E_ARG, "cfg_small_r2c: more than %d planes", small_capacity(c));
   cudaSetDevice(c->dev);
   const Geom& g = c->g;
@@ -1216,6 +1316,7 @@ int cfg_small_r2c(cfg_ctx* c, const double* data, double* cdata, int nplanes) {
 
 int cfg_small_c2r(cfg_ctx* c, const double* cdata, double* data, int nplanes) {
   if (!c || !cdata || !data || nplanes < 1) return CFG_E_ARG;
+  if (c->nranks > 1) return single_only(c, "cfg_small_c2r");
   if (nplanes > small_capacity(c)) return fail(c, CFG_E_ARG, "cfg_small_c2r: more than %d planes", small_capacity(c));
   cudaSetDevice(c->dev);
   const Geom& g = c->g;
@@ -1246,6 +1347,7 @@ int cfg_small_c2r(cfg_ctx* c, const double* cdata, double* data, int nplanes) {
 
 int cfg_set_jet(cfg_ctx* c, const cfg_jet* j) {
   if (!c) return CFG_E_ARG;
+  if (c->nranks > 1) return single_only(c, "cfg_set_jet");
   cudaSetDevice(c->dev);
   if (!j || j->mode == 0) {
     c->crossflow = false;
@@ -1278,6 +1380,7 @@ int cfg_set_jet(cfg_ctx* c, const cfg_jet* j) {
 
 int cfg_jet_profile(cfg_ctx* c, double time, double time_incr) {
   if (!c) return CFG_E_ARG;
+  if (c->nranks > 1) return single_only(c, "cfg_jet_profile");
   if (!c->crossflow) return fail(c, CFG_E_STATE, "cfg_jet_profile: no jet set (cfg_set_jet)");
   cudaSetDevice(c->dev);
   return DISPATCH(c, jet(c, 0, time, time_incr, 0));
@@ -1285,6 +1388,7 @@ int cfg_jet_profile(cfg_ctx* c, double time, double time_incr) {
 
 int cfg_get_jet_forcing(cfg_ctx* c, double* jet_forcing, double* jet_forcing_incr) {
   if (!c) return CFG_E_ARG;
+  if (c->nranks > 1) return single_only(c, "cfg_get_jet_forcing");
   if (!c->jst) return fail(c, CFG_E_STATE, "cfg_get_jet_forcing: no jet set (cfg_set_jet)");
   cudaSetDevice(c->dev);
   JetState h{};
@@ -1297,12 +1401,14 @@ int cfg_get_jet_forcing(cfg_ctx* c, double* jet_forcing, double* jet_forcing_inc
 
 int cfg_l2_norm(cfg_ctx* c, double* l2, double* drag) {
   if (!c) return CFG_E_ARG;
+  if (c->nranks > 1) return single_only(c, "cfg_l2_norm");
   cudaSetDevice(c->dev);
   return DISPATCH(c, l2(c, l2, drag));
 }
 
 int cfg_diagnostics(cfg_ctx* c, double* bulk_flux, double* max_div) {
   if (!c) return CFG_E_ARG;
+  if (c->nranks > 1) return single_only(c, "cfg_diagnostics");
   cudaSetDevice(c->dev);
   const Geom& g = c->g;
   CK(cudaMemsetAsync(c->divbits, 0, sizeof(unsigned long long), c->st));
@@ -1387,6 +1493,7 @@ int cfg_synchronize(cfg_ctx* c) {
 // compute_time_deriv (PFC/arnoldi.f90:485-567) on the device; see chanflow.h
 int cfg_arnoldi_matvec(cfg_ctx* c, int tend, const double* v, double* w) {
   if (!c || !v || !w || tend < 0) return CFG_E_ARG;
+  if (c->nranks > 1) return single_only(c, "cfg_arnoldi_matvec");
   cudaSetDevice(c->dev);
   const Geom& g = c->g;
   const int np = 3 * g.ny1;
@@ -1521,6 +1628,7 @@ static int start_io(cfg_ctx* c, size_t bytes, F write) {
 
 int cfg_save_velocity(cfg_ctx* c, const char* path) {
   if (!c || !path) return CFG_E_ARG;
+  if (c->nranks > 1) return single_only(c, "cfg_save_velocity");
   cudaSetDevice(c->dev);
   int r = cfg_wait_io(c);
   if (r) return r;
@@ -1544,6 +1652,7 @@ int cfg_save_velocity(cfg_ctx* c, const char* path) {
 
 int cfg_read_velocity(cfg_ctx* c, const char* path) {
   if (!c || !path) return CFG_E_ARG;
+  if (c->nranks > 1) return single_only(c, "cfg_read_velocity");
   cudaSetDevice(c->dev);
   int r = cfg_wait_io(c);
   if (r) return r;
@@ -1577,6 +1686,7 @@ int cfg_read_velocity(cfg_ctx* c, const char* path) {
 
 int cfg_write_vtk(cfg_ctx* c, const char* path) {
   if (!c || !path) return CFG_E_ARG;
+  if (c->nranks > 1) return single_only(c, "cfg_write_vtk");
   cudaSetDevice(c->dev);
   int r = cfg_wait_io(c);
   if (r) return r;
@@ -1687,6 +1797,7 @@ static int postproc(cfg_ctx* c, uint32_t* out) {
 
 int cfg_write_vtk_derived(cfg_ctx* c, const char* path) {
   if (!c || !path) return CFG_E_ARG;
+  if (c->nranks > 1) return single_only(c, "cfg_write_vtk_derived");
   cudaSetDevice(c->dev);
   int r = cfg_wait_io(c);
   if (r) return r;
@@ -1708,6 +1819,7 @@ int cfg_write_vtk_derived(cfg_ctx* c, const char* path) {
 
 int cfg_plane_statistics(cfg_ctx* c, double* stats) {
   if (!c || !stats) return CFG_E_ARG;
+  if (c->nranks > 1) return single_only(c, "cfg_plane_statistics");
   cudaSetDevice(c->dev);
   int r = ensure_postproc(c);
   if (r) return r;
@@ -1742,6 +1854,7 @@ int cfg_plane_statistics(cfg_ctx* c, double* stats) {
 // init_buffer (PFC/init_jet_buffer.f90:358-483) on the device
 int cfg_init_buffer(cfg_ctx* c, const cfg_fringe* f) {
   if (!c || !f) return CFG_E_ARG;
+  if (c->nranks > 1) return single_only(c, "cfg_init_buffer");
   cudaSetDevice(c->dev);
   const Geom& g = c->g;
   if (f->xfringe == 0 && f->zfringe == 0) {
@@ -1792,6 +1905,7 @@ int cfg_init_buffer(cfg_ctx* c, const cfg_fringe* f) {
 
 int cfg_get_buffer(cfg_ctx* c, double* buffer, double* target_inflow) {
   if (!c) return CFG_E_ARG;
+  if (c->nranks > 1) return single_only(c, "cfg_get_buffer");
   cudaSetDevice(c->dev);
   const Geom& g = c->g;
   const size_t np = (size_t)g.nx2 * g.nz2;
@@ -1813,3 +1927,234 @@ int cfg_get_buffer(cfg_ctx* c, double* buffer, double* target_inflow) {
   return CFG_OK;
 }
 
+
+// ----------------------------------------------------------------------------
+// Multi-rank runs: one context per rank, each holding a kx slab of the
+// spectral state and a z2 slab of the physical planes (distribute_data,
+// PFC/setup.f90:298-437).  The two MPI_ALLTOALLV transposes of the reference's
+// x-z transforms (PFC/transform.f90:345-409, 573-690) are the scatter stores
+// of k_zinv_r and k_flux_r into the owners' buffers (peer memory when the
+// ranks sit on different GPUs); a barrier of events separates the phases.
+
+struct cfg_group {
+  std::vector<cfg_ctx*> r;
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> nx_proc, x_start, nz_proc, z_start;
+};
+
+int cfg_partition(int nx, int nz, int nz2, int nproc, int* nx_proc, int* x_start, int* nz_proc, int* z_start,
+                  int* nz_small_proc, int* z_small_start) {
+  if (nx < 2 || nz < 1 || nz2 < nz || nproc < 1) return CFG_E_ARG;
+  // the first (n mod nproc) ranks take one more column / row
+  const int nxh = nx / 2 + 1;
+  const int xl = nxh % nproc, zl = nz2 % nproc, sl = nz % nproc;
+  int xs = 0, zs = 0, ss = 0;
+  for (int n = 0; n < nproc; ++n) {
+    const int a = (nxh - xl) / nproc + (n < xl ? 1 : 0);
+    const int b = (nz2 - zl) / nproc + (n < zl ? 1 : 0);
+    const int d = (nz - sl) / nproc + (n < sl ? 1 : 0);
+    if (nx_proc) nx_proc[n] = a;
+    if (x_start) x_start[n] = xs;
+    if (nz_proc) nz_proc[n] = b;
+    if (z_start) z_start[n] = zs;
+    if (nz_small_proc) nz_small_proc[n] = d;
+    if (z_small_start) z_small_start[n] = ss;
+    xs += a;
+    zs += b;
+    ss += d;
+  }
+  return CFG_OK;
+}
+
+static int group_barrier(cfg_group* G) {
+  const int n = (int)G->r.size();
+  if (n < 2) return CFG_OK;
+  for (int i = 0; i < n; ++i) {
+    cudaSetDevice(G->r[i]->dev);
+    if (cudaEventRecord(G->ev[i], G->r[i]->st) != cudaSuccess) return fail(G->r[i], CFG_E_CUDA, "barrier record");
+  }
+  for (int s = 0; s < n; ++s) {
+    cudaSetDevice(G->r[s]->dev);
+    for (int i = 0; i < n; ++i)
+      if (i != s && cudaStreamWaitEvent(G->r[s]->st, G->ev[i], 0) != cudaSuccess)
+        return fail(G->r[s], CFG_E_CUDA, "barrier wait");
+  }
+  return CFG_OK;
+}
+
+void cfg_group_destroy(cfg_group* G) {
+  if (!G) return;
+  for (size_t i = 0; i < G->r.size(); ++i) {
+    if (!G->r[i]) continue;
+    cudaSetDevice(G->r[i]->dev);
+    cudaStreamSynchronize(G->r[i]->st);
+  }
+  for (size_t i = 0; i < G->ev.size(); ++i)
+    if (G->ev[i]) {
+      cudaSetDevice(G->r[i]->dev);
+      cudaEventDestroy(G->ev[i]);
+    }
+  for (cfg_ctx* c : G->r) cfg_destroy(c);
+  delete G;
+}
+
+int cfg_group_create(const cfg_params* p, const cfg_grid* gr, int nranks, const int* devices, cfg_group** out) {
+  if (!p || !gr || !out || nranks < 1 || nranks > 64) return CFG_E_ARG;
+  *out = nullptr;
+  if (p->ctrlu != 0.0 || p->ctrlw != 0.0) {
+    fprintf(stderr, "cfg_group_create: wall feedback (ctrlu, ctrlw) needs a single context\n");
+    return CFG_E_ARG;
+  }
+  cfg_group* G = new cfg_group();
+  const int n = nranks;
+  G->nx_proc.resize(n); G->x_start.resize(n); G->nz_proc.resize(n); G->z_start.resize(n);
+  cfg_partition(p->nx, p->nz, p->nz2, n, G->nx_proc.data(), G->x_start.data(), G->nz_proc.data(), G->z_start.data(),
+                nullptr, nullptr);
+  for (int i = 0; i < n; ++i) {
+    // every rank needs a kx column, and its z2 rows in whole tiles of the
+    // x-stage kernels (8 rows)
+    if (G->nx_proc[i] < 1 || G->nz_proc[i] < 8 || G->nz_proc[i] % 8 != 0) {
+      fprintf(stderr, "cfg_group_create: rank %d gets %d kx columns and %d z2 rows (needs >= 1 and a multiple of 8)\n",
+              i, G->nx_proc[i], G->nz_proc[i]);
+      delete G;
+      return CFG_E_ARG;
+    }
+  }
+  G->r.assign(n, nullptr);
+  G->ev.assign(n, nullptr);
+  for (int i = 0; i < n; ++i) {
+    cfg_params pi = *p;
+    pi.device = devices ? devices[i] : p->device;
+    SlabPart sp{i, n, G->x_start[i], G->nx_proc[i], G->z_start[i], G->nz_proc[i]};
+    int r = create_impl(&pi, gr, &sp, &G->r[i]);
+    if (r) { cfg_group_destroy(G); return r; }
+    cfg_ctx* c = G->r[i];
+    if (n > 1 && !(c->split_x && c->fast_z)) {
+      fprintf(stderr, "cfg_group_create: transform lengths %d x %d have no register-FFT kernels\n", p->nx2, p->nz2);
+      cfg_group_destroy(G);
+      return CFG_E_ARG;
+    }
+    cudaSetDevice(c->dev);
+    if (cudaEventCreateWithFlags(&G->ev[i], cudaEventDisableTiming) != cudaSuccess) {
+      cfg_group_destroy(G);
+      return CFG_E_CUDA;
+    }
+  }
+  if (n > 1) {
+    // peer access between the ranks' GPUs
+    for (int s = 0; s < n; ++s)
+      for (int i = 0; i < n; ++i) {
+        const int ds = G->r[s]->dev, di = G->r[i]->dev;
+        if (ds == di) continue;
+        int can = 0;
+        cudaDeviceCanAccessPeer(&can, ds, di);
+        if (!can) {
+          fprintf(stderr, "cfg_group_create: GPU %d cannot reach GPU %d\n", ds, di);
+          cfg_group_destroy(G);
+          return CFG_E_CUDA;
+        }
+        cudaSetDevice(ds);
+        const cudaError_t e = cudaDeviceEnablePeerAccess(di, 0);
+        if (e != cudaSuccess && e != cudaErrorPeerAccessAlreadyEnabled) {
+          cudaGetLastError();
+          fprintf(stderr, "cfg_group_create: peer access %d -> %d failed\n", ds, di);
+          cfg_group_destroy(G);
+          return CFG_E_CUDA;
+        }
+        cudaGetLastError();
+      }
+    // scatter tables of each rank
+    const int nz2 = p->nz2, nxh = p->nx / 2 + 1;
+    std::vector<int> zown(nz2), xown(nxh);
+    for (int i = 0; i < n; ++i) {
+      for (int z = G->z_start[i]; z < G->z_start[i] + G->nz_proc[i]; ++z) zown[z] = i;
+      for (int x = G->x_start[i]; x < G->x_start[i] + G->nx_proc[i]; ++x) xown[x] = i;
+    }
+    for (int s = 0; s < n; ++s) {
+      cfg_ctx* c = G->r[s];
+      const size_t cs = csize(c);
+      std::vector<unsigned long long> tab((size_t)2 * nz2 + 2 * nxh);
+      unsigned long long* zdst = tab.data();
+      long long* zpitch = reinterpret_cast<long long*>(zdst + nz2);
+      unsigned long long* xdst = zdst + 2 * nz2;
+      long long* xpitch = reinterpret_cast<long long*>(xdst + nxh);
+      for (int z = 0; z < nz2; ++z) {
+        const cfg_ctx* o = G->r[zown[z]];
+        zdst[z] = (unsigned long long)((const char*)o->T1 + cs * (size_t)(z - o->z0s));
+        zpitch[z] = o->gP.nz2;
+      }
+      for (int x = 0; x < nxh; ++x) {
+        const cfg_ctx* o = G->r[xown[x]];
+        xdst[x] = (unsigned long long)((const char*)o->T2 + cs * ((size_t)(x - o->g.kx0) * nz2 + c->z0s));
+        xpitch[x] = (long long)o->g.nxh * nz2;
+      }
+      cudaSetDevice(c->dev);
+      std::vector<unsigned long long*> peers;
+      for (int i = 0; i < n; ++i)
+        if (i != s) peers.push_back(G->r[i]->cflbits);
+      if (cudaMalloc(&c->scat_tab, sizeof(unsigned long long) * tab.size()) != cudaSuccess ||
+          cudaMalloc(&c->cfl_peers, sizeof(unsigned long long*) * peers.size()) != cudaSuccess) {
+        cfg_group_destroy(G);
+        return CFG_E_NOMEM;
+      }
+      cudaMemcpy(c->scat_tab, tab.data(), sizeof(unsigned long long) * tab.size(), cudaMemcpyHostToDevice);
+      cudaMemcpy(c->cfl_peers, peers.data(), sizeof(unsigned long long*) * peers.size(), cudaMemcpyHostToDevice);
+      const unsigned long long* d = (const unsigned long long*)c->scat_tab;
+      c->scat.n = n;
+      c->scat.zdst = d;
+      c->scat.zpitch = reinterpret_cast<const long long*>(d + nz2);
+      c->scat.xdst = d + 2 * nz2;
+      c->scat.xpitch = reinterpret_cast<const long long*>(d + 2 * nz2 + nxh);
+      c->n_cfl_peers = n - 1;
+    }
+  }
+  *out = G;
+  return CFG_OK;
+}
+
+int cfg_group_size(const cfg_group* G) { return G ? (int)G->r.size() : 0; }
+
+cfg_ctx* cfg_group_rank(cfg_group* G, int rank) {
+  if (!G || rank < 0 || rank >= (int)G->r.size()) return nullptr;
+  return G->r[rank];
+}
+
+int cfg_group_timestep(cfg_group* G, int nsteps) {
+  if (!G || nsteps < 0) return CFG_E_ARG;
+  const int n = (int)G->r.size();
+  int r;
+  for (int s = 0; s < nsteps; ++s) {
+    for (cfg_ctx* c : G->r) {
+      cudaSetDevice(c->dev);
+      c->step = c->step < 0 ? 1 : c->step + 1;
+      if ((r = DISPATCH(c, boundary(c)))) return r;
+    }
+    for (int rk = 1; rk <= 3; ++rk) {
+      for (int ph = 1; ph <= 3; ++ph) {
+        for (cfg_ctx* c : G->r) {
+          cudaSetDevice(c->dev);
+          if ((r = DISPATCH(c, nl_phase(c, c->step, rk, false, ph)))) return r;
+          if (ph == 3 && (r = DISPATCH(c, rhs(c, rk, 0)))) return r;
+        }
+        if (ph < 3 && (r = group_barrier(G))) return r;
+      }
+    }
+    for (cfg_ctx* c : G->r) {
+      cudaSetDevice(c->dev);
+      prof_begin(c, "k_advance_time");
+      k_advance_time<<<1, 1, 0, c->st>>>(c->sc);
+      CKL();
+    }
+  }
+  (void)n;
+  return CFG_OK;
+}
+
+int cfg_group_synchronize(cfg_group* G) {
+  if (!G) return CFG_E_ARG;
+  for (cfg_ctx* c : G->r) {
+    const int r = cfg_synchronize(c);
+    if (r) return r;
+  }
+  return CFG_OK;
+}

@@ -27,6 +27,24 @@ struct Geom {
   int nxh;   // nx/2+1 Fourier columns in x
   int ny1;   // ny+1 planes
   int nw;    // nz*nxh wavenumbers
+  // slab of a multi-rank run (PFC/setup.f90:298-437 split kx in Fourier
+  // space): global index of the first local kx column and the global column
+  // count; 0 and nxh for one rank
+  int kx0, nxh_all;
+};
+
+// Scatter targets of the two transposes of a multi-rank run.  The inverse z
+// transform of each rank writes element z2 of hybrid row R to the rank that
+// owns z2, at zdst[z2] + R * zpitch[z2] (complex elements); the flux kernel
+// writes column kx of x-transformed row R to the rank that owns kx, at
+// xdst[kx] + R * xpitch[kx].  Addresses are byte addresses in the owners'
+// buffers (peer memory on other GPUs).  n == 0: one rank, local layouts.
+struct Scatter {
+  int n;
+  const unsigned long long* zdst;
+  const long long* zpitch;
+  const unsigned long long* xdst;
+  const long long* xpitch;
 };
 
 // FFT plan for one length: Stockham passes, radices in {2,3,4,8}.

@@ -24,6 +24,7 @@ struct P1Launch {
   int lin;
   void* P;              // physical planes (split x stage)
   int FZR;              // z rows per k_flux_r block (2 or 4)
+  Scatter sc;           // transposes of a multi-rank run (n == 0: one rank)
   cudaStream_t st;
 };
 
@@ -31,7 +32,7 @@ struct P1Launch {
 // Returns 0, or -1 when the length is not compiled in, or -2 on a launch error.
 int p1_fast_launch(int which, int n, bool f32, const P1Launch& a);
 // shared memory bytes of kernel `which` at length n with its tile parameter
-// (YB for 0/2, ZR for 1 and 4, unused for 3); 0 when unsupported.
+// (YB for 0/2, ZR for 1 and 4, the z2 row count for 3); 0 when unsupported.
 size_t p1_fast_smem(int which, int n, bool f32, int param, int nxh, int nz);
 
 }  // namespace cfd

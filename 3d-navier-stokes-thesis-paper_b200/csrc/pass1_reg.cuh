@@ -55,7 +55,7 @@ template <typename T> struct ZRawPad {   // 32 bytes between component blocks
 template <typename T, int NZ2>
 __global__ void __launch_bounds__(288, sizeof(T) == 4 ? 3 : 1) k_zinv_r(const cplx_t<T>* __restrict__ vel,
                                                 cplx_t<T>* __restrict__ T1, Geom g,
-                                                const cplx_t<T>* __restrict__ twz, int YB) {
+                                                const cplx_t<T>* __restrict__ twz, int YB, Scatter sc) {
   using C = cplx_t<T>;
   constexpr int N1 = Split<NZ2>::N1, N2 = Split<NZ2>::N2, PITCH = N2 + 1, SEQ = SeqPitch<NZ2>::V;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(288, sizeof(T) == 4 ? 3 : 1) k_zinv_r(const cp
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   __syncthreads();
   const T half = (T)0.5;
-  const bool halve_x = (g.nx2 > g.nx) && (kx == NXH - 1) && (NZ2 > NZ);
+  const bool halve_x = (g.nx2 > g.nx) && (g.kx0 + kx == g.nxh_all - 1) && (NZ2 > NZ);
   // stage 1: consecutive threads take consecutive sequences (planes fastest)
   for (int t = threadIdx.x; t < nseq * N2; t += blockDim.x) {
     const int s = t % nseq, n2 = t / nseq;
@@ -130,10 +130,18 @@ __global__ void __launch_bounds__(288, sizeof(T) == 4 ? 3 : 1) k_zinv_r(const cp
 #pragma unroll
     for (int n2 = 0; n2 < N2; ++n2) u[n2] = y[n2];
     SmallFFT<T, N2, +1>::template run<1>(u);
-    if (jj < nj) {
+    if (jj < nj && sc.n == 0) {
       C* out = T1 + (((size_t)(j0 + jj) * 3 + c) * NXH + kx) * NZ2;
 #pragma unroll
       for (int k2 = 0; k2 < N2; ++k2) out[k1 + N1 * k2] = u[k2];
+    } else if (jj < nj) {
+      // transpose to z2 slabs: element z2 goes to the rank that owns it
+      const long long row = ((long long)(j0 + jj) * 3 + c) * g.nxh_all + g.kx0 + kx;
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) {
+        const int z = k1 + N1 * k2;
+        reinterpret_cast<C*>(__ldg(sc.zdst + z))[row * __ldg(sc.zpitch + z)] = u[k2];
+      }
     }
   }
 }
@@ -209,7 +217,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_zfwd_r(const cp
   }
   __syncthreads();
   const T scale = (T)(1.0 / ((double)g.nx2 * (double)g.nz2));
-  const T wsc = (kx == NXH - 1) ? (T)2 * scale : scale;
+  const T wsc = (g.kx0 + kx == g.nxh_all - 1) ? (T)2 * scale : scale;
   for (int idx = threadIdx.x; idx < NZ * 3 * YB; idx += blockDim.x) {
     const int jj = idx % YB, e = (idx / YB) % 3, kz = idx / (3 * YB);
     const int j = j0 + jj;
@@ -616,7 +624,7 @@ template <typename T, int NX2, int ZR, int NT, bool LIN>
 __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT == 256 ? 1 : 2)) k_flux_r(const T* __restrict__ P, cplx_t<T>* __restrict__ T2, Geom g,
                                                const cplx_t<T>* __restrict__ twx, GridDev gd,
                                                const T* __restrict__ fringe, int has_fringe,
-                                               unsigned long long* __restrict__ cflbits, int do_cfl) {
+                                               unsigned long long* __restrict__ cflbits, int do_cfl, Scatter sc) {
   using C = cplx_t<T>;
   constexpr int N1 = Split<NX2>::N1, N2 = Split<NX2>::N2, PITCH = N2 + 1, SEQ = SeqPitch<NX2>::V;
   constexpr int N = NX2;
@@ -788,7 +796,10 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT
     const int r = idx % ZR, kx = idx / ZR;
     const T kxv = skx[kx];
     const int km = (kx == 0) ? 0 : N - kx;
-#define OUT(e, part) T2[((base + (e) * 2 + (part)) * NXH + kx) * NZ2 + z0 + r]
+    // one rank: local layout; several: column kx goes to the rank that owns it
+    C* const od = sc.n ? reinterpret_cast<C*>(__ldg(sc.xdst + kx)) + z0 + r : T2 + (size_t)kx * NZ2 + z0 + r;
+    const size_t op = sc.n ? (size_t)__ldg(sc.xpitch + kx) : (size_t)NXH * NZ2;
+#define OUT(e, part) od[(base + (e) * 2 + (part)) * op]
 #pragma unroll
     for (int e4 = 0; e4 < 4; ++e4) {
       if (e4 == 2 && !veq) continue;

@@ -285,6 +285,46 @@ int cfg_profile_enable(cfg_ctx *c, int on);
 int cfg_profile_read(cfg_ctx *c, int idx, char *name, int namelen, int *launches,
                      double *total_ms);
 
+/* ---- multi-rank runs (slab decomposition of one field) ----------------
+ *
+ * distribute_data (PFC/setup.f90:298-437): the split of the nx/2+1 Fourier
+ * columns (nx_proc, x_start), of the nz2 physical z rows (nz_proc, z_start)
+ * and of the nz undealiased z rows (nz_small_proc, z_small_start) among
+ * nproc ranks -- the first (n mod nproc) ranks take one more.  Each output
+ * array has nproc entries; any may be NULL. */
+int cfg_partition(int nx, int nz, int nz2, int nproc, int *nx_proc, int *x_start,
+                  int *nz_proc, int *z_start, int *nz_small_proc, int *z_small_start);
+
+/* A group of nranks contexts that advance one field together, rank i owning
+ * the Fourier columns [x_start[i], x_start[i] + nx_proc[i]) of the state and
+ * the z2 rows [z_start[i], ...) of the physical planes, as the reference's
+ * MPI ranks do (PFC/main_mpi.f90 under mpirun).  It replaces the MPI
+ * decomposition of pass1::nonlinear: the two MPI_ALLTOALLV transposes of
+ * the x-z transforms (PFC/transform.f90:345-409, 573-690) become stores of
+ * the z and flux kernels straight into the owning rank's buffers (peer
+ * memory when the ranks are on different GPUs, peer access enabled here),
+ * and the CFL MPI_ALLREDUCE (PFC/pass1.f90:202-250) a fold of the other
+ * ranks' per-plane maxima.  devices[i] is rank i's GPU (NULL: p->device
+ * for all; ranks may share a GPU).  Each rank needs >= 1 kx column and a
+ * multiple of 8 z2 rows; ctrlu = ctrlw = 0 (the wall feedback transforms
+ * whole planes).  cfg_group_rank gives rank i's context for
+ * cfg_upload_state / cfg_download_state (arrays of the rank's local sizes,
+ * data1(nz, nx_proc[i], ny+1, 3) as in PFC/setup.f90:447-449),
+ * cfg_set_scalars, cfg_get_scalars, cfg_set_wall_bc, cfg_rhs_solve,
+ * cfg_status; entry points that need whole planes return CFG_E_ARG on a
+ * rank of a group of two or more. */
+typedef struct cfg_group cfg_group;
+int cfg_group_create(const cfg_params *p, const cfg_grid *g, int nranks, const int *devices,
+                     cfg_group **out);
+int cfg_group_size(const cfg_group *grp);
+cfg_ctx *cfg_group_rank(cfg_group *grp, int rank);
+/* timestep (PFC/main_mpi.f90:55-116) of all ranks: per RK substep the
+ * inverse z transforms, a barrier, the x stages, a barrier, the forward z
+ * transforms and rhs_solve.  Asynchronous. */
+int cfg_group_timestep(cfg_group *grp, int nsteps);
+int cfg_group_synchronize(cfg_group *grp);
+void cfg_group_destroy(cfg_group *grp);
+
 /* cfg_xz_c2r_noalloc -- no counterpart in the reference.  The inverse x-z
  * transform of one plane (the semantics of cfg_xz_c2r /
  * xz_fft_complex_to_real) for callers that cannot allocate device memory:

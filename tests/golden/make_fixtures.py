@@ -4,6 +4,11 @@ project's shipped data (run in a container where the reference is mounted).
 makegrid_ny200.json: y(200), yh(201) written by output_grids
 (PFC/setup.f90:1331-1359) for ny=200 with STRETCH=2.75, as printed in
 PFC/makegrid.m (format f16.8).
+
+partition_nproc24.json: the partition table distribute_data
+(PFC/setup.f90:298-437) printed for Nx=128, Nz=64 (Nz2=96) on 24 ranks in
+PFC/diagnostics.txt (the leftover line and the per-rank nx_proc, x_start,
+nz_proc, z_start, nz_small, z_small columns).
 """
 import json
 import os
@@ -26,6 +31,24 @@ def main():
     with open(os.path.join(HERE, "makegrid_ny200.json"), "w") as f:
         json.dump(out, f)
     print("wrote makegrid_ny200.json", len(out["y"]), len(out["yh"]))
+
+    lines = open(os.path.join(REF, "ParallelFortran-Code", "diagnostics.txt")).read().splitlines()
+    head = next(i for i, l in enumerate(lines) if l.strip().startswith("Proc   nx_proc"))
+    left = [int(v) for v in lines[head - 1].split()]
+    rows = []
+    for l in lines[head + 1:]:
+        f = l.split()
+        if len(f) != 7:
+            break
+        rows.append([int(v) for v in f])
+    cols = ["proc", "nx_proc", "x_start", "nz_proc", "z_start", "nz_small_proc", "z_small_start"]
+    part = {"source": "ParallelFortran-Code/diagnostics.txt", "nx": 128, "nz": 64, "nz2": 96, "nproc": len(rows),
+            "xleft_zleft_zsmallleft": left}
+    for k, name in enumerate(cols):
+        part[name] = [r[k] for r in rows]
+    with open(os.path.join(HERE, "partition_nproc24.json"), "w") as f:
+        json.dump(part, f)
+    print("wrote partition_nproc24.json", len(rows))
 
 
 if __name__ == "__main__":

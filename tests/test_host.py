@@ -132,3 +132,35 @@ def test_arnoldi_driver_eigenvalues(cf):
     np.testing.assert_allclose(lam.real, [-0.01, -0.2, -0.35], rtol=1e-8)
     assert np.abs(lam.imag).max() < 1e-12
     assert vec.shape == (f.mu.size, 3)
+
+
+def test_partition_matches_reference_table(cf):
+    """cfg_partition against the distribute_data table the reference printed
+    for Nx=128, Nz=64 (Nz2=96) on 24 ranks (PFC/diagnostics.txt:17-43)."""
+    import json
+    gold = json.load(open(os.path.join(ROOT, "tests", "golden", "partition_nproc24.json")))
+    part = cf.partition(gold["nx"], gold["nz"], gold["nz2"], gold["nproc"])
+    for k in cf.PARTITION_KEYS:
+        assert list(part[k]) == gold[k], k
+    nxh = gold["nx"] // 2 + 1
+    assert gold["xleft_zleft_zsmallleft"] == [nxh % 24, gold["nz2"] % 24, gold["nz"] % 24]
+
+
+@pytest.mark.parametrize("nx,nz,nproc", [(256, 256, 8), (32, 32, 5), (6, 4, 4), (384, 384, 7)])
+def test_partition_covers_grid(cf, nx, nz, nproc):
+    nz2 = 3 * nz // 2
+    p = cf.partition(nx, nz, nz2, nproc)
+    for cnt, start, total in (("nx_proc", "x_start", nx // 2 + 1), ("nz_proc", "z_start", nz2),
+                              ("nz_small_proc", "z_small_start", nz)):
+        c, s = p[cnt], p[start]
+        assert c.sum() == total and s[0] == 0
+        assert np.all(s[1:] == np.cumsum(c)[:-1])
+        assert c.max() - c.min() <= 1 and np.all(np.diff(c) <= 0)
+
+
+def test_group_rejects_partition_without_whole_tiles(cf):
+    # 48 z2 rows on 4 ranks: 12 rows each, not a multiple of 8 (refused on
+    # the host before any device work)
+    grid = cf.Grid(32, 33, 32, stretch=1.5)
+    with pytest.raises(cf.ChanflowError):
+        cf.Group(grid, 4)
