@@ -12,6 +12,13 @@ Metric: Mpts*steps/s with Mpts = nx*ny*nz = 12.648.
 With N > 1 (torchrun, one process per GPU) every rank advances its own
 independent domain (replicas, weak scaling); the timed region is bracketed by a
 barrier and the maximum device time over ranks is used.
+
+  python bench.py --slab P [--steps K] [--warmup W]
+
+runs ONE field split into P slab ranks (cfg_group, one process, ranks placed
+round robin on the visible GPUs; several ranks may share a GPU): strong
+scaling of a single domain, timed with an event pair on every rank's stream,
+maximum over ranks.
 """
 import argparse
 import json
@@ -251,6 +258,49 @@ def timed_steps(torch, flow, steps, profile=False):
     return e0.elapsed_time(e1), n1 - n0, prof
 
 
+def run_slab(args):
+    import torch
+    import __graft_entry__
+    cf = __graft_entry__.load_package()
+    nx, ny, nz, K, W, P = args.nx, args.ny, args.nz, args.steps, args.warmup, args.slab
+    ndev = max(1, torch.cuda.device_count())
+    devs = [i % ndev for i in range(P)]
+    # the initial state (divergence removal and initial pressure need whole
+    # planes) is made on one context and split among the ranks
+    one = make_flow(cf, nx, ny, nz, cf.MIXED, 0)
+    st, sc = one.download_state(), one.scalars()
+    grid = one.grid
+    one.close()
+    grp = cf.Group(grid, P, devices=devs, re=RE, dt=DT, fix_mass=1, precision=cf.MIXED)
+    grp.upload_state(*st)
+    grp.set_scalars(sc["t_total"], sc["dt"], sc["p_grad"], sc["d_um_dy"])
+    grp.timestep(W)
+    grp.synchronize()
+    ev = []
+    for i, f in enumerate(grp.ranks):
+        with torch.cuda.device(devs[i]):
+            s_ = torch.cuda.ExternalStream(f.stream_ptr())
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev.append((s_, e0, e1))
+    for s_, e0, _ in ev:
+        e0.record(s_)
+    grp.timestep(K)
+    for s_, _, e1 in ev:
+        e1.record(s_)
+    grp.synchronize()
+    ms = max(e0.elapsed_time(e1) for _, e0, e1 in ev)
+    status = grp.status()
+    grp.close()
+    cfg = workload_config(nx, ny, nz, "mixed")
+    cfg["parallelism"] = f"slab x{P}: one field, {P} ranks on {len(set(devs))} GPU(s), one process"
+    line = {"metric": METRIC, "value": mpts(nx, ny, nz) * K / (ms / 1e3), "unit": UNIT,
+            "n_gpus": len(set(devs)), "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": cfg, "status": status}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_ours(args):
     import torch
     import __graft_entry__
@@ -416,11 +466,14 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--slab", type=int, default=0, help="one field in P slab ranks (one process)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.slab > 0:
+        return run_slab(args)
     return run_ours(args)
 
 
