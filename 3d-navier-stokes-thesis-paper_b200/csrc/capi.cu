@@ -564,7 +564,7 @@ struct Impl {
       a.vel = c->vel; a.cru = c->cru; a.prs = c->prs;
       a.cbc_top = (const C*)c->cbc + 3 * (size_t)g.nw; a.cbc_bot = c->cbc;
       a.g = g; a.gd = c->gd; a.sc = c->sc; a.rkt = c->rkt; a.rk = rk; a.re = c->p.re;
-      a.wlist = c->wl_fast; a.nlist = c->n_fast; a.warps = sizeof(T) == 4 ? 4 : 2; a.lanes = c->rhs2_lanes;
+      a.wlist = c->wl_fast; a.nlist = c->n_fast; a.warps = sizeof(T) == 4 ? 3 : 2; a.lanes = c->rhs2_lanes;
       a.tbl = c->rhs2_tbl;
       a.st = c->st;
       prof_begin(c, "k_rhs");

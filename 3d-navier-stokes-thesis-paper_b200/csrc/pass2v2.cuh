@@ -58,102 +58,74 @@ __device__ __forceinline__ void pcr_step(T& A, T& B, T& Cc, cplx_t<T> (&Fv)[NR],
 // Partition + PCR solve over the G lanes of a lane group, NR right-hand sides.
 // Row j = g*M + i of lane g:  a[i] x_{j-1} + b[i] x_j + c[i] x_{j+1} = f[r][i].
 // Rows past the system are identity rows.  Solutions overwrite f.
+// Each lane eliminates its first M-1 rows in terms of the two interface
+// unknowns next to them -- x_L, the previous lane's last row, and x_E, its own
+// last row: x_i = y_i - x_L v_i - x_E w_i (Thomas on the M-1 rows with the
+// right-hand sides f, a_0 e_0 and c_{M-2} e_{M-2}).  The last rows then form a
+// tridiagonal system of G unknowns, one per lane, solved by cyclic reduction
+// across the lanes (log2 G shuffle steps); the interior rows follow.
 template <typename T, int M, int G, int NR>
 __device__ __forceinline__ void tri_group_solve(T (&a)[M], T (&b)[M], T (&c)[M],
                                                 cplx_t<T> (&f)[NR][M], int g) {
   using C = cplx_t<T>;
   static_assert(M >= 2, "at least two rows per lane");
-  T ap[M], cq[M], rb[M];
-  ap[0] = 0;
-  ap[1] = a[1];
+  T v[M], w[M], rb[M];
+  // forward sweep over the first M-1 rows
   rb[0] = rcpv(b[0]);
-  rb[1] = rcpv(b[1]);
+  v[0] = a[0];
 #pragma unroll
-  for (int i = 2; i < M; ++i) {
-    const T rr = a[i] * rb[i - 1];
-    ap[i] = -rr * ap[i - 1];
-    b[i] = b[i] - rr * c[i - 1];
+  for (int i = 1; i < M - 1; ++i) {
+    const T m = a[i] * rb[i - 1];
+    b[i] = b[i] - m * c[i - 1];
     rb[i] = rcpv(b[i]);
+    v[i] = -m * v[i - 1];
 #pragma unroll
-    for (int r = 0; r < NR; ++r) f[r][i] = mk<C>(f[r][i].x - rr * f[r][i - 1].x, f[r][i].y - rr * f[r][i - 1].y);
+    for (int r = 0; r < NR; ++r) f[r][i] = mk<C>(f[r][i].x - m * f[r][i - 1].x, f[r][i].y - m * f[r][i - 1].y);
   }
+  // backward sweep: y (in f), v, w
+  w[M - 2] = c[M - 2] * rb[M - 2];
+  v[M - 2] = v[M - 2] * rb[M - 2];
 #pragma unroll
-  for (int i = 0; i < M; ++i) cq[i] = 0;
-  if (M > 2) cq[M - 2] = c[M - 2];
+  for (int r = 0; r < NR; ++r) f[r][M - 2] = mk<C>(f[r][M - 2].x * rb[M - 2], f[r][M - 2].y * rb[M - 2]);
 #pragma unroll
-  for (int i = M - 3; i >= 1; --i) {
-    const T rr = c[i] * rb[i + 1];
-    ap[i] = ap[i] - rr * ap[i + 1];
-    cq[i] = -rr * cq[i + 1];
+  for (int i = M - 3; i >= 0; --i) {
+    w[i] = -c[i] * w[i + 1] * rb[i];
+    v[i] = (v[i] - c[i] * v[i + 1]) * rb[i];
 #pragma unroll
-    for (int r = 0; r < NR; ++r) f[r][i] = mk<C>(f[r][i].x - rr * f[r][i + 1].x, f[r][i].y - rr * f[r][i + 1].y);
+    for (int r = 0; r < NR; ++r)
+      f[r][i] = mk<C>((f[r][i].x - c[i] * f[r][i + 1].x) * rb[i], (f[r][i].y - c[i] * f[r][i + 1].y) * rb[i]);
   }
-  T A0 = a[0], B0 = b[0], C0 = c[0];
-  C F0[NR];
-#pragma unroll
-  for (int r = 0; r < NR; ++r) F0[r] = f[r][0];
-  if (M > 2) {
-    const T rr = c[0] * rb[1];
-    B0 = b[0] - rr * ap[1];
-    C0 = -rr * cq[1];
-#pragma unroll
-    for (int r = 0; r < NR; ++r) F0[r] = mk<C>(f[r][0].x - rr * f[r][1].x, f[r][0].y - rr * f[r][1].y);
-  }
-  T A1 = ap[M - 1], B1 = b[M - 1], C1 = c[M - 1];
-  C F1[NR];
-#pragma unroll
-  for (int r = 0; r < NR; ++r) F1[r] = f[r][M - 1];
+  // interface row (local row M-1) with the next lane's first row substituted
   const unsigned full = 0xffffffffu;
-  {
-    // stride 1: slot 0's lower neighbour is lane g-1 slot 1, slot 1's upper is lane g+1 slot 0
-    T la = __shfl_up_sync(full, A1, 1, G), lb = __shfl_up_sync(full, B1, 1, G), lc = __shfl_up_sync(full, C1, 1, G);
-    T ua = __shfl_down_sync(full, A0, 1, G), ub = __shfl_down_sync(full, B0, 1, G), uc = __shfl_down_sync(full, C0, 1, G);
-    C lf[NR], uf[NR];
+  T vn = __shfl_down_sync(full, v[0], 1, G), wn = __shfl_down_sync(full, w[0], 1, G);
+  C yn[NR];
 #pragma unroll
-    for (int r = 0; r < NR; ++r) {
-      lf[r] = mk<C>(__shfl_up_sync(full, F1[r].x, 1, G), __shfl_up_sync(full, F1[r].y, 1, G));
-      uf[r] = mk<C>(__shfl_down_sync(full, F0[r].x, 1, G), __shfl_down_sync(full, F0[r].y, 1, G));
-    }
-    if (g == 0) {
-      la = 0; lb = 1; lc = 0;
+  for (int r = 0; r < NR; ++r) yn[r] = mk<C>(__shfl_down_sync(full, f[r][0].x, 1, G), __shfl_down_sync(full, f[r][0].y, 1, G));
+  if (g == G - 1) {
+    vn = 0; wn = 0;
 #pragma unroll
-      for (int r = 0; r < NR; ++r) lf[r] = czero<C>();
-    }
-    if (g == G - 1) {
-      ua = 0; ub = 1; uc = 0;
-#pragma unroll
-      for (int r = 0; r < NR; ++r) uf[r] = czero<C>();
-    }
-    const T rB0 = rcpv(B0), rB1 = rcpv(B1);
-    const T k1a = A0 * rcpv(lb), k2a = C0 * rB1;
-    const T k1b = A1 * rB0, k2b = C1 * rcpv(ub);
-    const T nA0 = -k1a * la, nC0 = -k2a * C1, nB0 = B0 - k1a * lc - k2a * A1;
-    const T nA1 = -k1b * A0, nC1 = -k2b * uc, nB1 = B1 - k1b * C0 - k2b * ua;
-#pragma unroll
-    for (int r = 0; r < NR; ++r) {
-      const C nF0 = mk<C>(F0[r].x - k1a * lf[r].x - k2a * F1[r].x, F0[r].y - k1a * lf[r].y - k2a * F1[r].y);
-      const C nF1 = mk<C>(F1[r].x - k1b * F0[r].x - k2b * uf[r].x, F1[r].y - k1b * F0[r].y - k2b * uf[r].y);
-      F0[r] = nF0;
-      F1[r] = nF1;
-    }
-    A0 = nA0; B0 = nB0; C0 = nC0;
-    A1 = nA1; B1 = nB1; C1 = nC1;
+    for (int r = 0; r < NR; ++r) yn[r] = czero<C>();
   }
+  const T aE = a[M - 1], cE = c[M - 1];
+  T A = -aE * v[M - 2];
+  T B = b[M - 1] - aE * w[M - 2] - cE * vn;
+  T Cc = -cE * wn;
+  C F[NR];
 #pragma unroll
-  for (int t = 1; t < G; t <<= 1) {
-    pcr_step<T, G, NR>(A0, B0, C0, F0, t, g);
-    pcr_step<T, G, NR>(A1, B1, C1, F1, t, g);
-  }
-  const T r0 = rcpv(B0), r1 = rcpv(B1);
+  for (int r = 0; r < NR; ++r)
+    F[r] = mk<C>(f[r][M - 1].x - aE * f[r][M - 2].x - cE * yn[r].x, f[r][M - 1].y - aE * f[r][M - 2].y - cE * yn[r].y);
+#pragma unroll
+  for (int t = 1; t < G; t <<= 1) pcr_step<T, G, NR>(A, B, Cc, F, t, g);
+  const T rB = rcpv(B);
 #pragma unroll
   for (int r = 0; r < NR; ++r) {
-    const C x0 = mk<C>(F0[r].x * r0, F0[r].y * r0);
-    const C xl = mk<C>(F1[r].x * r1, F1[r].y * r1);
+    const C xE = mk<C>(F[r].x * rB, F[r].y * rB);
+    C xL = mk<C>(__shfl_up_sync(full, xE.x, 1, G), __shfl_up_sync(full, xE.y, 1, G));
+    if (g == 0) xL = czero<C>();
 #pragma unroll
-    for (int i = 1; i < M - 1; ++i)
-      f[r][i] = mk<C>((f[r][i].x - ap[i] * x0.x - cq[i] * xl.x) * rb[i], (f[r][i].y - ap[i] * x0.y - cq[i] * xl.y) * rb[i]);
-    f[r][0] = x0;
-    f[r][M - 1] = xl;
+    for (int i = 0; i < M - 1; ++i)
+      f[r][i] = mk<C>(f[r][i].x - xL.x * v[i] - xE.x * w[i], f[r][i].y - xL.y * v[i] - xE.y * w[i]);
+    f[r][M - 1] = xE;
   }
 }
 
@@ -190,7 +162,7 @@ __host__ __device__ __forceinline__ int rhs2_ld(int n1) { return (n1 + 1) & ~1; 
 // T is the arithmetic precision, S the storage precision of the state (the
 // mixed path runs its |k| < 4 list with T = double over S = float).
 template <typename T, typename S, int M, int G>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 1) k_rhs2(cplx_t<S>* __restrict__ vel, cplx_t<S>* __restrict__ cru,
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 5 : 1) k_rhs2(cplx_t<S>* __restrict__ vel, cplx_t<S>* __restrict__ cru,
                                               cplx_t<S>* __restrict__ prs,
                                               const cplx_t<S>* __restrict__ cbc_top,
                                               const cplx_t<S>* __restrict__ cbc_bot, Geom g,
