@@ -160,6 +160,11 @@ SYMBOLS = {
     "cfg_group_timestep": (C.c_int, [_VP, C.c_int]),
     "cfg_group_synchronize": (C.c_int, [_VP]),
     "cfg_group_destroy": (None, [_VP]),
+    "cfg_rank_record_size": (C.c_size_t, []),
+    "cfg_rank_create": (C.c_int, [C.POINTER(CfgParams), C.POINTER(CfgGrid), C.c_int, C.c_int, C.POINTER(_VP)]),
+    "cfg_rank_export": (C.c_int, [_VP, _VP]),
+    "cfg_rank_connect": (C.c_int, [_VP, _VP]),
+    "cfg_rank_timestep": (C.c_int, [_VP, C.c_int, C.c_void_p, _VP]),
     "cfh_run_defaults": (None, [C.POINTER(CfhRun)]),
     "cfh_read_flow_dat": (C.c_int, [C.c_char_p, C.POINTER(CfhRun), C.c_char_p, C.c_int]),
     "cfh_grid_alloc": (C.POINTER(CfhGrid), [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
@@ -672,4 +677,74 @@ class Group:
 
     def status(self):
         return [f.status() for f in self.ranks]
+
+
+_BARRIER = C.CFUNCTYPE(C.c_int, C.c_void_p)
+
+
+class Rank(ChannelFlow):
+    """One rank of a multi-process run (cfg_rank_*, one process per GPU as
+    under mpirun): this process's slabs of one field (distribute_data,
+    PFC/setup.f90:298-437); the other ranks' transpose targets are reached
+    through CUDA IPC mappings.  After record()s have been all-gathered and
+    passed to connect(), timestep() advances the field; `barrier` (default
+    torch.distributed.barrier) runs between the phases of every substep and
+    must return once all ranks have called it.  Arrays passed to
+    upload_state are this rank's local slabs, data1(nz, nx_proc, ny+1, 3)."""
+
+    def __init__(self, grid, rank, nranks, re=2500.0, dt=0.005, beta=0.0, cfl_max=0.95, fix_mass=1,
+                 dt_flag=0, precision=FP64, device=0):
+        self.L = load_library()
+        self.grid = grid
+        self.nx, self.ny, self.nz = grid.nx, grid.ny, grid.nz
+        self.nx2, self.nz2 = grid.nx2, grid.nz2
+        self.precision = precision
+        self.rank, self.nranks = rank, nranks
+        self.part = partition(grid.nx, grid.nz, grid.nz2, nranks)
+        self.nxh = int(self.part["nx_proc"][rank])
+        self.x_start = int(self.part["x_start"][rank])
+        self.params = CfgParams(grid.nx, grid.ny, grid.nz, grid.nx2, grid.nz2, re, grid.lx, grid.lz,
+                                beta, dt, cfl_max, fix_mass, dt_flag, 0.0, 0.0, precision, device)
+        g, keep = grid.cfg_grid()
+        h = C.c_void_p()
+        r = self.L.cfg_rank_create(C.byref(self.params), C.byref(g), rank, nranks, C.byref(h))
+        if r != 0:
+            raise ChanflowError(f"cfg_rank_create failed ({ERRORS.get(r, r)})")
+        self.h = h
+        self.step = 0
+
+    def slab(self):
+        """Slice of the global kx index held by this rank."""
+        return slice(self.x_start, self.x_start + self.nxh)
+
+    def record(self):
+        b = C.create_string_buffer(self.L.cfg_rank_record_size())
+        self._chk(self.L.cfg_rank_export(self.h, b))
+        return b.raw
+
+    def connect(self, records):
+        blob = b"".join(records)
+        assert len(blob) == self.nranks * self.L.cfg_rank_record_size()
+        buf = C.create_string_buffer(blob, len(blob))
+        self._chk(self.L.cfg_rank_connect(self.h, buf))
+
+    def timestep(self, nsteps=1, barrier=None):
+        if barrier is None:
+            import torch.distributed as dist
+            barrier = dist.barrier
+        err = []
+
+        def cb(_user):
+            try:
+                barrier()
+                return 0
+            except Exception as e:  # reported after the C call returns
+                err.append(e)
+                return -1
+
+        fn = _BARRIER(cb)
+        r = self.L.cfg_rank_timestep(self.h, nsteps, C.cast(fn, C.c_void_p), None)
+        if err:
+            raise err[0]
+        self._chk(r)
 

@@ -214,6 +214,7 @@ struct cfg_ctx {
   void* scat_tab = nullptr;
   unsigned long long** cfl_peers = nullptr;   // the other ranks' cflbits
   int n_cfl_peers = 0;
+  std::vector<void*> ipc_open;   // other processes' buffers mapped by cfg_rank_connect
 };
 
 // slab of one rank (cfg_group_create); one rank: the whole grid
@@ -978,6 +979,7 @@ void cfg_destroy(cfg_ctx* c) {
   if (c->ev_io_start) cudaEventDestroy(c->ev_io_start);
   if (c->ev_io_done) cudaEventDestroy(c->ev_io_done);
   if (c->st_io) cudaStreamDestroy(c->st_io);
+  for (void* q : c->ipc_open) cudaIpcCloseMemHandle(q);
   void* bufs[] = {c->dgrid, c->fringe, c->vel, c->cru, c->prs, c->mvel64, c->mcru64, c->T1, c->T2, c->P, c->rhs2_tbl, c->rhs2_tbl64, c->jst, c->pp_wy, c->pp_sy, c->pp_acc, c->cbc,
                   c->sc, c->d_um_dy, c->cflp, c->cflbits, c->l2acc, c->divbits, c->plist, c->pw_H,
                   c->pw_phys, c->pw_phys2, c->pw_in, c->stage, c->twx, c->twz, c->twxs, c->twzs,
@@ -1936,6 +1938,71 @@ int cfg_get_buffer(cfg_ctx* c, double* buffer, double* target_inflow) {
 // of k_zinv_r and k_flux_r into the owners' buffers (peer memory when the
 // ranks sit on different GPUs); a barrier of events separates the phases.
 
+// what one rank needs of another: where its T1 / T2 / CFL maxima live (a
+// pointer valid on this rank's GPU: the peer's own, or an IPC mapping) and
+// its slabs
+struct PeerView {
+  const void *T1, *T2;
+  unsigned long long* cfl;
+  int x0, nxl, z0, nzl;
+};
+
+static PeerView view_of(const cfg_ctx* o) {
+  return PeerView{o->T1, o->T2, o->cflbits, o->g.kx0, o->g.nxh, o->z0s, o->gP.nz2};
+}
+
+// scatter tables and CFL peer list of rank c from the views of all ranks
+static int build_scatter(cfg_ctx* c, const std::vector<PeerView>& v) {
+  const int n = (int)v.size(), nz2 = c->g.nz2, nxh = c->g.nxh_all;
+  const size_t cs = csize(c);
+  std::vector<int> zown(nz2, -1), xown(nxh, -1);
+  for (int i = 0; i < n; ++i) {
+    for (int z = v[i].z0; z < v[i].z0 + v[i].nzl && z < nz2; ++z) zown[z] = i;
+    for (int x = v[i].x0; x < v[i].x0 + v[i].nxl && x < nxh; ++x) xown[x] = i;
+  }
+  for (int z = 0; z < nz2; ++z)
+    if (zown[z] < 0) return fail(c, CFG_E_ARG, "z2 row %d has no owner", z);
+  for (int x = 0; x < nxh; ++x)
+    if (xown[x] < 0) return fail(c, CFG_E_ARG, "kx column %d has no owner", x);
+  std::vector<unsigned long long> tab((size_t)2 * nz2 + 2 * nxh);
+  unsigned long long* zdst = tab.data();
+  long long* zpitch = reinterpret_cast<long long*>(zdst + nz2);
+  unsigned long long* xdst = zdst + 2 * nz2;
+  long long* xpitch = reinterpret_cast<long long*>(xdst + nxh);
+  for (int z = 0; z < nz2; ++z) {
+    const PeerView& o = v[zown[z]];
+    zdst[z] = (unsigned long long)((const char*)o.T1 + cs * (size_t)(z - o.z0));
+    zpitch[z] = o.nzl;
+  }
+  for (int x = 0; x < nxh; ++x) {
+    const PeerView& o = v[xown[x]];
+    xdst[x] = (unsigned long long)((const char*)o.T2 + cs * ((size_t)(x - o.x0) * nz2 + c->z0s));
+    xpitch[x] = (long long)o.nxl * nz2;
+  }
+  std::vector<unsigned long long*> peers;
+  for (int i = 0; i < n; ++i)
+    if (i != c->rank) peers.push_back(v[i].cfl);
+  cudaSetDevice(c->dev);
+  if (c->scat_tab) cudaFree(c->scat_tab);
+  if (c->cfl_peers) cudaFree(c->cfl_peers);
+  c->scat_tab = nullptr;
+  c->cfl_peers = nullptr;
+  if (cudaMalloc(&c->scat_tab, sizeof(unsigned long long) * tab.size()) != cudaSuccess ||
+      cudaMalloc(&c->cfl_peers, sizeof(unsigned long long*) * std::max<size_t>(1, peers.size())) != cudaSuccess)
+    return fail(c, CFG_E_NOMEM, "scatter tables");
+  CK(cudaMemcpy(c->scat_tab, tab.data(), sizeof(unsigned long long) * tab.size(), cudaMemcpyHostToDevice));
+  if (!peers.empty())
+    CK(cudaMemcpy(c->cfl_peers, peers.data(), sizeof(unsigned long long*) * peers.size(), cudaMemcpyHostToDevice));
+  const unsigned long long* d = (const unsigned long long*)c->scat_tab;
+  c->scat.n = n;
+  c->scat.zdst = d;
+  c->scat.zpitch = reinterpret_cast<const long long*>(d + nz2);
+  c->scat.xdst = d + 2 * nz2;
+  c->scat.xpitch = reinterpret_cast<const long long*>(d + 2 * nz2 + nxh);
+  c->n_cfl_peers = n - 1;
+  return CFG_OK;
+}
+
 struct cfg_group {
   std::vector<cfg_ctx*> r;
   std::vector<cudaEvent_t> ev;
@@ -2063,49 +2130,11 @@ int cfg_group_create(const cfg_params* p, const cfg_grid* gr, int nranks, const 
         }
         cudaGetLastError();
       }
-    // scatter tables of each rank
-    const int nz2 = p->nz2, nxh = p->nx / 2 + 1;
-    std::vector<int> zown(nz2), xown(nxh);
-    for (int i = 0; i < n; ++i) {
-      for (int z = G->z_start[i]; z < G->z_start[i] + G->nz_proc[i]; ++z) zown[z] = i;
-      for (int x = G->x_start[i]; x < G->x_start[i] + G->nx_proc[i]; ++x) xown[x] = i;
-    }
+    std::vector<PeerView> views(n);
+    for (int i = 0; i < n; ++i) views[i] = view_of(G->r[i]);
     for (int s = 0; s < n; ++s) {
-      cfg_ctx* c = G->r[s];
-      const size_t cs = csize(c);
-      std::vector<unsigned long long> tab((size_t)2 * nz2 + 2 * nxh);
-      unsigned long long* zdst = tab.data();
-      long long* zpitch = reinterpret_cast<long long*>(zdst + nz2);
-      unsigned long long* xdst = zdst + 2 * nz2;
-      long long* xpitch = reinterpret_cast<long long*>(xdst + nxh);
-      for (int z = 0; z < nz2; ++z) {
-        const cfg_ctx* o = G->r[zown[z]];
-        zdst[z] = (unsigned long long)((const char*)o->T1 + cs * (size_t)(z - o->z0s));
-        zpitch[z] = o->gP.nz2;
-      }
-      for (int x = 0; x < nxh; ++x) {
-        const cfg_ctx* o = G->r[xown[x]];
-        xdst[x] = (unsigned long long)((const char*)o->T2 + cs * ((size_t)(x - o->g.kx0) * nz2 + c->z0s));
-        xpitch[x] = (long long)o->g.nxh * nz2;
-      }
-      cudaSetDevice(c->dev);
-      std::vector<unsigned long long*> peers;
-      for (int i = 0; i < n; ++i)
-        if (i != s) peers.push_back(G->r[i]->cflbits);
-      if (cudaMalloc(&c->scat_tab, sizeof(unsigned long long) * tab.size()) != cudaSuccess ||
-          cudaMalloc(&c->cfl_peers, sizeof(unsigned long long*) * peers.size()) != cudaSuccess) {
-        cfg_group_destroy(G);
-        return CFG_E_NOMEM;
-      }
-      cudaMemcpy(c->scat_tab, tab.data(), sizeof(unsigned long long) * tab.size(), cudaMemcpyHostToDevice);
-      cudaMemcpy(c->cfl_peers, peers.data(), sizeof(unsigned long long*) * peers.size(), cudaMemcpyHostToDevice);
-      const unsigned long long* d = (const unsigned long long*)c->scat_tab;
-      c->scat.n = n;
-      c->scat.zdst = d;
-      c->scat.zpitch = reinterpret_cast<const long long*>(d + nz2);
-      c->scat.xdst = d + 2 * nz2;
-      c->scat.xpitch = reinterpret_cast<const long long*>(d + 2 * nz2 + nxh);
-      c->n_cfl_peers = n - 1;
+      const int r = build_scatter(G->r[s], views);
+      if (r) { cfg_group_destroy(G); return r; }
     }
   }
   *out = G;
@@ -2158,3 +2187,109 @@ int cfg_group_synchronize(cfg_group* G) {
   }
   return CFG_OK;
 }
+
+// ---- one process per rank ---------------------------------------------------
+// The same decomposition with each rank in its own process (one per GPU, as
+// under mpirun): the ranks exchange CUDA IPC handles of their T1, T2 and CFL
+// buffers through the host (any all-gather: MPI, torch.distributed), map the
+// others' buffers, and step with a host barrier between the phases.
+
+struct cfg_rank_rec {
+  int magic, rank, nranks, x0, nxl, z0, nzl, elem;
+  cudaIpcMemHandle_t t1, t2, cfl;
+};
+static const int RANK_MAGIC = 0x43464752;
+
+size_t cfg_rank_record_size(void) { return sizeof(cfg_rank_rec); }
+
+int cfg_rank_create(const cfg_params* p, const cfg_grid* gr, int rank, int nranks, cfg_ctx** out) {
+  if (!p || !gr || !out || nranks < 1 || nranks > 64 || rank < 0 || rank >= nranks) return CFG_E_ARG;
+  *out = nullptr;
+  if (p->ctrlu != 0.0 || p->ctrlw != 0.0) {
+    fprintf(stderr, "cfg_rank_create: wall feedback (ctrlu, ctrlw) needs a single context\n");
+    return CFG_E_ARG;
+  }
+  std::vector<int> nxp(nranks), xs(nranks), nzp(nranks), zs(nranks);
+  cfg_partition(p->nx, p->nz, p->nz2, nranks, nxp.data(), xs.data(), nzp.data(), zs.data(), nullptr, nullptr);
+  for (int i = 0; i < nranks; ++i)
+    if (nxp[i] < 1 || nzp[i] < 8 || nzp[i] % 8 != 0) {
+      fprintf(stderr, "cfg_rank_create: rank %d gets %d kx columns and %d z2 rows (needs >= 1 and a multiple of 8)\n",
+              i, nxp[i], nzp[i]);
+      return CFG_E_ARG;
+    }
+  SlabPart sp{rank, nranks, xs[rank], nxp[rank], zs[rank], nzp[rank]};
+  int r = create_impl(p, gr, &sp, out);
+  if (r) return r;
+  if (nranks > 1 && !((*out)->split_x && (*out)->fast_z)) {
+    fprintf(stderr, "cfg_rank_create: transform lengths %d x %d have no register-FFT kernels\n", p->nx2, p->nz2);
+    cfg_destroy(*out);
+    *out = nullptr;
+    return CFG_E_ARG;
+  }
+  return CFG_OK;
+}
+
+int cfg_rank_export(cfg_ctx* c, void* record) {
+  if (!c || !record) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  cfg_rank_rec h{};
+  h.magic = RANK_MAGIC; h.rank = c->rank; h.nranks = c->nranks;
+  h.x0 = c->g.kx0; h.nxl = c->g.nxh; h.z0 = c->z0s; h.nzl = c->gP.nz2; h.elem = (int)csize(c);
+  CK(cudaIpcGetMemHandle(&h.t1, c->T1));
+  CK(cudaIpcGetMemHandle(&h.t2, c->T2));
+  CK(cudaIpcGetMemHandle(&h.cfl, c->cflbits));
+  memcpy(record, &h, sizeof(h));
+  return CFG_OK;
+}
+
+int cfg_rank_connect(cfg_ctx* c, const void* records) {
+  if (!c || !records) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  const int n = c->nranks;
+  std::vector<cfg_rank_rec> h(n);
+  memcpy(h.data(), records, sizeof(cfg_rank_rec) * n);
+  std::vector<PeerView> v(n);
+  for (int i = 0; i < n; ++i) {
+    if (h[i].magic != RANK_MAGIC || h[i].rank != i || h[i].nranks != n || h[i].elem != (int)csize(c))
+      return fail(c, CFG_E_ARG, "rank record %d does not belong to this run", i);
+    if (i == c->rank) {
+      v[i] = view_of(c);
+      continue;
+    }
+    void* m[3] = {nullptr, nullptr, nullptr};
+    const cudaIpcMemHandle_t* hh[3] = {&h[i].t1, &h[i].t2, &h[i].cfl};
+    for (int k = 0; k < 3; ++k) {
+      CK(cudaIpcOpenMemHandle(&m[k], *hh[k], cudaIpcMemLazyEnablePeerAccess));
+      c->ipc_open.push_back(m[k]);
+    }
+    v[i] = PeerView{m[0], m[1], (unsigned long long*)m[2], h[i].x0, h[i].nxl, h[i].z0, h[i].nzl};
+  }
+  return build_scatter(c, v);
+}
+
+int cfg_rank_timestep(cfg_ctx* c, int nsteps, cfg_barrier_fn barrier, void* user) {
+  if (!c || nsteps < 0 || (c->nranks > 1 && (!barrier || !c->scat.n))) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  int r;
+  for (int s = 0; s < nsteps; ++s) {
+    c->step = c->step < 0 ? 1 : c->step + 1;
+    if ((r = DISPATCH(c, boundary(c)))) return r;
+    for (int rk = 1; rk <= 3; ++rk)
+      for (int ph = 1; ph <= 3; ++ph) {
+        if ((r = DISPATCH(c, nl_phase(c, c->step, rk, false, ph)))) return r;
+        if (ph == 3) {
+          if ((r = DISPATCH(c, rhs(c, rk, 0)))) return r;
+        } else if (c->nranks > 1) {
+          // this rank's stores into the others' buffers are complete, then
+          // every rank's
+          CK(cudaStreamSynchronize(c->st));
+          if (barrier(user) != 0) return fail(c, CFG_E_ARG, "barrier callback failed");
+        }
+      }
+    prof_begin(c, "k_advance_time");
+    k_advance_time<<<1, 1, 0, c->st>>>(c->sc);
+    CKL();
+  }
+  return CFG_OK;
+}
+

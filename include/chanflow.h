@@ -25,6 +25,8 @@
 #ifndef CHANFLOW_H
 #define CHANFLOW_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -324,6 +326,25 @@ cfg_ctx *cfg_group_rank(cfg_group *grp, int rank);
 int cfg_group_timestep(cfg_group *grp, int nsteps);
 int cfg_group_synchronize(cfg_group *grp);
 void cfg_group_destroy(cfg_group *grp);
+
+/* The same decomposition with one process per rank (one per GPU, as the
+ * reference runs under mpirun; PFC/setup.f90:298-437 in each process).
+ * cfg_rank_create makes rank `rank`'s context (its slabs, on p->device);
+ * cfg_rank_export writes a record of cfg_rank_record_size() bytes (CUDA IPC
+ * handles of the rank's transpose targets and CFL maxima, its slabs); the
+ * caller all-gathers the nranks records in rank order (MPI_ALLGATHER,
+ * torch.distributed) and passes them to cfg_rank_connect, which maps the
+ * other ranks' buffers.  cfg_rank_timestep then advances this rank; between
+ * the phases of each substep it completes its own stores and calls
+ * barrier(user), which must return 0 once every rank has called it
+ * (MPI_BARRIER) -- the exchange of the MPI_ALLTOALLV transposes of
+ * PFC/transform.f90:345-409, 573-690.  Same limits as cfg_group_create. */
+typedef int (*cfg_barrier_fn)(void *user);
+size_t cfg_rank_record_size(void);
+int cfg_rank_create(const cfg_params *p, const cfg_grid *g, int rank, int nranks, cfg_ctx **out);
+int cfg_rank_export(cfg_ctx *c, void *record);
+int cfg_rank_connect(cfg_ctx *c, const void *records);
+int cfg_rank_timestep(cfg_ctx *c, int nsteps, cfg_barrier_fn barrier, void *user);
 
 /* cfg_xz_c2r_noalloc -- no counterpart in the reference.  The inverse x-z
  * transform of one plane (the semantics of cfg_xz_c2r /
