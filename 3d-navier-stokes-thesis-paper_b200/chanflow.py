@@ -160,6 +160,13 @@ SYMBOLS = {
     "cfg_group_timestep": (C.c_int, [_VP, C.c_int]),
     "cfg_group_synchronize": (C.c_int, [_VP]),
     "cfg_group_destroy": (None, [_VP]),
+    "cfg_autotune": (C.c_int, [_VP, C.c_int, _VP]),
+    "cfg_set_tiles": (C.c_int, [_VP, _VP]),
+    "cfg_ensemble_create": (C.c_int, [C.c_int, _VP, C.c_int, C.POINTER(_VP)]),
+    "cfg_ensemble_timestep": (C.c_int, [_VP, C.c_int]),
+    "cfg_ensemble_synchronize": (C.c_int, [_VP]),
+    "cfg_ensemble_stream": (_VP, [_VP]),
+    "cfg_ensemble_destroy": (None, [_VP]),
     "cfg_rank_record_size": (C.c_size_t, []),
     "cfg_rank_create": (C.c_int, [C.POINTER(CfgParams), C.POINTER(CfgGrid), C.c_int, C.c_int, C.POINTER(_VP)]),
     "cfg_rank_export": (C.c_int, [_VP, _VP]),
@@ -518,6 +525,17 @@ class ChannelFlow:
     def status(self):
         return self.L.cfg_status(self.h)
 
+    def autotune(self, trial_steps=3):
+        """Tune the kernels' tiles on this grid (cfg_autotune); the state is
+        restored.  Returns (rhs warps, flux rows, zinv planes, zfwd planes)."""
+        t = np.zeros(4, np.int32)
+        self._chk(self.L.cfg_autotune(self.h, trial_steps, _p(t)))
+        return tuple(int(v) for v in t)
+
+    def set_tiles(self, tiles):
+        t = np.ascontiguousarray(tiles, dtype=np.int32)
+        self._chk(self.L.cfg_set_tiles(self.h, _p(t)))
+
     def synchronize(self):
         self._chk(self.L.cfg_synchronize(self.h))
 
@@ -747,4 +765,47 @@ class Rank(ChannelFlow):
         if err:
             raise err[0]
         self._chk(r)
+
+
+class Ensemble:
+    """cfg_ensemble: independent ChannelFlow members on one GPU advanced
+    together, one CUDA graph launch per step after the first (configuration
+    C5: many grids, Reynolds numbers, seeds and forcings).  autotune tunes the
+    tiles once per distinct grid.  Call synchronize() before reading a
+    member."""
+
+    def __init__(self, members, autotune=True):
+        self.L = load_library()
+        self.members = list(members)
+        hs = (C.c_void_p * len(self.members))(*[m.h.value for m in self.members])
+        h = C.c_void_p()
+        r = self.L.cfg_ensemble_create(len(self.members), C.cast(hs, C.c_void_p), 1 if autotune else 0,
+                                       C.byref(h))
+        if r != 0:
+            msg = self.L.cfg_last_error(self.members[0].h)
+            raise ChanflowError(f"cfg_ensemble_create failed ({ERRORS.get(r, r)}): {msg.decode() if msg else ''}")
+        self.h = h
+
+    def timestep(self, nsteps=1):
+        r = self.L.cfg_ensemble_timestep(self.h, nsteps)
+        if r != 0:
+            raise ChanflowError(f"cfg_ensemble_timestep failed ({ERRORS.get(r, r)})")
+
+    def synchronize(self):
+        if self.L.cfg_ensemble_synchronize(self.h) != 0:
+            raise ChanflowError("cfg_ensemble_synchronize failed")
+
+    def stream_ptr(self):
+        return self.L.cfg_ensemble_stream(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.cfg_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 

@@ -195,6 +195,7 @@ struct cfg_ctx {
   bool fast_z = false, fast_x = false;
   bool use_rhs2 = true;
   int rhs2_lanes = 32;
+  int rhs2_warps = 3;   // warps (wavenumbers) per k_rhs2 block
   int fYB1 = 1, fYB3 = 1, fZR = 1;
   // optional per-launch CUDA-event timing on the context stream
   bool prof_on = false;
@@ -405,6 +406,7 @@ struct Impl {
     }
     c->use_rhs2 = rhs2_supported(g.ny1) && !getenv("CHANFLOW_RHS_V1");
     c->rhs2_lanes = (getenv("CHANFLOW_RHS2_LANES") && atoi(getenv("CHANFLOW_RHS2_LANES")) == 16) ? 16 : 32;
+    c->rhs2_warps = f32 ? 3 : 2;
     c->twx = make_twiddles<T>(g.nx2);
     c->twz = make_twiddles<T>(g.nz2);
     c->twxs = make_twiddles<T>(g.nx);
@@ -565,7 +567,7 @@ struct Impl {
       a.vel = c->vel; a.cru = c->cru; a.prs = c->prs;
       a.cbc_top = (const C*)c->cbc + 3 * (size_t)g.nw; a.cbc_bot = c->cbc;
       a.g = g; a.gd = c->gd; a.sc = c->sc; a.rkt = c->rkt; a.rk = rk; a.re = c->p.re;
-      a.wlist = c->wl_fast; a.nlist = c->n_fast; a.warps = sizeof(T) == 4 ? 3 : 2; a.lanes = c->rhs2_lanes;
+      a.wlist = c->wl_fast; a.nlist = c->n_fast; a.warps = c->rhs2_warps; a.lanes = c->rhs2_lanes;
       a.tbl = c->rhs2_tbl;
       a.st = c->st;
       prof_begin(c, "k_rhs");
@@ -1161,26 +1163,34 @@ int cfg_rhs_solve(cfg_ctx* c, int step, int rk_step) {
   return DISPATCH(c, rhs(c, rk_step, 0));
 }
 
+// one time step (PFC/main_mpi.f90:70-86), enqueued only: boundary, three
+// (nonlinear, rhs_solve) substeps, t_total += dt
+static int step_enqueue(cfg_ctx* c, bool lin) {
+  c->step = c->step < 0 ? 1 : c->step + 1;
+  int r;
+  if (!lin) {
+    r = DISPATCH(c, boundary(c));
+    if (r) return r;
+  }
+  for (int rk = 1; rk <= 3; ++rk) {
+    r = DISPATCH(c, nonlinear(c, c->step, rk, lin));
+    if (r) return r;
+    r = DISPATCH(c, rhs(c, rk, 0));
+    if (r) return r;
+  }
+  prof_begin(c, "k_advance_time");
+  k_advance_time<<<1, 1, 0, c->st>>>(c->sc);
+  CKL();
+  return CFG_OK;
+}
+
 static int timestep_impl(cfg_ctx* c, int nsteps, bool lin) {
   if (!c || nsteps < 0) return CFG_E_ARG;
   if (c->nranks > 1) return single_only(c, "cfg_timestep");
   cudaSetDevice(c->dev);
   for (int s = 0; s < nsteps; ++s) {
-    c->step = c->step < 0 ? 1 : c->step + 1;
-    int r;
-    if (!lin) {
-      r = DISPATCH(c, boundary(c));
-      if (r) return r;
-    }
-    for (int rk = 1; rk <= 3; ++rk) {
-      r = DISPATCH(c, nonlinear(c, c->step, rk, lin));
-      if (r) return r;
-      r = DISPATCH(c, rhs(c, rk, 0));
-      if (r) return r;
-    }
-    prof_begin(c, "k_advance_time");
-    k_advance_time<<<1, 1, 0, c->st>>>(c->sc);
-    CKL();
+    const int r = step_enqueue(c, lin);
+    if (r) return r;
   }
   return CFG_OK;
 }
@@ -2293,3 +2303,279 @@ int cfg_rank_timestep(cfg_ctx* c, int nsteps, cfg_barrier_fn barrier, void* user
   return CFG_OK;
 }
 
+
+// ---- launch-shape autotuner ------------------------------------------------
+// Tries the tile parameters of the step's kernels on this context's own
+// grid -- warps per k_rhs2 block, z rows per k_flux_r block, planes per
+// k_zinv_r / k_zfwd_r block -- one at a time (coordinate descent), timing a
+// few steps of the real state with CUDA events, and keeps the fastest.  The
+// state, the scalars, the wall values and the jet walk are restored after
+// every trial, so the run continues as if nothing had happened.  Every
+// choice gives the same results bit for bit (each wavenumber, row and plane
+// goes through the same arithmetic whatever the tile), only the time differs.
+
+struct TuneSnap {
+  std::vector<std::pair<void*, void*>> bufs;   // (live, copy)
+  std::vector<size_t> bytes;
+};
+
+static int snap_take(cfg_ctx* c, TuneSnap& s) {
+  const Geom& g = c->g;
+  const size_t cs = csize(c), nf = (size_t)g.nw * 3 * g.ny1;
+  std::vector<std::pair<void*, size_t>> live = {
+      {c->vel, cs * nf}, {c->cru, cs * nf}, {c->prs, cs * (size_t)g.nw * g.ny1}, {c->cbc, cs * 6 * (size_t)g.nw},
+      {c->sc, sizeof(DevScalars)}, {c->d_um_dy, sizeof(double) * g.ny}};
+  if (c->mvel64) live.push_back({c->mvel64, sizeof(double2) * 3 * g.ny1});
+  if (c->mcru64) live.push_back({c->mcru64, sizeof(double2) * 3 * g.ny1});
+  if (c->jst) live.push_back({c->jst, sizeof(JetState)});
+  for (auto& l : live) {
+    void* d = nullptr;
+    if (cudaMalloc(&d, l.second) != cudaSuccess) return fail(c, CFG_E_NOMEM, "autotune snapshot");
+    s.bufs.push_back({l.first, d});
+    s.bytes.push_back(l.second);
+    CK(cudaMemcpyAsync(d, l.first, l.second, cudaMemcpyDeviceToDevice, c->st));
+  }
+  return CFG_OK;
+}
+static int snap_restore(cfg_ctx* c, TuneSnap& s) {
+  for (size_t i = 0; i < s.bufs.size(); ++i)
+    CK(cudaMemcpyAsync(s.bufs[i].first, s.bufs[i].second, s.bytes[i], cudaMemcpyDeviceToDevice, c->st));
+  return CFG_OK;
+}
+static void snap_free(TuneSnap& s) {
+  for (auto& b : s.bufs) cudaFree(b.second);
+  s.bufs.clear();
+}
+
+int cfg_autotune(cfg_ctx* c, int trial_steps, int* choice) {
+  if (!c || trial_steps < 1) return CFG_E_ARG;
+  if (c->nranks > 1) return single_only(c, "cfg_autotune");
+  if (c->prof_on) return fail(c, CFG_E_STATE, "cfg_autotune: profiling is on");
+  cudaSetDevice(c->dev);
+  CK(cudaStreamSynchronize(c->st));
+  TuneSnap snap;
+  int r = snap_take(c, snap);
+  if (r) { snap_free(snap); return r; }
+  const int step0 = c->step;
+  const long long launches0 = c->launches;
+  const bool mean_ok = c->mean64_valid;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  // one trial: restore, one untimed step, trial_steps timed steps; a
+  // failing launch or a device error flag disqualifies the setting
+  auto trial = [&]() -> float {
+    if (snap_restore(c, snap)) return -1.f;
+    c->step = step0;
+    if (step_enqueue(c, false)) { cudaGetLastError(); return -1.f; }
+    cudaEventRecord(e0, c->st);
+    for (int i = 0; i < trial_steps; ++i)
+      if (step_enqueue(c, false)) { cudaGetLastError(); cudaStreamSynchronize(c->st); return -1.f; }
+    cudaEventRecord(e1, c->st);
+    if (cudaEventSynchronize(e1) != cudaSuccess) { cudaGetLastError(); return -1.f; }
+    DevScalars h;
+    cudaMemcpy(&h, c->sc, sizeof(h), cudaMemcpyDeviceToHost);
+    if (h.status != 0) return -1.f;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    return ms;
+  };
+  float best = trial();
+  if (best < 0.f) {
+    snap_restore(c, snap);
+    cudaStreamSynchronize(c->st);
+    snap_free(snap);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->step = step0;
+    c->launches = launches0;
+    return fail(c, CFG_E_STATE, "cfg_autotune: the current settings do not run");
+  }
+  const bool f32 = c->mixed;
+  auto tune = [&](int* knob, std::initializer_list<int> vals) {
+    const int keep = *knob;
+    int bestv = keep;
+    for (int v : vals) {
+      if (v == keep) continue;
+      *knob = v;
+      const float t = trial();
+      if (t >= 0.f && t < best) { best = t; bestv = v; }
+    }
+    *knob = bestv;
+  };
+  if (c->use_rhs2) {
+    if (f32) tune(&c->rhs2_warps, {2, 3, 4});
+    else tune(&c->rhs2_warps, {1, 2});
+  }
+  if (c->split_x) tune(&c->flux_zr, {2, 4});   // a row count that does not split fails its trial
+  if (c->fast_z) {
+    tune(&c->fYB1, {1, 2, 3, 4});
+    tune(&c->fYB3, {1, 2, 3, 4});
+  }
+  snap_restore(c, snap);
+  CK(cudaStreamSynchronize(c->st));
+  snap_free(snap);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->step = step0;
+  c->launches = launches0;
+  c->mean64_valid = mean_ok;
+  if (choice) {
+    choice[0] = c->rhs2_warps;
+    choice[1] = c->flux_zr;
+    choice[2] = c->fYB1;
+    choice[3] = c->fYB3;
+  }
+  return CFG_OK;
+}
+
+int cfg_set_tiles(cfg_ctx* c, const int* tiles) {
+  if (!c || !tiles) return CFG_E_ARG;
+  const int w = tiles[0], fz = tiles[1], y1 = tiles[2], y3 = tiles[3];
+  if (w < 1 || w > 4 || (fz != 2 && fz != 4) || y1 < 1 || y1 > 4 || y3 < 1 || y3 > 4 ||
+      (c->split_x && c->gP.nz2 % fz != 0))
+    return fail(c, CFG_E_ARG, "cfg_set_tiles: unsupported tiles");
+  c->rhs2_warps = w;
+  c->flux_zr = fz;
+  c->fYB1 = y1;
+  c->fYB3 = y3;
+  return CFG_OK;
+}
+
+// ---- ensembles: many independent contexts stepped by one graph ------------
+// Configuration C5: members of different grids, Reynolds numbers, seeds and
+// forcing on one GPU.  One time step of every member is captured once into a
+// CUDA graph (each member's work on its own branch, forked from and joined to
+// the ensemble stream), so a step of the whole ensemble is one graph launch.
+
+struct cfg_ensemble {
+  std::vector<cfg_ctx*> m;
+  int dev = 0;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev_fork = nullptr;
+  std::vector<cudaEvent_t> ev_done;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<long long> launches_per_step;
+};
+
+void cfg_ensemble_destroy(cfg_ensemble* e) {
+  if (!e) return;
+  cudaSetDevice(e->dev);
+  if (e->st) cudaStreamSynchronize(e->st);
+  if (e->exec) cudaGraphExecDestroy(e->exec);
+  if (e->graph) cudaGraphDestroy(e->graph);
+  for (cudaEvent_t v : e->ev_done) cudaEventDestroy(v);
+  if (e->ev_fork) cudaEventDestroy(e->ev_fork);
+  if (e->st) cudaStreamDestroy(e->st);
+  delete e;
+}
+
+int cfg_ensemble_create(int n, cfg_ctx* const* members, int autotune, cfg_ensemble** out) {
+  if (n < 1 || !members || !out) return CFG_E_ARG;
+  *out = nullptr;
+  for (int i = 0; i < n; ++i)
+    if (!members[i] || members[i]->nranks > 1 || members[i]->dev != members[0]->dev || members[i]->prof_on)
+      return CFG_E_ARG;
+  cfg_ensemble* e = new cfg_ensemble();
+  e->m.assign(members, members + n);
+  e->dev = members[0]->dev;
+  cudaSetDevice(e->dev);
+  e->ev_done.assign(n, nullptr);
+  bool ok = cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming) == cudaSuccess;
+  for (int i = 0; i < n && ok; ++i) ok = cudaEventCreateWithFlags(&e->ev_done[i], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) { cfg_ensemble_destroy(e); return CFG_E_CUDA; }
+  if (autotune) {
+    // one trial run per distinct grid and precision; the others take its tiles
+    for (int i = 0; i < n; ++i) {
+      cfg_ctx* c = e->m[i];
+      int first = -1;
+      for (int j = 0; j < i && first < 0; ++j) {
+        const cfg_ctx* o = e->m[j];
+        if (o->mixed == c->mixed && o->p.nx == c->p.nx && o->p.ny == c->p.ny && o->p.nz == c->p.nz &&
+            o->p.nx2 == c->p.nx2 && o->p.nz2 == c->p.nz2)
+          first = j;
+      }
+      if (first >= 0) {
+        const cfg_ctx* o = e->m[first];
+        const int t[4] = {o->rhs2_warps, o->flux_zr, o->fYB1, o->fYB3};
+        const int r = cfg_set_tiles(c, t);
+        if (r) { cfg_ensemble_destroy(e); return r; }
+      } else {
+        const int r = cfg_autotune(c, 3, nullptr);
+        if (r) { cfg_ensemble_destroy(e); return r; }
+      }
+    }
+  }
+  *out = e;
+  return CFG_OK;
+}
+
+// one step of every member on its own stream, forked from and joined to the
+// ensemble stream (eagerly, or under stream capture)
+static int ensemble_enqueue(cfg_ensemble* e) {
+  if (cudaEventRecord(e->ev_fork, e->st) != cudaSuccess) return CFG_E_CUDA;
+  for (size_t i = 0; i < e->m.size(); ++i) {
+    cfg_ctx* c = e->m[i];
+    if (cudaStreamWaitEvent(c->st, e->ev_fork, 0) != cudaSuccess) return fail(c, CFG_E_CUDA, "ensemble fork");
+    const int r = step_enqueue(c, false);
+    if (r) return r;
+    if (cudaEventRecord(e->ev_done[i], c->st) != cudaSuccess ||
+        cudaStreamWaitEvent(e->st, e->ev_done[i], 0) != cudaSuccess)
+      return fail(c, CFG_E_CUDA, "ensemble join");
+  }
+  return CFG_OK;
+}
+
+int cfg_ensemble_timestep(cfg_ensemble* e, int nsteps) {
+  if (!e || nsteps < 0) return CFG_E_ARG;
+  cudaSetDevice(e->dev);
+  int r;
+  if (!e->exec && nsteps > 0) {
+    // the first step runs eagerly (it also sets every kernel's shared-memory
+    // limit), the second is captured
+    if ((r = ensemble_enqueue(e))) return r;
+    --nsteps;
+    if (nsteps == 0) return CFG_OK;
+    std::vector<long long> before(e->m.size());
+    for (size_t i = 0; i < e->m.size(); ++i) before[i] = e->m[i]->launches;
+    if (cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return CFG_E_CUDA;
+    r = ensemble_enqueue(e);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(e->st, &g);
+    if (r || ce != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      return r ? r : CFG_E_CUDA;
+    }
+    e->graph = g;
+    if (cudaGraphInstantiate(&e->exec, e->graph, 0) != cudaSuccess) {
+      cudaGetLastError();
+      return CFG_E_CUDA;
+    }
+    e->launches_per_step.resize(e->m.size());
+    for (size_t i = 0; i < e->m.size(); ++i) {
+      e->launches_per_step[i] = e->m[i]->launches - before[i];
+      // the capture advanced the host step counters without running a step
+      e->m[i]->step -= 1;
+      e->m[i]->launches = before[i];
+    }
+  }
+  for (int s = 0; s < nsteps; ++s) {
+    if (cudaGraphLaunch(e->exec, e->st) != cudaSuccess) return CFG_E_CUDA;
+    for (size_t i = 0; i < e->m.size(); ++i) {
+      e->m[i]->step += 1;
+      e->m[i]->launches += e->launches_per_step[i];
+    }
+  }
+  return CFG_OK;
+}
+
+int cfg_ensemble_synchronize(cfg_ensemble* e) {
+  if (!e) return CFG_E_ARG;
+  cudaSetDevice(e->dev);
+  return cudaStreamSynchronize(e->st) == cudaSuccess ? CFG_OK : CFG_E_CUDA;
+}
+
+void* cfg_ensemble_stream(cfg_ensemble* e) { return e ? (void*)e->st : nullptr; }

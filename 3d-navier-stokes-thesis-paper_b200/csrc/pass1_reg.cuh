@@ -71,8 +71,12 @@ __global__ void __launch_bounds__(288, sizeof(T) == 4 ? 3 : 1) k_zinv_r(const cp
   const C* col = vel + (size_t)kx * NZ * 3 * NY1;
   {
     // gather: runs of nj planes at (kz, c), 16-byte pieces when aligned
+    // 16-byte pieces need 16-byte aligned sources (data1 run starts) and
+    // destinations (raw tile: the kz stride YB and the component stride RS)
     const int rb = nj * (int)sizeof(C);
-    const bool v16 = (rb % 16) == 0 && ((size_t)NY1 * sizeof(C)) % 16 == 0 && ((size_t)j0 * sizeof(C)) % 16 == 0;
+    const bool v16 = (rb % 16) == 0 && ((size_t)NY1 * sizeof(C)) % 16 == 0 && ((size_t)j0 * sizeof(C)) % 16 == 0 &&
+                     ((size_t)YB * sizeof(C)) % 16 == 0 && ((size_t)RS * sizeof(C)) % 16 == 0 &&
+                     ((size_t)NZ2 * sizeof(C)) % 16 == 0;
     const int psz = v16 ? 16 : 8, np = rb / psz;
     for (int idx = threadIdx.x; idx < 3 * NZ * np; idx += blockDim.x) {
       const int part = idx % np, r = idx / np, kz = r % NZ, c = r / NZ;

@@ -346,6 +346,34 @@ int cfg_rank_export(cfg_ctx *c, void *record);
 int cfg_rank_connect(cfg_ctx *c, const void *records);
 int cfg_rank_timestep(cfg_ctx *c, int nsteps, cfg_barrier_fn barrier, void *user);
 
+/* ---- launch shapes and ensembles (no counterpart in the reference) -----
+ *
+ * cfg_autotune: times trial_steps steps of this context's own state per
+ * candidate tile setting -- warps per rhs block, z rows per flux block,
+ * planes per z-transform block, one parameter at a time -- keeps the fastest
+ * and restores the state, scalars, wall values and jet walk afterwards.
+ * Results do not depend on the tiles (bit for bit).  choice (nullable, 4
+ * ints) receives the tiles; cfg_set_tiles sets them directly. */
+int cfg_autotune(cfg_ctx *c, int trial_steps, int *choice);
+int cfg_set_tiles(cfg_ctx *c, const int *tiles);
+
+/* An ensemble of independent contexts on one GPU (different grids,
+ * Reynolds numbers, seeds, forcing): members of one run of the reference
+ * each, advanced together.  cfg_ensemble_timestep runs the first step
+ * eagerly and captures one step of every member into a CUDA graph (each
+ * member on its own branch); every further step is one graph launch on the
+ * ensemble's stream.  autotune != 0 tunes the tiles once per distinct grid.
+ * The members stay owned by the caller and must outlive the ensemble; call
+ * cfg_ensemble_synchronize before reading or changing a member, and do not
+ * change a member's parameters (jet, baseflow, tiles) once the ensemble has
+ * stepped (the graph holds them). */
+typedef struct cfg_ensemble cfg_ensemble;
+int cfg_ensemble_create(int nmembers, cfg_ctx *const *members, int autotune, cfg_ensemble **out);
+int cfg_ensemble_timestep(cfg_ensemble *e, int nsteps);
+int cfg_ensemble_synchronize(cfg_ensemble *e);
+void *cfg_ensemble_stream(cfg_ensemble *e);
+void cfg_ensemble_destroy(cfg_ensemble *e);
+
 /* cfg_xz_c2r_noalloc -- no counterpart in the reference.  The inverse x-z
  * transform of one plane (the semantics of cfg_xz_c2r /
  * xz_fft_complex_to_real) for callers that cannot allocate device memory:
