@@ -377,8 +377,9 @@ struct Impl {
     if (c->fast_z) {
       const size_t zb = f32 ? 52 * 1024 : 108 * 1024;
       // z inverse: three blocks per SM with the raw tile and the exchange
+      // (FP32); one plane per block in FP64 (measured best at 256x193x256)
       c->fYB1 = 1;
-      for (int yb = 4; yb >= 1; --yb)
+      for (int yb = f32 ? 4 : 1; yb >= 1; --yb)
         if (p1_fast_smem(0, g.nz2, f32, yb, g.nxh, g.nz) <= 74 * 1024) { c->fYB1 = yb; break; }
       c->fYB3 = 1;
       for (int yb = 4; yb >= 1; --yb)
@@ -392,7 +393,8 @@ struct Impl {
     }
     if (getenv("CHANFLOW_GENERIC_FFT")) c->fast_x = c->fast_z = false;
     // split x stage: physical planes written once, fluxes read three of them
-    c->flux_zr = getenv("CHANFLOW_FLUX_ZR") ? atoi(getenv("CHANFLOW_FLUX_ZR")) : 4;
+    // z rows per flux block: 4 (FP32) or 2 (FP64, half the shared memory)
+    c->flux_zr = getenv("CHANFLOW_FLUX_ZR") ? atoi(getenv("CHANFLOW_FLUX_ZR")) : (f32 ? 4 : 2);
     if (c->flux_zr != 2) c->flux_zr = 4;
     // (gP: the x stage's geometry, all kx and this rank's z2 rows)
     const Geom& gp = c->gP;

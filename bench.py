@@ -400,6 +400,9 @@ def run_ours(args):
         if prec_name == "fp64" and args.no_fp64:
             continue
         flow = make_flow(cf, nx, ny, nz, prec, dev)
+        # launch tiles tuned on this grid (outside the timed region; the
+        # state is restored, results do not depend on the tiles)
+        tiles = flow.autotune(3)
         clocks = Clocks(dev) if prec_name == "mixed" else None
         flow.timestep(W)
         flow.synchronize()
@@ -416,7 +419,7 @@ def run_ours(args):
         # around every launch (not part of the timed number)
         kp = max(1, min(K, 10))
         _, _, prof = timed_steps(torch, flow, kp, profile=True)
-        results[prec_name] = {"ms_total": ms_max, "launches": sum_over_ranks(nlaunch), "prof": prof,
+        results[prec_name] = {"ms_total": ms_max, "launches": sum_over_ranks(nlaunch), "prof": prof, "tiles": tiles,
                               "prof_steps": kp, "clocks": cl, "status": st, "div": div, "q": q}
         if prec_name == "mixed":
             # end to end through the public API with host buffers: every step
@@ -512,7 +515,8 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 (f64 mean mode and |k|<4 solves)", "data": "synthetic (seeded initial field)",
-            "config": workload_config(nx, ny, nz, "mixed"),
+            "config": dict(workload_config(nx, ny, nz, "mixed"),
+                           tiles={k: list(v["tiles"]) for k, v in results.items() if "tiles" in v}),
             "roofline": best,
             "roofline_step": {"bound": "hbm", "achieved": step_bytes / (ms_step / 1e3) / 1e9, "peak": hbm,
                               "unit": "GB/s", "frac": step_bytes / (ms_step / 1e3) / 1e9 / hbm,
