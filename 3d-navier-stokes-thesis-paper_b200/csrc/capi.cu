@@ -2256,6 +2256,7 @@ int cfg_rank_export(cfg_ctx* c, void* record) {
 
 int cfg_rank_connect(cfg_ctx* c, const void* records) {
   if (!c || !records) return CFG_E_ARG;
+  if (c->scat.n != 0 || !c->ipc_open.empty()) return fail(c, CFG_E_STATE, "cfg_rank_connect: already connected");
   cudaSetDevice(c->dev);
   const int n = c->nranks;
   std::vector<cfg_rank_rec> h(n);

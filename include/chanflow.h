@@ -334,7 +334,8 @@ void cfg_group_destroy(cfg_group *grp);
  * handles of the rank's transpose targets and CFL maxima, its slabs); the
  * caller all-gathers the nranks records in rank order (MPI_ALLGATHER,
  * torch.distributed) and passes them to cfg_rank_connect, which maps the
- * other ranks' buffers.  cfg_rank_timestep then advances this rank; between
+ * other ranks' buffers (once per context; CFG_E_STATE after that).
+ * cfg_rank_timestep then advances this rank; between
  * the phases of each substep it completes its own stores and calls
  * barrier(user), which must return 0 once every rank has called it
  * (MPI_BARRIER) -- the exchange of the MPI_ALLTOALLV transposes of
