@@ -27,6 +27,14 @@ runs configuration C5 on one GPU: M members with grids from {48x49x48,
 (amplitude 1e-2), the Gaussian wall jet on odd members, mixed precision,
 tiles autotuned per grid, one CUDA graph launch per step; the same members
 stepped one call per member per step are timed beside it.
+
+  python bench.py --arnoldi [--arnoldi-maxiter R]
+
+runs configuration C3: the Arnoldi stability solver about laminar Poiseuille
+flow at Re 2900 on 64x65x64, T = 1 (100 linearized steps of dt 0.01 per
+matvec), Krylov dimension 60, 10 leading eigenvalues, a seeded FP64 start
+vector; FP64 and mixed matvecs through the host ARPACK driver, with their
+matvec counts, times and the agreement of the leading eigenvalues.
 """
 import argparse
 import json
@@ -383,6 +391,55 @@ def run_ensemble(args):
     return 0
 
 
+def run_arnoldi(args):
+    import __graft_entry__
+    cf = __graft_entry__.load_package()
+    from chanflow_b200.chanflow import arnoldi_eigs
+    nx, ny, nz, tend = 64, 65, 64, 100
+    grid = cf.Grid(nx, ny, nz, lx=4 * np.pi, lz=2 * np.pi, stretch=STRETCH)
+    n = nx * nz * (ny + 1) * 3
+    v0 = np.random.default_rng(3).standard_normal(n)
+    out = {}
+    for name, prec, tol in (("fp64", cf.FP64, 1e-8), ("mixed", cf.MIXED, 1e-6)):
+        f = cf.ChannelFlow(grid, re=2900.0, dt=0.01, fix_mass=0, precision=prec)
+        base = np.zeros((ny + 1, 3), order="F")
+        base[:, 0] = 1 - grid.yh ** 2
+        f.set_baseflow(base)
+        calls = [0]
+        mv = f.arnoldi_matvec
+
+        def counted(x, t, mv=mv):
+            calls[0] += 1
+            return mv(x, t)
+
+        f.arnoldi_matvec = counted
+        t0 = time.perf_counter()
+        try:
+            mu, lam, _ = arnoldi_eigs(f, tend, nev=10, ncv=60, tol=tol, v0=v0, maxiter=args.arnoldi_maxiter)
+            ok = True
+        except Exception as e:  # no convergence within maxiter: report what converged
+            ok = False
+            out[name + "_error"] = type(e).__name__
+            mu = np.asarray(getattr(e, "eigenvalues", np.array([])))
+            mu = mu[np.argsort(-np.abs(mu))] if mu.size else mu
+            T = tend * 0.01
+            lam = (np.log(np.abs(mu) + np.finfo(np.float64).eps) + 1j * np.arctan2(mu.imag, mu.real)) / T
+        out[name] = {"converged": ok, "matvecs": calls[0], "s": time.perf_counter() - t0,
+                     "mu": [[float(z.real), float(z.imag)] for z in mu],
+                     "lambda": [[float(z.real), float(z.imag)] for z in lam]}
+        f.close()
+    if out["fp64"]["mu"] and out["mixed"]["mu"]:
+        a = np.array([complex(*z) for z in out["fp64"]["mu"]])
+        b = np.array([complex(*z) for z in out["mixed"]["mu"]])
+        out["leading_rel_diff"] = float(abs(b[0] - a[0]) / abs(a[0]))
+        out["max_rel_diff_nearest"] = float(max(np.abs(b - m).min() / abs(m) for m in a))
+    line = {"metric": "Arnoldi eigenvalues (C3)", "config": {"workload": "linearized channel about Poiseuille, "
+            "Re 2900, 64x65x64, T = 1 (100 steps of dt 0.01), Krylov 60, nev 10, seeded start vector"},
+            "n_gpus": 1, "data": "synthetic (seeded)", "result": out}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_ours(args):
     import torch
     import __graft_entry__
@@ -554,6 +611,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--slab", type=int, default=0, help="one field in P slab ranks (one process)")
     ap.add_argument("--ensemble", type=int, default=0, help="configuration C5 with M members (one GPU)")
+    ap.add_argument("--arnoldi", action="store_true", help="configuration C3 (Arnoldi eigenvalues)")
+    ap.add_argument("--arnoldi-maxiter", type=int, default=60)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -563,6 +622,8 @@ def main():
         return run_slab(args)
     if args.ensemble > 0:
         return run_ensemble(args)
+    if args.arnoldi:
+        return run_arnoldi(args)
     return run_ours(args)
 
 
