@@ -407,7 +407,9 @@ struct Impl {
       c->split_x = false;
     }
     c->use_rhs2 = rhs2_supported(g.ny1) && !getenv("CHANFLOW_RHS_V1");
-    c->rhs2_lanes = (getenv("CHANFLOW_RHS2_LANES") && atoi(getenv("CHANFLOW_RHS2_LANES")) == 16) ? 16 : 32;
+    // 16 lanes per wavenumber exists for FP32 only (the FP64 kernel and its
+    // coefficient table stay at 32)
+    c->rhs2_lanes = (f32 && getenv("CHANFLOW_RHS2_LANES") && atoi(getenv("CHANFLOW_RHS2_LANES")) == 16) ? 16 : 32;
     c->rhs2_warps = f32 ? 3 : 2;
     c->twx = make_twiddles<T>(g.nx2);
     c->twz = make_twiddles<T>(g.nz2);
