@@ -5,6 +5,9 @@ makegrid_ny200.json: y(200), yh(201) written by output_grids
 (PFC/setup.f90:1331-1359) for ny=200 with STRETCH=2.75, as printed in
 PFC/makegrid.m (format f16.8).
 
+flow_ref.dat: the reference's own run-parameter file
+(ParallelFortran-Code/flow.dat), copied as the flow.dat reader's fixture.
+
 partition_nproc24.json: the partition table distribute_data
 (PFC/setup.f90:298-437) printed for Nx=128, Nz=64 (Nz2=96) on 24 ranks in
 PFC/diagnostics.txt (the leftover line and the per-rank nx_proc, x_start,
@@ -49,6 +52,11 @@ def main():
     with open(os.path.join(HERE, "partition_nproc24.json"), "w") as f:
         json.dump(part, f)
     print("wrote partition_nproc24.json", len(rows))
+
+    src = open(os.path.join(REF, "ParallelFortran-Code", "flow.dat")).read()
+    with open(os.path.join(HERE, "flow_ref.dat"), "w") as f:
+        f.write(src)
+    print("wrote flow_ref.dat", len(src.splitlines()), "lines")
 
 
 if __name__ == "__main__":

@@ -89,10 +89,10 @@ def test_flow_dat_reader_rejects_truncated(cf, tmp_path):
         cf.read_flow_dat(str(p))
 
 
-@pytest.mark.skipif(not os.path.exists("/root/reference/ParallelFortran-Code/flow.dat"),
-                    reason="reference not mounted")
 def test_flow_dat_reader_on_reference_file(cf):
-    run = cf.read_flow_dat("/root/reference/ParallelFortran-Code/flow.dat")
+    """The reference's own flow.dat (tests/golden/flow_ref.dat, copied from
+    ParallelFortran-Code/flow.dat by tests/golden/make_fixtures.py)."""
+    run = cf.read_flow_dat(os.path.join(ROOT, "tests", "golden", "flow_ref.dat"))
     assert (run.nx, run.ny, run.nz, run.nx2, run.nz2) == (128, 200, 64, 192, 96)
     assert run.re == 7500.0 and run.which_test == 9 and run.l2_step == 20
     assert abs(run.lx - 6 * np.pi) < 1e-14 and abs(run.lz - 2 * np.pi) < 1e-14
