@@ -5,7 +5,7 @@
  * (PFC = ParallelFortran-Code/).  The reference has no FFI layer of its own:
  * its boundary is a set of Fortran module procedures that talk through module
  * globals.  Each entry point below replaces one of them; a Fortran caller
- * binds them with ISO_C_BINDING (see INTEGRATION.md) and keeps its module
+ * binds them with ISO_C_BINDING and keeps its module
  * interfaces, flow.dat parameters and read_write file layouts unchanged.
  *
  * Conventions
