@@ -172,6 +172,7 @@ SYMBOLS = {
     "cfg_rank_export": (C.c_int, [_VP, _VP]),
     "cfg_rank_connect": (C.c_int, [_VP, _VP]),
     "cfg_rank_timestep": (C.c_int, [_VP, C.c_int, C.c_void_p, _VP]),
+    "cfg_rank_timestep_ordered": (C.c_int, [_VP, C.c_int, C.c_void_p, _VP]),
     "cfh_run_defaults": (None, [C.POINTER(CfhRun)]),
     "cfh_read_flow_dat": (C.c_int, [C.c_char_p, C.POINTER(CfhRun), C.c_char_p, C.c_int]),
     "cfh_grid_alloc": (C.POINTER(CfhGrid), [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
@@ -740,16 +741,36 @@ class Rank(ChannelFlow):
         self._chk(self.L.cfg_rank_export(self.h, b))
         return b.raw
 
+    def nccl_barrier(self):
+        """A stream-ordered barrier for timestep(ordered=True): an all-reduce
+        of one word on this rank's stream (torch.distributed with NCCL, one
+        GPU per rank)."""
+        import torch
+        import torch.distributed as dist
+        dev = torch.device("cuda", self.params.device)
+        word = torch.zeros(1, device=dev)
+        stream = torch.cuda.ExternalStream(self.stream_ptr(), device=dev)
+
+        def barrier():
+            with torch.cuda.stream(stream):
+                dist.all_reduce(word)
+
+        return barrier
+
     def connect(self, records):
         blob = b"".join(records)
         assert len(blob) == self.nranks * self.L.cfg_rank_record_size()
         buf = C.create_string_buffer(blob, len(blob))
         self._chk(self.L.cfg_rank_connect(self.h, buf))
 
-    def timestep(self, nsteps=1, barrier=None):
+    def timestep(self, nsteps=1, barrier=None, ordered=False):
+        """ordered=False: `barrier` is a host barrier (the rank's stream is
+        synchronised before it).  ordered=True: `barrier` must enqueue a
+        stream-ordered barrier on stream_ptr() (nccl_barrier() does, with an
+        NCCL all-reduce of one word), and the host never waits."""
         if barrier is None:
             import torch.distributed as dist
-            barrier = dist.barrier
+            barrier = self.nccl_barrier() if ordered else dist.barrier
         err = []
 
         def cb(_user):
@@ -761,7 +782,8 @@ class Rank(ChannelFlow):
                 return -1
 
         fn = _BARRIER(cb)
-        r = self.L.cfg_rank_timestep(self.h, nsteps, C.cast(fn, C.c_void_p), None)
+        step = self.L.cfg_rank_timestep_ordered if ordered else self.L.cfg_rank_timestep
+        r = step(self.h, nsteps, C.cast(fn, C.c_void_p), None)
         if err:
             raise err[0]
         self._chk(r)

@@ -2282,7 +2282,7 @@ int cfg_rank_connect(cfg_ctx* c, const void* records) {
   return build_scatter(c, v);
 }
 
-int cfg_rank_timestep(cfg_ctx* c, int nsteps, cfg_barrier_fn barrier, void* user) {
+static int rank_timestep(cfg_ctx* c, int nsteps, cfg_barrier_fn barrier, void* user, bool host_sync) {
   if (!c || nsteps < 0 || (c->nranks > 1 && (!barrier || !c->scat.n))) return CFG_E_ARG;
   cudaSetDevice(c->dev);
   int r;
@@ -2295,9 +2295,10 @@ int cfg_rank_timestep(cfg_ctx* c, int nsteps, cfg_barrier_fn barrier, void* user
         if (ph == 3) {
           if ((r = DISPATCH(c, rhs(c, rk, 0)))) return r;
         } else if (c->nranks > 1) {
-          // this rank's stores into the others' buffers are complete, then
-          // every rank's
-          CK(cudaStreamSynchronize(c->st));
+          // host barrier: this rank's stores into the others' buffers are
+          // complete, then every rank's; stream-ordered barrier: the callback
+          // enqueues it on this context's stream
+          if (host_sync) CK(cudaStreamSynchronize(c->st));
           if (barrier(user) != 0) return fail(c, CFG_E_ARG, "barrier callback failed");
         }
       }
@@ -2584,3 +2585,12 @@ int cfg_ensemble_synchronize(cfg_ensemble* e) {
 }
 
 void* cfg_ensemble_stream(cfg_ensemble* e) { return e ? (void*)e->st : nullptr; }
+
+int cfg_rank_timestep(cfg_ctx* c, int nsteps, cfg_barrier_fn barrier, void* user) {
+  return rank_timestep(c, nsteps, barrier, user, true);
+}
+
+int cfg_rank_timestep_ordered(cfg_ctx* c, int nsteps, cfg_barrier_fn barrier, void* user) {
+  return rank_timestep(c, nsteps, barrier, user, false);
+}
+

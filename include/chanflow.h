@@ -346,6 +346,11 @@ int cfg_rank_create(const cfg_params *p, const cfg_grid *g, int rank, int nranks
 int cfg_rank_export(cfg_ctx *c, void *record);
 int cfg_rank_connect(cfg_ctx *c, const void *records);
 int cfg_rank_timestep(cfg_ctx *c, int nsteps, cfg_barrier_fn barrier, void *user);
+/* The same without the host synchronisation: barrier(user) must enqueue a
+ * barrier on this context's stream (cfg_stream) that completes only after
+ * every rank's stream has reached it -- e.g. an NCCL all-reduce of one word
+ * on that stream -- so the host never waits between the phases. */
+int cfg_rank_timestep_ordered(cfg_ctx *c, int nsteps, cfg_barrier_fn barrier, void *user);
 
 /* ---- launch shapes and ensembles (no counterpart in the reference) -----
  *

@@ -21,7 +21,7 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _worker(rank, nranks, port, prec, dt_flag, inp, outp):
+def _worker(rank, nranks, port, prec, dt_flag, inp, outp, ordered):
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
@@ -37,7 +37,16 @@ def _worker(rank, nranks, port, prec, dt_flag, inp, outp):
     sl = me.slab()
     me.upload_state(z["d1"][:, sl], z["d2"][..., sl], z["d4"][..., sl])
     me.set_scalars(float(z["t"]), float(z["dt"]), float(z["pg"]), z["dud"])
-    me.timestep(4, barrier=dist.barrier)
+    if ordered:
+        # the stream-ordered entry point; NCCL cannot put two ranks on one
+        # GPU, so the barrier here waits for this rank's stream on the host,
+        # then meets the others (a valid, stronger stream-ordered barrier)
+        def barrier():
+            me.synchronize()
+            dist.barrier()
+        me.timestep(4, barrier=barrier, ordered=True)
+    else:
+        me.timestep(4, barrier=dist.barrier)
     d1, d2, d4 = me.download_state()
     sc = me.scalars()
     np.savez(outp % rank, d1=d1, d2=d2, d4=d4, dt=sc["dt"], pg=sc["p_grad"], dud=sc["d_um_dy"],
@@ -47,8 +56,8 @@ def _worker(rank, nranks, port, prec, dt_flag, inp, outp):
     dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("prec,dt_flag", [(0, 1), (1, 0)])
-def test_two_processes_match_single_context(cf, tmp_path, prec, dt_flag):
+@pytest.mark.parametrize("prec,dt_flag,ordered", [(0, 1, False), (1, 0, False), (1, 1, True)])
+def test_two_processes_match_single_context(cf, tmp_path, prec, dt_flag, ordered):
     import multiprocessing as mp
     grid = cf.Grid(32, 33, 32, stretch=1.5)
     d1 = cf.initial_field(grid, 10, seed=11, ampl=5e-2)
@@ -68,7 +77,8 @@ def test_two_processes_match_single_context(cf, tmp_path, prec, dt_flag):
     outp = str(tmp_path / "out%d.npz")
     ctx = mp.get_context("spawn")
     port = _free_port()
-    ps = [ctx.Process(target=_worker, args=(r, nranks, port, prec, dt_flag, inp, outp)) for r in range(nranks)]
+    ps = [ctx.Process(target=_worker, args=(r, nranks, port, prec, dt_flag, inp, outp, ordered))
+          for r in range(nranks)]
     for p in ps:
         p.start()
     for p in ps:
