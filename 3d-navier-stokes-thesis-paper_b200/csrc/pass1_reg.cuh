@@ -625,7 +625,7 @@ __global__ void __launch_bounds__(256) k_xinv_r(const cplx_t<T>* __restrict__ T1
 // transform and the Hermitian unpacking into T2 -- the same arithmetic and
 // output as k_xflux_r (PFC/pass1.f90:134-226, PFC/transform.f90:287-315).
 template <typename T, int NX2, int ZR, int NT, bool LIN>
-__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT == 256 ? 1 : 2)) k_flux_r(const T* __restrict__ P, cplx_t<T>* __restrict__ T2, Geom g,
+__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT == 256 ? 1 : 3)) k_flux_r(const T* __restrict__ P, cplx_t<T>* __restrict__ T2, Geom g,
                                                const cplx_t<T>* __restrict__ twx, GridDev gd,
                                                const T* __restrict__ fringe, int has_fringe,
                                                unsigned long long* __restrict__ cflbits, int do_cfl, Scatter sc) {
