@@ -1,5 +1,6 @@
 """Ensembles (configuration C5) on one GPU: members of different grids,
-Reynolds numbers, noise seeds and jet forcing, tuned once per grid and
+Reynolds numbers, noise seeds, jet forcing and precisions, tuned once per
+grid and
 advanced by one CUDA graph launch per step, must reproduce each member run
 alone with the default tiles bit for bit (the tiles change the schedule,
 never the arithmetic)."""
@@ -8,17 +9,18 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-MEMBERS = [  # (nx, ny, nz, Re, seed, jet)
-    (48, 49, 48, 2000.0, 1001, True),
-    (48, 49, 48, 2600.0, 1002, False),
-    (64, 65, 64, 2300.0, 1003, True),
-    (96, 97, 96, 2900.0, 1004, False),
+MEMBERS = [  # (nx, ny, nz, Re, seed, jet, precision: 1 mixed, 0 FP64)
+    (48, 49, 48, 2000.0, 1001, True, 1),
+    (48, 49, 48, 2600.0, 1002, False, 1),
+    (64, 65, 64, 2300.0, 1003, True, 1),
+    (96, 97, 96, 2900.0, 1004, False, 1),
+    (48, 49, 48, 2400.0, 1005, True, 0),
 ]
 
 
-def member(cf, nx, ny, nz, re, seed, jet):
+def member(cf, nx, ny, nz, re, seed, jet, prec=1):
     grid = cf.Grid(nx, ny, nz, stretch=1.5)
-    f = cf.ChannelFlow(grid, re=re, dt=0.0025, precision=cf.MIXED)
+    f = cf.ChannelFlow(grid, re=re, dt=0.0025, precision=prec)
     f.define_initial_field(10, seed=seed, ampl=1e-2)
     if jet:
         j = cf.CfgJet()
@@ -55,8 +57,8 @@ def test_ensemble_graph_matches_members_alone(cf):
 
 
 def test_autotune_restores_state(cf):
-    f = member(cf, 64, 65, 64, 2300.0, 7, True)
-    g = member(cf, 64, 65, 64, 2300.0, 7, True)
+    f = member(cf, 64, 65, 64, 2300.0, 7, True, 1)
+    g = member(cf, 64, 65, 64, 2300.0, 7, True, 1)
     tiles = f.autotune(2)
     assert len(tiles) == 4
     f.timestep(3)
