@@ -1,9 +1,8 @@
 """Ensembles (configuration C5) on one GPU: members of different grids,
 Reynolds numbers, noise seeds, jet forcing and precisions, tuned once per
-grid and
-advanced by one CUDA graph launch per step, must reproduce each member run
-alone with the default tiles bit for bit (the tiles change the schedule,
-never the arithmetic)."""
+grid and advanced by one CUDA graph launch per step, must reproduce each
+member run alone with the default tiles bit for bit (the tiles change the
+schedule, never the arithmetic)."""
 import numpy as np
 import pytest
 
