@@ -320,6 +320,21 @@ __global__ void k_cfl_merge(unsigned long long* __restrict__ own, unsigned long 
   }
 }
 
+// Lets a kernel take as much dynamic shared memory as the device allows.
+// The limit is an attribute of the kernel on its device, shared by every
+// context there, so contexts only ever raise it (to the device maximum) and
+// never lower it under another context's launches.
+template <typename K>
+static cudaError_t allow_smem(K kernel) {
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaError_t e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e != cudaSuccess) return e;
+  cudaFuncAttributes fa;
+  if ((e = cudaFuncGetAttributes(&fa, kernel)) != cudaSuccess) return e;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+}
+
 template <typename T>
 struct Impl {
   using C = cplx_t<T>;
@@ -346,25 +361,23 @@ struct Impl {
     if (c->M > 8) return fail(c, CFG_E_ARG, "ny+1 = %d exceeds 256 rows", g.ny1);
     if (c->sm_zinv > 200 * 1024 || c->sm_zfwd > 200 * 1024 || c->sm_xflux > 200 * 1024)
       return fail(c, CFG_E_ARG, "transform lengths too large for shared memory");
-    CK(cudaFuncSetAttribute(k_zinv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_zinv));
-    CK(cudaFuncSetAttribute(k_zfwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_zfwd));
-    CK(cudaFuncSetAttribute(k_xflux<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_xflux));
-    CK(cudaFuncSetAttribute(k_xflux<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_xflux));
-    const int maxn = std::max(std::max(g.nx2, g.nz2), std::max(g.nx, g.nz));
-    const int smp = (int)(cs * (3 * maxn + 3 * maxn * 2 + 64));
-    CK(cudaFuncSetAttribute(k_pz_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smp));
-    CK(cudaFuncSetAttribute(k_pz_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smp));
-    CK(cudaFuncSetAttribute(k_px_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smp));
-    CK(cudaFuncSetAttribute(k_px_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smp));
-    CK(cudaFuncSetAttribute(k_l2_rows<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smp));
+    CK(allow_smem(k_zinv<T>));
+    CK(allow_smem(k_zfwd<T>));
+    CK(allow_smem(k_xflux<T, false>));
+    CK(allow_smem(k_xflux<T, true>));
+    CK(allow_smem(k_pz_inv<T>));
+    CK(allow_smem(k_pz_fwd<T>));
+    CK(allow_smem(k_px_inv<T>));
+    CK(allow_smem(k_px_fwd<T>));
+    CK(allow_smem(k_l2_rows<T>));
     c->sm_rhs = 0;
     switch (c->M) {
 #define RHS_ATTR(MM)                                                                              \
   case MM:                                                                                        \
     c->sm_rhs = 4 * 5 * ColIdx<MM>::SIZE * cs;                                                   \
     c->sm_rhs64 = 4 * 5 * ColIdx<MM>::SIZE * sizeof(double2);                                    \
-    CK(cudaFuncSetAttribute(k_rhs<T, T, MM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_rhs)); \
-    CK(cudaFuncSetAttribute(k_rhs<double, T, MM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_rhs64)); \
+    CK(allow_smem(k_rhs<T, T, MM>));                                                              \
+    CK(allow_smem(k_rhs<double, T, MM>));                                                         \
     break;
       RHS_ATTR(2) RHS_ATTR(3) RHS_ATTR(4) RHS_ATTR(5) RHS_ATTR(6) RHS_ATTR(7) RHS_ATTR(8)
 #undef RHS_ATTR

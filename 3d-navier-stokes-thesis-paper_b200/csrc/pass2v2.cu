@@ -11,7 +11,13 @@ namespace cfd {
 template <typename T, int M, int G>
 static int launch_m(const Rhs2Launch& a) {
   const size_t sm = rhs2_smem<T, M, G>(a.warps, a.g.ny1);
-  static size_t cur = 48 * 1024;
+  // the limit raised so far on each device (the attribute is per device)
+  static size_t cur_dev[64];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return -2;
+  size_t& cur = cur_dev[dev];
+  if (cur == 0) cur = 48 * 1024;
   if (sm > cur) {
     if (cudaFuncSetAttribute(k_rhs2<T, T, M, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) {
       cudaGetLastError();
