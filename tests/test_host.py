@@ -164,3 +164,18 @@ def test_group_rejects_partition_without_whole_tiles(cf):
     grid = cf.Grid(32, 33, 32, stretch=1.5)
     with pytest.raises(cf.ChanflowError):
         cf.Group(grid, 4)
+
+
+def test_headers_compile_as_c99(tmp_path):
+    """The C ABI headers are plain C (what a Fortran ISO_C_BINDING or any
+    other FFI binds against): they compile as C99 with -pedantic."""
+    import shutil
+    import subprocess
+    if not shutil.which("gcc"):
+        pytest.skip("no C compiler")
+    src = tmp_path / "h.c"
+    src.write_text('#include "chanflow.h"\n#include "chanflow_host.h"\n'
+                   "int main(void) { return (int)cfg_rank_record_size(); }\n")
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-fsyntax-only",
+                        "-I" + os.path.join(ROOT, "include"), str(src)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
