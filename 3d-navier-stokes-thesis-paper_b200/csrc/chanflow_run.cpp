@@ -1,0 +1,210 @@
+// chanflow_run.cpp -- the reference's DNS program (PFC/main_mpi.f90, the
+// `mpiflow` executable) as a host program over the C ABI, on one GPU and
+// without MPI: reads flow.dat (read_parms), sets up the grid and the
+// wavenumbers (define_coordinates, define_parameters), makes the initial
+// field (define_initial_field) and runs `timestep` with the reference's
+// output cadence: WTIME every output_step steps, a VTK snapshot when vel_out,
+// a restart file every save_step steps when save_vel, the l2 norm every
+// l2_step steps (PFC/main_mpi.f90:55-116).
+//
+//   chanflow_run flow.dat [--steps N] [--outdir DIR] [--device D] [--restart FILE]
+//
+// The reference's RANDOM_NUMBER draws (initial field, jet forcing) are the
+// library's seeded counter generator (cfh_rng_u01) with the flow.dat seed.
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "chanflow.h"
+#include "chanflow_host.h"
+
+namespace {
+
+void usage(FILE* f) {
+  fprintf(f,
+          "usage: chanflow_run flow.dat [--steps N] [--outdir DIR] [--device D] [--restart FILE]\n"
+          "  runs the channel-flow DNS of flow.dat on one GPU (mpiflow's time loop):\n"
+          "  --steps N      override tend\n"
+          "  --outdir DIR   where t_###.vtk and restart files go (default .)\n"
+          "  --device D     CUDA device (default 0)\n"
+          "  --restart FILE initial field from a restart file (read_vel)\n");
+}
+
+int check(cfg_ctx* c, int r, const char* what) {
+  if (r == CFG_OK) return 0;
+  if (r == CFG_E_CFL) fprintf(stderr, "CFL IS TOO BIG\n");
+  else if (r == CFG_E_DT) fprintf(stderr, "DT IS TOO BIG\n");
+  else fprintf(stderr, "%s failed (%d): %s\n", what, r, c ? cfg_last_error(c) : "");
+  return 1;
+}
+
+// the jet forcing parameters of define_parameters (PFC/setup.f90:1481-1491):
+// amplitude, Strouhal number and two phases per (component, wall), and a
+// random-walk increment of +-0.1 each
+void jet_forcing_init(unsigned long long seed, double* jf, double* inc) {
+  const double two_pi = 2.0 * std::acos(-1.0);
+  for (int i = 0; i < 24; ++i) {
+    const double u = cfh_rng_u01(seed, i, 0, 0, 5), v = cfh_rng_u01(seed, i, 0, 0, 6);
+    const int kind = i / 6;   // (3,2,4) column-major: the last index is the slowest
+    jf[i] = kind == 0 ? 0.01 + 0.06 * u : kind == 1 ? 0.1 + 0.6 * u : two_pi * u;
+    inc[i] = v - 0.5 >= 0.0 ? 0.1 : -0.1;
+  }
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  const char* path = nullptr;
+  const char* restart = nullptr;
+  std::string outdir = ".";
+  int steps = -1, device = 0;
+  for (int i = 1; i < argc; ++i) {
+    const std::string a = argv[i];
+    if (a == "-h" || a == "--help") {
+      usage(stdout);
+      return 0;
+    } else if (a == "--steps" && i + 1 < argc) {
+      steps = atoi(argv[++i]);
+    } else if (a == "--outdir" && i + 1 < argc) {
+      outdir = argv[++i];
+    } else if (a == "--device" && i + 1 < argc) {
+      device = atoi(argv[++i]);
+    } else if (a == "--restart" && i + 1 < argc) {
+      restart = argv[++i];
+    } else if (!a.empty() && a[0] != '-' && !path) {
+      path = argv[i];
+    } else {
+      usage(stderr);
+      return 2;
+    }
+  }
+  if (!path) {
+    usage(stderr);
+    return 2;
+  }
+  // read_parms
+  cfh_run run;
+  cfh_run_defaults(&run);
+  char err[256] = {0};
+  if (cfh_read_flow_dat(path, &run, err, sizeof(err)) != 0) {
+    fprintf(stderr, "%s: %s\n", path, err);
+    return 1;
+  }
+  if (steps >= 0) run.tend = steps;
+  if (run.output_step < 1) run.output_step = 1;
+  if (run.save_step < 1) run.save_step = 1;
+  if (run.l2_step < 1) run.l2_step = 1;
+  // define_coordinates, define_parameters
+  cfh_grid* g = cfh_grid_alloc(run.nx, run.ny, run.nz, run.nx2, run.nz2);
+  if (!g || cfh_define_grid(g, run.lx, run.lz, run.stretch, run.uniform_grid) != 0) {
+    fprintf(stderr, "grid set-up failed\n");
+    cfh_grid_free(g);
+    return 1;
+  }
+  cfg_params p{};
+  p.nx = run.nx; p.ny = run.ny; p.nz = run.nz; p.nx2 = run.nx2; p.nz2 = run.nz2;
+  p.re = run.re; p.lx = run.lx; p.lz = run.lz; p.beta = run.beta;
+  p.dt = run.dt > 0.0 ? run.dt : 0.25 * run.lx / run.nx;   // PFC/setup.f90:1377
+  p.cfl_max = 0.95;                                         // :1378
+  p.fix_mass = run.fix_mass; p.dt_flag = run.dt_flag;
+  p.ctrlu = run.ctrlu; p.ctrlw = run.ctrlw;
+  p.precision = run.precision; p.device = device;
+  cfg_grid cg{g->y, g->yh, g->hn, g->dh, g->dn, g->iu, g->dm, g->d2h, g->d2n, g->dyh, g->dy, g->kx, g->kz,
+              nullptr, nullptr};
+  cfg_ctx* c = nullptr;
+  int r = cfg_create(&p, &cg, &c);
+  if (r != CFG_OK) {
+    fprintf(stderr, "cfg_create failed (%d)\n", r);
+    cfh_grid_free(g);
+    return 1;
+  }
+  int bad = 0;
+  // the fringe (init_buffer) and the crossflow jet (define_parameters)
+  if (run.fringe_gain != 0.0 && (run.xfringe || run.zfringe)) {
+    cfg_fringe f{run.fringe_gain, run.xfringe, run.zfringe, run.frac_xbuff, run.buff_xrise, run.buff_xfall,
+                 run.frac_zbuff};
+    bad = bad || check(c, cfg_init_buffer(c, &f), "cfg_init_buffer");
+  }
+  if (!bad && (run.crossflow == 1 || run.jet_mode != 0)) {
+    cfg_jet j{};
+    j.mode = run.jet_mode != 0 ? run.jet_mode : 1;
+    j.xjet[0] = run.lx * run.xjet_bot; j.xjet[1] = run.lx * run.xjet_top;
+    j.zjet[0] = run.lz * run.zjet_bot; j.zjet[1] = run.lz * run.zjet_top;
+    j.jetmag[0] = run.jetmag_bot; j.jetmag[1] = run.jetmag_top;
+    if (j.mode == 2) j.jetmag[0] = run.jet_peak;
+    j.forcing[0] = run.forcing_bot; j.forcing[1] = run.forcing_top;
+    j.for_freq[0] = run.for_freq_bot; j.for_freq[1] = run.for_freq_top;
+    j.jet_diam = run.jet_diam;
+    j.width = run.jet_width; j.freq = run.jet_freq;
+    j.frac_xbuff = run.frac_xbuff;
+    j.filter_jet_profile = run.filter_jet_profile;
+    j.seed = run.seed;
+    jet_forcing_init(run.seed, j.jet_forcing, j.jet_forcing_incr);
+    bad = bad || check(c, cfg_set_jet(c, &j), "cfg_set_jet");
+  }
+  // define_initial_field
+  if (!bad && restart && run.read_vel) {
+    bad = check(c, cfg_read_velocity(c, restart), "cfg_read_velocity");
+  } else if (!bad) {
+    const size_t n = (size_t)run.nz * (run.nx / 2 + 1) * (run.ny + 1) * 3 * 2;
+    std::vector<double> d1(n, 0.0), d4(n / 3, 0.0);
+    if (cfh_initial_field(g, run.which_test, run.seed, run.disturb_ampl, run.beta, d1.data()) != 0) {
+      fprintf(stderr, "which_test %d is not supported\n", run.which_test);
+      bad = 1;
+    } else {
+      bad = check(c, cfg_upload_state(c, d1.data(), nullptr, d4.data()), "cfg_upload_state");
+      // which_test 6 (decaying vortices) runs without a mean pressure gradient
+      if (!bad && run.which_test == 6) bad = check(c, cfg_set_scalars(c, 0.0, p.dt, 0.0, nullptr), "cfg_set_scalars");
+    }
+  }
+  bad = bad || check(c, cfg_remove_initial_divergence(c), "cfg_remove_initial_divergence");
+  bad = bad || check(c, cfg_compute_initial_pressure(c, 0), "cfg_compute_initial_pressure");
+  double t_total = 0.0, dt = 0.0, p_grad = 0.0, l2 = 0.0, drag = 0.0;
+  if (!bad) {
+    cfg_get_scalars(c, &t_total, &dt, &p_grad, nullptr, nullptr);
+    printf(" INITIAL DT = %.16e\n INITIAL TIME = %.16e\n", dt, t_total);
+    bad = check(c, cfg_l2_norm(c, &l2, &drag), "cfg_l2_norm");
+    if (!bad) printf(" l2 = %.10e  drag = %.10e\n", l2, drag);
+  }
+  // timestep
+  auto t0 = std::chrono::steady_clock::now();
+  for (int step = 1; step <= run.tend && !bad; ++step) {
+    bad = check(c, cfg_timestep(c, 1), "cfg_timestep");
+    if (bad) break;
+    if (step % run.output_step == 0) {
+      bad = check(c, cfg_synchronize(c), "cfg_synchronize");
+      const auto t1 = std::chrono::steady_clock::now();
+      printf("WTIME = %12.6f  OVER %6d  STEPS\n", std::chrono::duration<double>(t1 - t0).count(), run.output_step);
+      fflush(stdout);
+      if (!bad && run.vel_out == 1) {
+        char name[64];
+        snprintf(name, sizeof(name), "/t_%03d.vtk", step / run.output_step);
+        bad = check(c, cfg_write_vtk(c, (outdir + name).c_str()), "cfg_write_vtk");
+      }
+      t0 = std::chrono::steady_clock::now();
+    }
+    if (!bad && run.save_vel == 1 && step % run.save_step == 0) {
+      char name[64];
+      snprintf(name, sizeof(name), "/vel_%07d.out", step);
+      bad = check(c, cfg_save_velocity(c, (outdir + name).c_str()), "cfg_save_velocity");
+    }
+    if (!bad && step % run.l2_step == 0) {
+      bad = check(c, cfg_status(c), "time step");
+      if (!bad) bad = check(c, cfg_l2_norm(c, &l2, &drag), "cfg_l2_norm");
+      if (!bad) printf(" step %d  l2 = %.10e  drag = %.10e\n", step, l2, drag);
+    }
+  }
+  if (!bad) bad = check(c, cfg_status(c), "time step");
+  if (!bad) bad = check(c, cfg_wait_io(c), "cfg_wait_io");
+  if (!bad) {
+    cfg_get_scalars(c, &t_total, &dt, &p_grad, nullptr, nullptr);
+    printf(" FINAL TIME = %.16e  DT = %.16e  P_GRAD = %.16e\n", t_total, dt, p_grad);
+  }
+  cfg_destroy(c);
+  cfh_grid_free(g);
+  return bad ? 3 : 0;
+}

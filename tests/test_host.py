@@ -179,3 +179,18 @@ def test_headers_compile_as_c99(tmp_path):
     r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-fsyntax-only",
                         "-I" + os.path.join(ROOT, "include"), str(src)], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+RUN_BIN = os.path.join(ROOT, "3d-navier-stokes-thesis-paper_b200", "lib", "chanflow_run")
+
+
+@pytest.mark.skipif(not os.path.exists(RUN_BIN), reason="chanflow_run not built")
+def test_run_program_arguments(tmp_path):
+    """chanflow_run (the DNS program over the C ABI): usage, a missing
+    argument and an unreadable flow.dat are refused before any device work."""
+    import subprocess
+    r = subprocess.run([RUN_BIN, "--help"], capture_output=True, text=True)
+    assert r.returncode == 0 and "usage: chanflow_run" in r.stdout
+    assert subprocess.run([RUN_BIN], capture_output=True).returncode == 2
+    r = subprocess.run([RUN_BIN, str(tmp_path / "missing.dat")], capture_output=True, text=True)
+    assert r.returncode == 1 and "cannot open" in r.stderr
