@@ -1,5 +1,15 @@
 // capi.cu -- the C ABI of include/chanflow.h: device state, plans, kernel
 // orchestration for one channel-flow context on one B200.
+//
+// Sections, in order: layout-conversion kernels (Fortran arrays <-> device
+// state); the context (cfg_ctx) and its per-launch timing; Impl<T>, the
+// step's orchestration per precision (set-up, the three nonlinear phases,
+// the rhs solve with its side streams, plane transforms, jet, boundary,
+// l2); the entry points of one context (create, state, step, transforms,
+// diagnostics, Arnoldi matvec); background file output and
+// post-processing; the fringe; multi-rank runs (partition, one-process
+// groups, one process per rank); the launch-shape autotuner; ensembles
+// stepped by CUDA graphs.
 #include <cuda_runtime.h>
 
 #include <cmath>
