@@ -194,3 +194,42 @@ def test_run_program_arguments(tmp_path):
     assert subprocess.run([RUN_BIN], capture_output=True).returncode == 2
     r = subprocess.run([RUN_BIN, str(tmp_path / "missing.dat")], capture_output=True, text=True)
     assert r.returncode == 1 and "cannot open" in r.stderr
+
+
+def test_group_splits_and_gathers_kx_slabs(cf):
+    """chanflow.Group's host side: whole-field arrays in the reference layouts
+    go to the ranks as their kx slabs (data1 axis 1, data2 and data4 the last
+    axis) and come back concatenated in rank order."""
+    nx, ny, nz, n = 32, 9, 16, 3
+    part = cf.partition(nx, nz, 3 * nz // 2, n)
+
+    class FakeRank:
+        def __init__(self, i):
+            self.i = i
+            self.got = None
+
+        def upload_state(self, d1, d2, d4):
+            self.got = (np.array(d1), np.array(d2), np.array(d4))
+
+        def download_state(self):
+            return self.got
+
+    g = cf.Group.__new__(cf.Group)
+    g.part = part
+    g.ranks = [FakeRank(i) for i in range(n)]
+    nxh = nx // 2 + 1
+    rng = np.random.default_rng(0)
+    d1 = rng.standard_normal((nz, nxh, ny + 1, 3)) + 0j
+    d2 = rng.standard_normal((ny + 1, 3, nz, nxh)) + 0j
+    d4 = rng.standard_normal((ny + 1, nz, nxh)) + 0j
+    g.upload_state(d1, d2, d4)
+    for i, r in enumerate(g.ranks):
+        x0, nl = int(part["x_start"][i]), int(part["nx_proc"][i])
+        np.testing.assert_array_equal(r.got[0], d1[:, x0:x0 + nl])
+        np.testing.assert_array_equal(r.got[1], d2[..., x0:x0 + nl])
+        np.testing.assert_array_equal(r.got[2], d4[..., x0:x0 + nl])
+    b1, b2, b4 = g.download_state()
+    np.testing.assert_array_equal(b1, d1)
+    np.testing.assert_array_equal(b2, d2)
+    np.testing.assert_array_equal(b4, d4)
+    g.h = None   # nothing to destroy
