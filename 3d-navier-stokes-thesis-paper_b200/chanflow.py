@@ -180,6 +180,9 @@ SYMBOLS = {
     "cfh_define_grid": (C.c_int, [C.POINTER(CfhGrid), C.c_double, C.c_double, C.c_double, C.c_int]),
     "cfh_initial_field": (C.c_int, [C.POINTER(CfhGrid), C.c_int, C.c_ulonglong, C.c_double,
                                     C.c_double, _VP]),
+    "cfh_read_efn": (C.c_int, [C.c_char_p, _VP]),
+    "cfh_interp_eigenfunction": (C.c_int, [C.POINTER(CfhGrid), _VP, _VP, _VP]),
+    "cfh_initial_field_mode": (C.c_int, [C.POINTER(CfhGrid), C.c_int, C.c_double, C.c_double, _VP, _VP, _VP]),
     "cfh_rng_u01": (C.c_double, [C.c_ulonglong, C.c_int, C.c_int, C.c_int, C.c_int]),
     "cfh_save_velocity": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                     C.c_double, C.c_double, _VP, C.c_char_p, C.c_int]),
@@ -256,18 +259,40 @@ class Grid:
         return g, keep
 
 
-def initial_field(grid, which_test, seed=1, ampl=1e-3, beta=0.0):
+def initial_field(grid, which_test, seed=1, ampl=1e-3, beta=0.0, efn=None):
     """Seeded which_test initial velocity in data1 layout (before the device
-    divergence removal and initial pressure)."""
+    divergence removal and initial pressure).  which_test 2, 5 and 8 (the
+    Orr-Sommerfeld mode, PFC/init_vel.f90:95-159) take the eigenfunction as
+    efn: the (65, 4) array of efn.m (Re u, Im u, Re v, Im v at the Chebyshev
+    points) or the path of such a file."""
     L = load_library()
     nxh = grid.nx // 2 + 1
     d1 = np.zeros((grid.nz, nxh, grid.ny + 1, 3), dtype=np.complex128, order="F")
     h = L.cfh_grid_alloc(grid.nx, grid.ny, grid.nz, grid.nx2, grid.nz2)
-    for name in ("y", "yh", "dh", "dyh", "kx", "kz"):
-        src = np.ascontiguousarray(getattr(grid, name).ravel(order="F"))
-        C.memmove(getattr(h.contents, name), src.ctypes.data, src.nbytes)
-    r = L.cfh_initial_field(h, which_test, seed, ampl, beta, d1.ctypes.data)
-    L.cfh_grid_free(h)
+    try:
+        for name in ("y", "yh", "dh", "dyh", "kx", "kz"):
+            src = np.ascontiguousarray(getattr(grid, name).ravel(order="F"))
+            C.memmove(getattr(h.contents, name), src.ctypes.data, src.nbytes)
+        if which_test in (2, 5, 8):
+            if efn is None:
+                raise ChanflowError(f"which_test {which_test} needs the eigenfunction (efn)")
+            if isinstance(efn, (str, bytes, os.PathLike)):
+                uin = np.zeros((65, 4), order="F")
+                r = L.cfh_read_efn(os.fsencode(efn), uin.ctypes.data)
+                if r != 0:
+                    raise ChanflowError(f"cannot read the eigenfunction file {efn!r} ({r})")
+            else:
+                uin = np.asfortranarray(efn, dtype=np.float64)
+                if uin.shape != (65, 4):
+                    raise ChanflowError(f"efn must be (65, 4), got {uin.shape}")
+            u = np.zeros(grid.ny + 1, np.complex128)
+            v = np.zeros(grid.ny + 1, np.complex128)
+            L.cfh_interp_eigenfunction(h, uin.ctypes.data, u.ctypes.data, v.ctypes.data)
+            r = L.cfh_initial_field_mode(h, which_test, ampl, beta, u.ctypes.data, v.ctypes.data, d1.ctypes.data)
+        else:
+            r = L.cfh_initial_field(h, which_test, seed, ampl, beta, d1.ctypes.data)
+    finally:
+        L.cfh_grid_free(h)
     if r != 0:
         raise ChanflowError(f"unsupported which_test {which_test}")
     return d1
@@ -564,8 +589,11 @@ class ChannelFlow:
         return out
 
     # ---- define_initial_field (PFC/init_vel.f90:25-353) on the device
-    def define_initial_field(self, which_test, seed=1, ampl=1e-3, beta=0.0):
-        d1 = initial_field(self.grid, which_test, seed, ampl, beta)
+    def define_initial_field(self, which_test, seed=1, ampl=1e-3, beta=0.0, efn=None):
+        """define_initial_field (PFC/init_vel.f90:24-352): the which_test
+        velocity (efn: the eigenfunction of which_test 2, 5, 8), its
+        divergence removed and the initial pressure computed, t = 0."""
+        d1 = initial_field(self.grid, which_test, seed, ampl, beta, efn)
         self.upload_state(d1, None, np.zeros(self.shapes()[2], np.complex128, order="F"))
         if which_test == 6:
             sc = self.scalars()

@@ -3,11 +3,24 @@
 // without MPI: reads flow.dat (read_parms), sets up the grid and the
 // wavenumbers (define_coordinates, define_parameters), makes the initial
 // field (define_initial_field) and runs `timestep` with the reference's
-// output cadence: WTIME every output_step steps, a VTK snapshot when vel_out,
-// a restart file every save_step steps when save_vel, the l2 norm every
-// l2_step steps (PFC/main_mpi.f90:55-116).
+// output cadence (PFC/main_mpi.f90:40-116): a VTK snapshot t_000.vtk before
+// the loop when vel_out, WTIME every output_step steps, a VTK snapshot then
+// when vel_out, the restart file newvel.out every save_step steps and once
+// after the loop when save_vel, the l2 norm every l2_step steps, and for
+// which_test 2 the mode's energy in fort.80 (PFC/pass2.f90:126-133).
 //
 //   chanflow_run flow.dat [--steps N] [--outdir DIR] [--device D] [--restart FILE]
+//
+// define_parameters' choices are kept: p_grad starts at -2/Re, or 0 with an
+// x fringe (PFC/setup.f90:1384-1385) or for which_test 6; with read_vel = 1
+// the initial field is the restart file (--restart, else savevel.out in the
+// working directory, as read_velocity opens it, PFC/read_write.f90:34), and
+// a missing file is an error; --restart with read_vel = 0 is refused.
+// which_test 2, 5, 8 (the Orr-Sommerfeld mode of PFC/init_vel.f90:95-159)
+// read the eigenfunction from efn.m in the working directory; their dt
+// (cfh_read_flow_dat: 2 (2 pi / 0.24989154) / tend for tend >= 40,
+// PFC/setup.f90:1386-1388) uses flow.dat's tend, so --steps runs a prefix of
+// that run.
 //
 // The reference's RANDOM_NUMBER draws (initial field, jet forcing) are the
 // library's seeded counter generator (cfh_rng_u01) with the flow.dat seed.
@@ -55,6 +68,26 @@ void jet_forcing_init(unsigned long long seed, double* jf, double* inc) {
   }
 }
 
+// ke(2,1) of rhs_solve (PFC/pass2.f90:113-117): the kinetic energy of Fourier
+// column (kz 1, kx 2) of data1, |u|^2 + |w|^2 on the yh planes and |v|^2
+// averaged onto them, integrated with dyh
+double mode_energy(const cfh_grid* g, const double* data1) {
+  const int nz = g->nz, nxh = g->nx / 2 + 1, n1 = g->ny + 1, ny = g->ny;
+  auto at = [&](int j, int c, int k) { return data1[2 * (0 + (size_t)nz * (1 + (size_t)nxh * (j + (size_t)n1 * c))) + k]; };
+  auto a2 = [&](int j, int c) { return at(j, c, 0) * at(j, c, 0) + at(j, c, 1) * at(j, c, 1); };
+  double ke = 0.0;
+  for (int j = 0; j < n1; ++j) {
+    double t = a2(j, 0) + a2(j, 2);
+    if (j == 0) t += a2(0, 1);
+    else if (j < ny) {
+      const double re = 0.5 * (at(j, 1, 0) + at(j - 1, 1, 0)), im = 0.5 * (at(j, 1, 1) + at(j - 1, 1, 1));
+      t += re * re + im * im;
+    } else t += a2(ny - 1, 1);
+    ke += g->dyh[j] * t;
+  }
+  return ke;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -94,6 +127,11 @@ int main(int argc, char** argv) {
     fprintf(stderr, "%s: %s\n", path, err);
     return 1;
   }
+  if (restart && run.read_vel != 1) {
+    fprintf(stderr, "--restart given but %s has read_vel = %d (the initial field would not be read)\n", path,
+            run.read_vel);
+    return 2;
+  }
   if (steps >= 0) run.tend = steps;
   if (run.output_step < 1) run.output_step = 1;
   if (run.save_step < 1) run.save_step = 1;
@@ -123,6 +161,8 @@ int main(int argc, char** argv) {
     return 1;
   }
   int bad = 0;
+  // p_grad = -2/Re, or 0 with an x fringe (PFC/setup.f90:1384-1385)
+  if (run.xfringe == 1) bad = check(c, cfg_set_scalars(c, 0.0, p.dt, 0.0, nullptr), "cfg_set_scalars");
   // the fringe (init_buffer) and the crossflow jet (define_parameters)
   if (run.fringe_gain != 0.0 && (run.xfringe || run.zfringe)) {
     cfg_fringe f{run.fringe_gain, run.xfringe, run.zfringe, run.frac_xbuff, run.buff_xrise, run.buff_xfall,
@@ -147,15 +187,32 @@ int main(int argc, char** argv) {
     bad = bad || check(c, cfg_set_jet(c, &j), "cfg_set_jet");
   }
   // define_initial_field
-  if (!bad && restart && run.read_vel) {
-    bad = check(c, cfg_read_velocity(c, restart), "cfg_read_velocity");
+  if (!bad && run.read_vel == 1) {
+    const char* file = restart ? restart : "savevel.out";
+    bad = check(c, cfg_read_velocity(c, file), "cfg_read_velocity");
+    if (bad) fprintf(stderr, "read_vel = 1: could not read the restart file %s\n", file);
   } else if (!bad) {
     const size_t n = (size_t)run.nz * (run.nx / 2 + 1) * (run.ny + 1) * 3 * 2;
     std::vector<double> d1(n, 0.0), d4(n / 3, 0.0);
-    if (cfh_initial_field(g, run.which_test, run.seed, run.disturb_ampl, run.beta, d1.data()) != 0) {
+    int ri = 0;
+    if (run.which_test == 2 || run.which_test == 5 || run.which_test == 8) {
+      // READ_EIGENFUNCTION: efn.m in the working directory
+      std::vector<double> uin(4 * 65), u(2 * (run.ny + 1)), v(2 * (run.ny + 1));
+      if (cfh_read_efn("efn.m", uin.data()) != 0) {
+        fprintf(stderr, "which_test %d needs the eigenfunction file efn.m in the working directory\n",
+                run.which_test);
+        bad = 1;
+      } else {
+        cfh_interp_eigenfunction(g, uin.data(), u.data(), v.data());
+        ri = cfh_initial_field_mode(g, run.which_test, run.disturb_ampl, run.beta, u.data(), v.data(), d1.data());
+      }
+    } else {
+      ri = cfh_initial_field(g, run.which_test, run.seed, run.disturb_ampl, run.beta, d1.data());
+    }
+    if (!bad && ri != 0) {
       fprintf(stderr, "which_test %d is not supported\n", run.which_test);
       bad = 1;
-    } else {
+    } else if (!bad) {
       bad = check(c, cfg_upload_state(c, d1.data(), nullptr, d4.data()), "cfg_upload_state");
       // which_test 6 (decaying vortices) runs without a mean pressure gradient
       if (!bad && run.which_test == 6) bad = check(c, cfg_set_scalars(c, 0.0, p.dt, 0.0, nullptr), "cfg_set_scalars");
@@ -169,6 +226,20 @@ int main(int argc, char** argv) {
     printf(" INITIAL DT = %.16e\n INITIAL TIME = %.16e\n", dt, t_total);
     bad = check(c, cfg_l2_norm(c, &l2, &drag), "cfg_l2_norm");
     if (!bad) printf(" l2 = %.10e  drag = %.10e\n", l2, drag);
+    // the snapshot of the initial field (PFC/main_mpi.f90:42)
+    if (!bad && run.vel_out == 1) bad = check(c, cfg_write_vtk(c, (outdir + "/t_000.vtk").c_str()), "cfg_write_vtk");
+  }
+  // the Orr-Sommerfeld run's record of the mode (fort.80, PFC/pass2.f90:126-133):
+  // time, ke(2,1), p_grad and half log(ke)/time at every output step
+  FILE* fort80 = nullptr;
+  std::vector<double> d1out;
+  if (!bad && run.which_test == 2 && run.read_vel == 0) {
+    fort80 = fopen((outdir + "/fort.80").c_str(), "w");
+    if (!fort80) {
+      fprintf(stderr, "cannot write %s/fort.80\n", outdir.c_str());
+      bad = 1;
+    }
+    d1out.resize((size_t)run.nz * (run.nx / 2 + 1) * (run.ny + 1) * 3 * 2);
   }
   // timestep
   auto t0 = std::chrono::steady_clock::now();
@@ -187,10 +258,15 @@ int main(int argc, char** argv) {
       }
       t0 = std::chrono::steady_clock::now();
     }
-    if (!bad && run.save_vel == 1 && step % run.save_step == 0) {
-      char name[64];
-      snprintf(name, sizeof(name), "/vel_%07d.out", step);
-      bad = check(c, cfg_save_velocity(c, (outdir + name).c_str()), "cfg_save_velocity");
+    if (!bad && run.save_vel == 1 && step % run.save_step == 0)
+      bad = check(c, cfg_save_velocity(c, (outdir + "/newvel.out").c_str()), "cfg_save_velocity");
+    if (!bad && fort80 && (step % run.output_step == 0 || step == run.tend)) {
+      bad = check(c, cfg_download_state(c, d1out.data(), nullptr, nullptr), "cfg_download_state");
+      if (!bad) {
+        cfg_get_scalars(c, &t_total, &dt, &p_grad, nullptr, nullptr);
+        const double ke = mode_energy(g, d1out.data());
+        fprintf(fort80, "%10.3f%24.14E%24.14E%24.14E\n", t_total, ke, p_grad, 0.5 * std::log(ke + 1e-16) / t_total);
+      }
     }
     if (!bad && step % run.l2_step == 0) {
       bad = check(c, cfg_status(c), "time step");
@@ -199,11 +275,15 @@ int main(int argc, char** argv) {
     }
   }
   if (!bad) bad = check(c, cfg_status(c), "time step");
+  // the final restart file (PFC/main_mpi.f90:46)
+  if (!bad && run.save_vel == 1)
+    bad = check(c, cfg_save_velocity(c, (outdir + "/newvel.out").c_str()), "cfg_save_velocity");
   if (!bad) bad = check(c, cfg_wait_io(c), "cfg_wait_io");
   if (!bad) {
     cfg_get_scalars(c, &t_total, &dt, &p_grad, nullptr, nullptr);
     printf(" FINAL TIME = %.16e  DT = %.16e  P_GRAD = %.16e\n", t_total, dt, p_grad);
   }
+  if (fort80) fclose(fort80);
   cfg_destroy(c);
   cfh_grid_free(g);
   return bad ? 3 : 0;

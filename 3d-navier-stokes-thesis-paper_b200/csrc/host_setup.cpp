@@ -96,12 +96,6 @@ int cfh_read_flow_dat(const char* path, cfh_run* r, char* err, int errlen) {
   r->beta = r->beta * asin(1.0);
   if (scale_by_pi == 1) r->lx = r->lx * pi;
   r->lz = r->lx / aspect;
-  if (r->read_vel == 0) {   // which_test presets, PFC/setup.f90:163-201
-    if (r->which_test == 2) { r->re = 7500; r->lx = 2 * pi; r->beta = 0; r->fix_mass = 0; r->crossflow = 0; r->bl_grid = 0; r->xfringe = r->zfringe = 0; }
-    else if (r->which_test == 5) { r->re = 7500; r->lz = 2 * pi; r->beta = pi / 2; r->fix_mass = 0; r->crossflow = 0; r->bl_grid = 0; r->xfringe = r->zfringe = 0; }
-    else if (r->which_test == 8) { r->re = 7500; r->lx = 2 * sqrt(2.0) * pi; r->lz = r->lx; r->beta = pi / 4; r->fix_mass = 0; r->crossflow = 0; r->bl_grid = 0; r->xfringe = r->zfringe = 0; }
-    else if (r->which_test == 6) { r->re = 10; r->lx = 2; r->fix_mass = 0; r->crossflow = 0; r->bl_grid = 0; r->xfringe = r->zfringe = 0; r->uniform_grid = 1; }
-  }
   // extension block (lines after 95, "value  name"); the Fortran reader ignores it
   for (size_t i = ln; i < lines.size(); ++i) {
     double v;
@@ -121,8 +115,19 @@ int cfh_read_flow_dat(const char* path, cfh_run* r, char* err, int errlen) {
     else if (n == "which_test") r->which_test = (int)v;
     else if (n == "disturb_ampl") r->disturb_ampl = v;
   }
-  if (r->dt <= 0) {   // define_parameters, PFC/setup.f90:1377,1389-1393
+  // which_test presets, PFC/setup.f90:163-201 (after the extension block,
+  // which may set which_test)
+  if (r->read_vel == 0) {
+    if (r->which_test == 2) { r->re = 7500; r->lx = 2 * pi; r->beta = 0; r->fix_mass = 0; r->crossflow = 0; r->bl_grid = 0; r->xfringe = r->zfringe = 0; }
+    else if (r->which_test == 5) { r->re = 7500; r->lz = 2 * pi; r->beta = pi / 2; r->fix_mass = 0; r->crossflow = 0; r->bl_grid = 0; r->xfringe = r->zfringe = 0; }
+    else if (r->which_test == 8) { r->re = 7500; r->lx = 2 * sqrt(2.0) * pi; r->lz = r->lx; r->beta = pi / 4; r->fix_mass = 0; r->crossflow = 0; r->bl_grid = 0; r->xfringe = r->zfringe = 0; }
+    else if (r->which_test == 6) { r->re = 10; r->lx = 2; r->fix_mass = 0; r->crossflow = 0; r->bl_grid = 0; r->xfringe = r->zfringe = 0; r->uniform_grid = 1; }
+  }
+  if (r->dt <= 0) {   // define_parameters, PFC/setup.f90:1377,1386-1393
     r->dt = 0.25 * r->lx / (double)r->nx;
+    // the Orr-Sommerfeld runs: two periods of the mode in tend steps
+    if (r->read_vel == 0 && r->which_test % 3 == 2 && r->tend >= 40)
+      r->dt = 2.0 * (2.0 * pi / 0.24989154) / (double)r->tend;
     if (r->read_vel == 0 && r->which_test == 6) {
       r->dt = 0.5 / (double)r->ny;
       r->tend = (int)(1.0 / r->dt);
@@ -312,6 +317,94 @@ int cfh_initial_field(const cfh_grid* g, int which_test, unsigned long long seed
         for (int c = 0; c < 3; ++c)
           for (int j = 0; j < n1; ++j) D1(z, x, j, c) = cu[c * n1 + j] * f;
       }
+  }
+  return 0;
+}
+
+int cfh_read_efn(const char* path, double* uin) {
+  FILE* f = fopen(path, "r");
+  if (!f) return -1;
+  char tok[128];
+  int n = 0;
+  while (n < 4 * 65 && fscanf(f, "%127s", tok) == 1) {
+    for (char* p = tok; *p; ++p)
+      if (*p == 'D' || *p == 'd') *p = 'e';   // Fortran double-precision exponent
+    char* end = nullptr;
+    const double v = strtod(tok, &end);
+    if (end == tok || *end != '\0') break;
+    uin[n++] = v;
+  }
+  fclose(f);
+  return n == 4 * 65 ? 0 : -2;
+}
+
+int cfh_interp_eigenfunction(const cfh_grid* g, const double* uin, double* u, double* v) {
+  constexpr int nc = 65;
+  const int ny = g->ny, n1 = ny + 1;
+  const double nn = nc - 1, pi = atan2(0.0, -1.0);
+  // Chebyshev coefficients: T(i,j) = (2/N) cos(pi (i-1)(j-1) / N), halved on
+  // the first and last row and column
+  double ucheb[nc][4] = {};
+  for (int i = 0; i < nc; ++i)
+    for (int j = 0; j < nc; ++j) {
+      double t = (2.0 / nn) * cos(pi * (double)(i * j) / nn);
+      if (i == 0 || i == nc - 1) t *= 0.5;
+      if (j == 0 || j == nc - 1) t *= 0.5;
+      for (int k = 0; k < 4; ++k) ucheb[i][k] += t * uin[j + nc * k];
+    }
+  auto series = [&](double y, int k) {
+    const double th = acos(y < -1.0 ? -1.0 : y > 1.0 ? 1.0 : y);
+    double s = 0.0;
+    for (int j = 0; j < nc; ++j) s += cos((double)j * th) * ucheb[j][k];
+    return s;
+  };
+  for (int p = 0; p < 2 * n1; ++p) u[p] = v[p] = 0.0;
+  for (int p = 1; p < ny; ++p) {   // yh(2..ny)
+    u[2 * p] = series(g->yh[p], 0);
+    u[2 * p + 1] = series(g->yh[p], 1);
+  }
+  for (int p = 0; p < ny; ++p) {   // y(1..ny)
+    v[2 * p] = series(g->y[p], 2);
+    v[2 * p + 1] = series(g->y[p], 3);
+  }
+  return 0;
+}
+
+int cfh_initial_field_mode(const cfh_grid* g, int which_test, double ampl, double beta, const double* u,
+                           const double* v, double* data1) {
+  if (which_test != 2 && which_test != 5 && which_test != 8) return -1;
+  const int nx = g->nx, ny = g->ny, nz = g->nz, nxh = nx / 2 + 1, n1 = ny + 1;
+  if (nxh < 2 || nz < 2) return -1;
+  cd* d1 = reinterpret_cast<cd*>(data1);
+  const cd* uu = reinterpret_cast<const cd*>(u);
+  const cd* vv = reinterpret_cast<const cd*>(v);
+  const size_t nf = (size_t)nz * nxh * n1;
+  for (size_t i = 0; i < 3 * nf; ++i) d1[i] = 0.0;
+  auto D1 = [&](int z, int x, int j, int c) -> cd& { return d1[z + (size_t)nz * (x + (size_t)nxh * (j + (size_t)n1 * c))]; };
+  for (int j = 0; j < n1; ++j) {
+    const double lam = 1.0 - g->yh[j] * g->yh[j];
+    if (which_test == 2) D1(0, 0, j, 0) = lam;
+    else if (which_test == 5) D1(0, 0, j, 2) = lam;
+    else { D1(0, 0, j, 0) = lam * cos(beta); D1(0, 0, j, 2) = lam * sin(beta); }
+  }
+  if (which_test == 2) {          // (z 1, x 2)
+    for (int j = 0; j < n1; ++j) D1(0, 1, j, 0) = ampl * uu[j];
+    for (int j = 0; j < ny; ++j) D1(0, 1, j, 1) = ampl * vv[j];
+  } else if (which_test == 5) {   // (z 2, x 1) and its conjugate (z nz, x 1)
+    for (int j = 0; j < n1; ++j) {
+      D1(1, 0, j, 2) = ampl * uu[j];
+      D1(nz - 1, 0, j, 2) = ampl * std::conj(uu[j]);
+    }
+    for (int j = 0; j < ny; ++j) {
+      D1(1, 0, j, 1) = ampl * vv[j];
+      D1(nz - 1, 0, j, 1) = ampl * std::conj(vv[j]);
+    }
+  } else {                        // (z 2, x 2), rotated by beta
+    for (int j = 0; j < n1; ++j) {
+      D1(1, 1, j, 0) = ampl * uu[j] * cos(beta);
+      D1(1, 1, j, 2) = ampl * uu[j] * sin(beta);
+    }
+    for (int j = 0; j < ny; ++j) D1(1, 1, j, 1) = ampl * vv[j];
   }
   return 0;
 }

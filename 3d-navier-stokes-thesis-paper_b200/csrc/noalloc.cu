@@ -32,10 +32,25 @@ constexpr int kMaxLen = 2048;                    // nx2, nz2 upper bound
 // contents.
 static __device__ __align__(256) double2 g_scratch[kMaxHybrid + 2 * (size_t)kMaxLen];
 
-// Device address of g_scratch per device, taken once with that device current.
+// Per device, with that device current at the first call: the device address
+// of g_scratch, and the transform lengths whose twiddle tables the array holds
+// now (0: none), so that a call of the same lengths does not rewrite them.
 constexpr int kMaxDevices = 64;
 double2* g_scratch_addr[kMaxDevices] = {nullptr};
+int g_tw_len[kMaxDevices][2] = {};
 std::mutex g_setup_mutex;
+
+// Raise a kernel's dynamic shared-memory limit on the current device to
+// `need` bytes if it is lower; never lower it (other contexts may have raised
+// it for larger launches of the same kernel).
+template <typename K>
+cudaError_t raise_smem(K kernel, size_t need) {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+  if (e != cudaSuccess) return e;
+  if ((size_t)fa.maxDynamicSharedSizeBytes >= need) return cudaSuccess;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need);
+}
 
 bool plan_2_3(int n, FftPlan& p) {
   p = FftPlan{};
@@ -80,7 +95,9 @@ extern "C" int cfg_xz_c2r_noalloc(int nx, int nz, int nx2, int nz2, const double
   }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return CFG_E_CUDA;
+  const size_t smz = sizeof(double2) * 3 * (size_t)nz2, smx = sizeof(double2) * 3 * (size_t)nx2;
   double2* base = nullptr;
+  bool write_twx = false, write_twz = false;
   {
     std::lock_guard<std::mutex> lock(g_setup_mutex);
     if (!g_scratch_addr[dev]) {
@@ -91,27 +108,33 @@ extern "C" int cfg_xz_c2r_noalloc(int nx, int nz, int nx2, int nz2, const double
         cudaGetLastError();
         return CFG_E_CUDA;
       }
-      const int lim = 200 * 1024;
-      if (cudaFuncSetAttribute(k_pz_inv<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim) != cudaSuccess ||
-          cudaFuncSetAttribute(k_px_inv<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim) != cudaSuccess) {
-        cudaGetLastError();
-        return CFG_E_CUDA;
-      }
       g_scratch_addr[dev] = p;
     }
     base = g_scratch_addr[dev];
+    if (raise_smem(k_pz_inv<double>, smz) != cudaSuccess || raise_smem(k_px_inv<double>, smx) != cudaSuccess) {
+      cudaGetLastError();
+      return CFG_E_CUDA;
+    }
+    write_twx = g_tw_len[dev][0] != nx2;
+    write_twz = g_tw_len[dev][1] != nz2;
+    g_tw_len[dev][0] = nx2;
+    g_tw_len[dev][1] = nz2;
   }
   cudaStream_t st = (cudaStream_t)stream;
   double2* H = base;                 // hybrid plane (nx/2+1, nz2): fully rewritten below
   double2* twx = base + kMaxHybrid;  // W_nx2
   double2* twz = twx + kMaxLen;      // W_nz2
-  k_twiddles<<<8, 256, 0, st>>>(twx, nx2);
-  k_twiddles<<<8, 256, 0, st>>>(twz, nz2);
+  // the twiddle tables are written when the lengths change and kept otherwise
+  if (write_twx) k_twiddles<<<8, 256, 0, st>>>(twx, nx2);
+  if (write_twz) k_twiddles<<<8, 256, 0, st>>>(twz, nz2);
   PlaneIn L{0, 0, (size_t)nz, 1, 1};
-  const size_t smz = sizeof(double2) * 3 * (size_t)nz2, smx = sizeof(double2) * 3 * (size_t)nx2;
   k_pz_inv<double><<<dim3(nxh, 1), 128, smz, st>>>(reinterpret_cast<const double2*>(cdata), L, nullptr, 1, H, nxh,
                                                    nz, nz2, 1, nx2 > nx, pz, twz);
   k_px_inv<double><<<dim3((nz2 + 1) / 2, 1), 128, smx, st>>>(H, data, nxh, nz2, nx2, px, twx);
-  if (cudaGetLastError() != cudaSuccess) return CFG_E_CUDA;
+  if (cudaGetLastError() != cudaSuccess) {
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    g_tw_len[dev][0] = g_tw_len[dev][1] = 0;  // the tables may not have been written
+    return CFG_E_CUDA;
+  }
   return CFG_OK;
 }

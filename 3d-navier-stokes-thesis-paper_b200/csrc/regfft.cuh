@@ -16,59 +16,34 @@
 
 namespace cfd {
 
-// cos(2 pi m / 48), m in [0, 48): literal values so that every twiddle of the
-// small FFTs folds to an immediate operand.
-__host__ __device__ __forceinline__ constexpr double cos48(int m) {
-  return false ? 0.0
-         : m == 0 ? 1.0
+// cos(2 pi m / 48) for m in [0, 12]: the quarter wave, correctly rounded
+// to FP64 (checked against 50-digit values).  Literals so that every twiddle
+// of the small FFTs folds to an immediate operand.
+__host__ __device__ __forceinline__ constexpr double cos48q(int m) {
+  return m == 0 ? 1.0
          : m == 1 ? 0.9914448613738104
          : m == 2 ? 0.9659258262890683
          : m == 3 ? 0.9238795325112867
-         : m == 4 ? 0.8660254037844387
+         : m == 4 ? 0.8660254037844386
          : m == 5 ? 0.7933533402912352
          : m == 6 ? 0.7071067811865476
          : m == 7 ? 0.6087614290087207
-         : m == 8 ? 0.5000000000000001
-         : m == 9 ? 0.38268343236508984
+         : m == 8 ? 0.5
+         : m == 9 ? 0.3826834323650898
          : m == 10 ? 0.25881904510252074
-         : m == 11 ? 0.1305261922200517
-         : m == 12 ? 0.0
-         : m == 13 ? -0.1305261922200516
-         : m == 14 ? -0.25881904510252063
-         : m == 15 ? -0.3826834323650895
-         : m == 16 ? -0.4999999999999998
-         : m == 17 ? -0.6087614290087207
-         : m == 18 ? -0.7071067811865475
-         : m == 19 ? -0.793353340291235
-         : m == 20 ? -0.8660254037844387
-         : m == 21 ? -0.9238795325112867
-         : m == 22 ? -0.9659258262890682
-         : m == 23 ? -0.9914448613738104
-         : m == 24 ? -1.0
-         : m == 25 ? -0.9914448613738104
-         : m == 26 ? -0.9659258262890683
-         : m == 27 ? -0.9238795325112868
-         : m == 28 ? -0.8660254037844388
-         : m == 29 ? -0.7933533402912352
-         : m == 30 ? -0.7071067811865479
-         : m == 31 ? -0.6087614290087209
-         : m == 32 ? -0.5000000000000004
-         : m == 33 ? -0.3826834323650895
-         : m == 34 ? -0.25881904510252063
-         : m == 35 ? -0.13052619222005163
-         : m == 36 ? 0.0
-         : m == 37 ? 0.13052619222005127
-         : m == 38 ? 0.2588190451025203
-         : m == 39 ? 0.38268343236508917
-         : m == 40 ? 0.5000000000000001
-         : m == 41 ? 0.6087614290087199
-         : m == 42 ? 0.7071067811865474
-         : m == 43 ? 0.7933533402912349
-         : m == 44 ? 0.8660254037844384
-         : m == 45 ? 0.9238795325112868
-         : m == 46 ? 0.9659258262890681
-         : m == 47 ? 0.9914448613738104
+         : m == 11 ? 0.1305261922200516
          : 0.0;
+}
+
+__host__ __device__ __forceinline__ constexpr double cos48_r(int r) {
+  return r <= 12 ? cos48q(r) : r <= 24 ? -cos48q(24 - r) : r <= 36 ? -cos48q(r - 24) : cos48q(48 - r);
+}
+
+// cos(2 pi m / 48) for any m, from the quarter wave by the symmetries
+// cos(pi - a) = -cos(a) and cos(2 pi - a) = cos(a): every entry is the
+// correctly rounded value, exact zeros at m = 12, 36 and exact halves.
+__host__ __device__ __forceinline__ constexpr double cos48(int m) {
+  return cos48_r(((m % 48) + 48) % 48);
 }
 
 // W_N^(m) with the transform sign: sign -1 -> exp(-2 pi i m/N), +1 -> conjugate

@@ -196,7 +196,11 @@ def throughput(world, units_per_rank, steps, ms_max):
 
 # --------------------------------------------------------------------------
 class Clocks:
-    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    """nvidia-smi samples of SM clock and throttle reasons during the timed
+    region, every 20 ms so that a timed region of a few tens of ms still has
+    samples of its own."""
+
+    PERIOD_MS = 20
 
     def __init__(self, device):
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
@@ -205,7 +209,7 @@ class Clocks:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                                       "-i", str(device), "-lms", "100"], stdout=self.f,
+                                       "-i", str(device), "-lms", str(self.PERIOD_MS)], stdout=self.f,
                                       stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
@@ -245,7 +249,8 @@ class Clocks:
         reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i]
                           and "Not" not in r[5 + i]})
         return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows),
+                "period_ms": self.PERIOD_MS}
 
 
 def make_flow(cf, nx, ny, nz, precision, device):
@@ -440,6 +445,87 @@ def run_arnoldi(args):
     return 0
 
 
+def pinned_state(torch, flow):
+    """Pinned host copies of the flow's data1, data2, data4 (reference
+    layouts, interleaved complex FP64) filled with its current state."""
+    s1, s2, s4 = flow.shapes()
+    pin = [torch.empty(int(np.prod(s)) * 2, dtype=torch.float64, pin_memory=True) for s in (s1, s2, s4)]
+    d1, d2, d4 = flow.download_state()
+    for t, a in zip(pin, (d1, d2, d4)):
+        t.numpy()[:] = np.asfortranarray(a).ravel(order="F").view(np.float64)
+    return pin
+
+
+def host_round_trip_steps(flow, ptr, n):
+    """n steps of a host-owned state through the C ABI: upload data1, data2,
+    data4 from pinned host memory, one time step, download them again."""
+    L = flow.L
+    for _ in range(n):
+        flow._chk(L.cfg_upload_state(flow.h, ptr[0], ptr[1], ptr[2]))
+        flow.timestep(1)
+        flow._chk(L.cfg_download_state(flow.h, ptr[0], ptr[1], ptr[2]))
+
+
+def e2e_overlapped(torch, cf, nx, ny, nz, dev, n):
+    """Two independent domains, each driven by its own host thread through
+    the same host round trip per step as the serial e2e: one domain's uploads
+    and downloads overlap the other's step and its copies in the other
+    direction (the C calls release the interpreter lock).  Device time from
+    events on both streams, first start to last end."""
+    import threading
+    flows = [make_flow(cf, nx, ny, nz, cf.MIXED, dev) for _ in range(2)]
+    pins = [pinned_state(torch, f) for f in flows]
+    streams = [torch.cuda.ExternalStream(f.stream_ptr()) for f in flows]
+    for f in flows:
+        host_round_trip_steps(f, [t.data_ptr() for t in pins[flows.index(f)]], 1)   # warm-up
+        f.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in flows]
+    for (e0, _), st in zip(ev, streams):
+        e0.record(st)
+    th = [threading.Thread(target=host_round_trip_steps, args=(f, [t.data_ptr() for t in pin], n))
+          for f, pin in zip(flows, pins)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    for (_, e1), st in zip(ev, streams):
+        e1.record(st)
+    for _, e1 in ev:
+        e1.synchronize()
+    ms = max(ev[0][0].elapsed_time(e1) for _, e1 in ev)
+    nbytes = sum(t.numel() * 8 for t in pins[0])
+    for f in flows:
+        f.close()
+    return ms, nbytes
+
+
+def error_vs_fp64(cf, nx, ny, nz, dev, steps):
+    """Relative L2 difference of the mixed-precision velocity (data1) from
+    the FP64 path's after `steps` steps from the same seeded initial field:
+    over the whole field and over its perturbation (every Fourier column
+    except the kx = kz = 0 mean), with the change of the FP64 field over the
+    run beside them."""
+    a = make_flow(cf, nx, ny, nz, cf.FP64, dev)
+    b = make_flow(cf, nx, ny, nz, cf.MIXED, dev)
+    d0 = a.download_state()[0]
+    a.timestep(steps)
+    b.timestep(steps)
+    da, db = a.download_state()[0], b.download_state()[0]
+    st = (a.status(), b.status())
+    a.close()
+    b.close()
+
+    def rel(x, y):
+        return float(np.linalg.norm(x - y) / np.linalg.norm(y))
+
+    pa, pb, p0 = da.copy(), db.copy(), d0.copy()
+    for arr in (pa, pb, p0):
+        arr[0, 0] = 0
+    return {"steps": steps, "whole_field": rel(db, da), "perturbation": rel(pb, pa),
+            "fp64_change_whole": rel(da, d0), "fp64_change_perturbation": rel(pa, p0), "status": list(st),
+            "field": "data1 (u, v, w), relative L2; perturbation = all columns but kx = kz = 0"}
+
+
 def run_ours(args):
     import torch
     import __graft_entry__
@@ -483,30 +569,38 @@ def run_ours(args):
             # uploads data1/data2/data4 from pinned host memory, advances one
             # step and downloads data1/data2/data4 (a host-owned state).
             ke = max(1, min(K, args.e2e_steps))
-            s1, s2, s4 = flow.shapes()
-            pin = [torch.empty(int(np.prod(s)) * 2, dtype=torch.float64, pin_memory=True) for s in (s1, s2, s4)]
-            d1, d2, d4 = flow.download_state()
-            for t, a in zip(pin, (d1, d2, d4)):
-                t.numpy()[:] = np.asfortranarray(a).ravel(order="F").view(np.float64)
+            pin = pinned_state(torch, flow)
             ptr = [t.data_ptr() for t in pin]
-            L = flow.L
             stream = torch.cuda.ExternalStream(flow.stream_ptr())
             barrier()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            for _ in range(ke):
-                flow._chk(L.cfg_upload_state(flow.h, ptr[0], ptr[1], ptr[2]))
-                flow.timestep(1)
-                flow._chk(L.cfg_download_state(flow.h, ptr[0], ptr[1], ptr[2]))
+            host_round_trip_steps(flow, ptr, ke)
             e1.record(stream)
             e1.synchronize()
             e2e_ms = max_over_ranks(e0.elapsed_time(e1))
             nbytes = sum(t.numel() * 8 for t in pin)
             results["e2e"] = {"value": throughput(world, units, ke, e2e_ms), "unit": UNIT,
-                              "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes}
+                              "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+                              "how": "serial: every step uploads data1/data2/data4 from pinned host memory, "
+                                     "steps once and downloads them (a host-owned state)"}
+            del pin
         flow.close()
         torch.cuda.synchronize()
+
+    # the same e2e with two domains whose host round trips overlap (two host
+    # threads); every rank does the same
+    ke = max(1, min(K, args.e2e_steps))
+    ms_ov, nb_ov = e2e_overlapped(torch, cf, nx, ny, nz, dev, ke)
+    ms_ov = max_over_ranks(ms_ov)
+    results["e2e_overlapped"] = {
+        "value": throughput(world, 2 * units, ke, ms_ov), "unit": UNIT,
+        "h2d_bytes_per_step": nb_ov, "d2h_bytes_per_step": nb_ov,
+        "how": "two independent domains per GPU, one host thread each, every domain step uploads, steps and "
+               "downloads its state as in the serial e2e; copies of one overlap the other's step"}
+    # mixed against FP64 on the workload (outside every timed region)
+    err = error_vs_fp64(cf, nx, ny, nz, dev, args.error_steps) if args.error_steps > 0 else None
 
     # CPU baseline on rank 0 at N = 1
     cpu = None
@@ -580,6 +674,8 @@ def run_ours(args):
                               "algorithmic_bytes": step_bytes},
             "kernels": kernels,
             "e2e": results.get("e2e"),
+            "e2e_overlapped": results.get("e2e_overlapped"),
+            "error_vs_fp64": err,
             "gpu_launches": int(mix["launches"]),
             "clocks": mix["clocks"],
             "cpu_baseline": cpu,
@@ -608,6 +704,8 @@ def main():
     ap.add_argument("--nz", type=int, default=NZ)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--error-steps", type=int, default=100,
+                    help="steps of the mixed-vs-FP64 error check outside the timed region (0: skip)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--slab", type=int, default=0, help="one field in P slab ranks (one process)")
     ap.add_argument("--ensemble", type=int, default=0, help="configuration C5 with M members (one GPU)")

@@ -397,9 +397,12 @@ void cfg_ensemble_destroy(cfg_ensemble *e);
  * device array of 4.06 MiB that every GPU loading the library holds until
  * exit.  Limits: (nx/2+1)*nz2 <= 262144 and nx2, nz2 <= 2048 (2^a 3^b, even);
  * larger planes return CFG_E_SIZE.  Every call shares that array and it keeps
- * the previous call's contents (each call rewrites all it reads, nothing must
- * start at zero), so calls whose executions overlap on the GPU -- other
- * streams, other host threads -- race; serialise them.  The first call on a
+ * the previous call's contents: each call rewrites the intermediate plane it
+ * reads (nothing must start at zero), and the twiddle tables are rewritten
+ * only when nx2 or nz2 differs from the previous call's on that device.  So
+ * calls whose executions overlap on the GPU -- other streams, other host
+ * threads -- race; serialise them.  The kernels' shared-memory limits are
+ * only ever raised, never lowered.  The first call on a
  * device performs a one-time set-up (it looks up the array's device address
  * with that device current); make that first call before any stream capture.
  * Returns CFG_OK, CFG_E_ARG, CFG_E_SIZE or CFG_E_CUDA. */

@@ -64,6 +64,31 @@ int cfh_define_grid(cfh_grid *g, double lx, double lz, double stretch, int unifo
 int cfh_initial_field(const cfh_grid *g, int which_test, unsigned long long seed,
                       double ampl, double beta, double *data1);
 
+/* The Orr-Sommerfeld initial fields, which_test 2, 5 and 8
+ * (PFC/init_vel.f90:95-159).
+ *
+ * cfh_read_efn: efn.m as READ_EIGENFUNCTION reads it (PFC/init_vel.f90:565-572):
+ * 4 x 65 numbers, one per line, column after column -- Re u, Im u, Re v, Im v
+ * at the Chebyshev-Gauss-Lobatto points y_j = cos(pi j / 64), j = 0..64 --
+ * into uin (65, 4) column-major.  Fortran D exponents are accepted.  Returns
+ * 0, -1 when the file cannot be opened, -2 when it is short or malformed.
+ *
+ * cfh_interp_eigenfunction: the rest of READ_EIGENFUNCTION (:583-633): the
+ * Chebyshev coefficients of the four columns, u summed onto yh(2..ny) with
+ * u(1) = u(ny+1) = 0, v onto y(1..ny) with v(ny+1) = 0.  u, v: (ny+1)
+ * complex, interleaved.
+ *
+ * cfh_initial_field_mode: the which_test 2 / 5 / 8 velocity before the
+ * divergence removal: the laminar profile plus ampl times the mode in
+ * Fourier column (kz 1, kx 2) for 2, (kz 2 and its conjugate kz nz, kx 1)
+ * for 5 and (kz 2, kx 2) for 8, rotated by beta as the reference does.
+ * data1 (nz, nx/2+1, ny+1, 3) complex interleaved.  Returns -1 for another
+ * which_test. */
+int cfh_read_efn(const char *path, double *uin);
+int cfh_interp_eigenfunction(const cfh_grid *g, const double *uin, double *u, double *v);
+int cfh_initial_field_mode(const cfh_grid *g, int which_test, double ampl, double beta,
+                           const double *u, const double *v, double *data1);
+
 /* read_write::save_velocity / read_velocity (PFC/read_write.f90:21-292) on
  * host arrays in data1 layout (nz, nx/2+1, ny+1, 3): the reference's restart
  * file, Fortran unformatted sequential (4-byte record markers, native byte

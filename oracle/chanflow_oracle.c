@@ -1098,6 +1098,21 @@ void orc_init_field(orc_ctx *c, int which_test, unsigned long long seed, double 
   orc_compute_initial_pressure(c, 0);
 }
 
+/* define_initial_field after its which_test branch (PFC/init_vel.f90:325-351)
+ * for a velocity the caller wrote into data1 (the Orr-Sommerfeld modes of
+ * which_test 2, 5, 8): t = 0, data2 and data4 cleared, divergence removed,
+ * d_um_dy, data2 = data1, initial pressure. */
+void orc_init_from_velocity(orc_ctx *c) {
+  size_t nf = (size_t)c->p.nz * c->nxh * (c->p.ny + 1);
+  c->t_total = 0;
+  memset(c->data2, 0, sizeof(cplx) * 3 * nf);
+  memset(c->data4, 0, sizeof(cplx) * nf);
+  orc_remove_initial_divergence(c);
+  orc_compute_d_um_dy(c);
+  copy_data1_to_data2(c);
+  orc_compute_initial_pressure(c, 0);
+}
+
 /* the which_test velocity before divergence removal, PFC/init_vel.f90:88-244 */
 void orc_initial_velocity(orc_ctx *c, int which_test, unsigned long long seed, double ampl) {
   int ny = c->p.ny, n1 = ny + 1, nz = c->p.nz, nxh = c->nxh;

@@ -89,6 +89,7 @@ void orc_initial_velocity(orc_ctx *c, int which_test, unsigned long long seed,
                           double ampl);
 double orc_rng_u01(unsigned long long seed, int x, int z, int j, int col);
 void orc_remove_initial_divergence(orc_ctx *c);
+void orc_init_from_velocity(orc_ctx *c);   /* PFC/init_vel.f90:325-351 on a caller-set data1 */
 void orc_compute_d_um_dy(orc_ctx *c);
 void orc_compute_initial_pressure(orc_ctx *c, int linearized);
 void orc_strip_divergence_column(orc_ctx *c, double complex *cu /*(ny+1,3)*/,

@@ -77,7 +77,7 @@ def lib():
             getattr(L, n).argtypes = [vp, vp, vp]
         L.orc_div_fluxes.argtypes = [vp, vp, vp, vp, vp]
         for n in ("orc_nonlinear", "orc_nonlinear_linearized", "orc_rhs_solve", "orc_boundary",
-                  "orc_remove_initial_divergence", "orc_compute_d_um_dy"):
+                  "orc_remove_initial_divergence", "orc_compute_d_um_dy", "orc_init_from_velocity"):
             getattr(L, n).argtypes = [vp]
         L.orc_l2_norm.argtypes = [vp, dp, dp]
         L.orc_init_field.argtypes = [vp, C.c_int, C.c_ulonglong, C.c_double]
@@ -261,6 +261,12 @@ class Oracle:
 
     def initial_velocity(self, which_test, seed=1, ampl=1e-3):
         self.L.orc_initial_velocity(self.h, which_test, seed, ampl)
+
+    def init_from_velocity(self, data1):
+        """define_initial_field's common tail for a given velocity (data1
+        layout): divergence removal, d_um_dy, data2 = data1, pressure."""
+        self.data1[...] = data1
+        self.L.orc_init_from_velocity(self.h)
 
     def remove_initial_divergence(self):
         self.L.orc_remove_initial_divergence(self.h)

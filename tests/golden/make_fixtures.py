@@ -1,5 +1,8 @@
 """Regenerates the golden fixtures under tests/golden/ from the reference
-project's shipped data (run in a container where the reference is mounted).
+project's shipped data.  The reference checkout's root is the first argument
+or the REFERENCE_ROOT environment variable:
+
+    python tests/golden/make_fixtures.py <reference checkout>
 
 makegrid_ny200.json: y(200), yh(201) written by output_grids
 (PFC/setup.f90:1331-1359) for ny=200 with STRETCH=2.75, as printed in
@@ -18,11 +21,18 @@ import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
+def reference_root():
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REFERENCE_ROOT")
+    if not ref:
+        sys.exit("usage: make_fixtures.py <reference checkout> (or set REFERENCE_ROOT)")
+    return ref
+
+
 def main():
+    REF = reference_root()
     txt = open(os.path.join(REF, "ParallelFortran-Code", "makegrid.m")).read()
 
     def block(name):

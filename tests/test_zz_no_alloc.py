@@ -17,15 +17,12 @@ def rel(a, b):
     return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
 
 
-def test_noalloc_matches_cfg_xz_c2r_twice(cf):
+def _check_calls(cf, L, nx, nz, ncalls, rng):
     import torch
-    L = cf.load_library()
-    nx, ny, nz = 32, 17, 24
-    grid = cf.Grid(nx, ny, nz, lx=4 * np.pi, lz=2 * np.pi, stretch=1.5)
+    grid = cf.Grid(nx, 17, nz, lx=4 * np.pi, lz=2 * np.pi, stretch=1.5)
     flow = cf.ChannelFlow(grid, precision=cf.FP64, device=0)
     nxh, nx2, nz2 = nx // 2 + 1, grid.nx2, grid.nz2
-    rng = np.random.default_rng(2024)
-    for trial in range(2):
+    for trial in range(ncalls):
         c = (rng.standard_normal((nz, nxh)) + 1j * rng.standard_normal((nz, nxh))) * (trial + 1)
         ref = flow.xz_fft_complex_to_real(c)
         cd = torch.from_numpy(np.ascontiguousarray(c.ravel(order="F")).view(np.float64).copy()).cuda()
@@ -35,8 +32,18 @@ def test_noalloc_matches_cfg_xz_c2r_twice(cf):
         torch.cuda.synchronize()
         assert r == 0
         got = out.cpu().numpy().reshape((nx2, nz2), order="F")
-        assert rel(got, ref) < 1e-12, (trial, rel(got, ref))
+        assert rel(got, ref) < 1e-12, (nx, nz, trial, rel(got, ref))
     flow.close()
+
+
+def test_noalloc_matches_cfg_xz_c2r_twice(cf):
+    L = cf.load_library()
+    rng = np.random.default_rng(2024)
+    # two calls in a row on one plane size (the second reuses the twiddle
+    # tables the first wrote), then another size and back
+    _check_calls(cf, L, 32, 24, 2, rng)
+    _check_calls(cf, L, 48, 16, 1, rng)
+    _check_calls(cf, L, 32, 24, 1, rng)
 
 
 def test_noalloc_rejects_oversized_plane(cf):
