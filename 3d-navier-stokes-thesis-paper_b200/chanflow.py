@@ -79,6 +79,16 @@ class CfgFringe(C.Structure):
     ]
 
 
+class CfgLes(C.Structure):
+    """cfg_les (include/chanflow.h): the LES mode's subgrid model."""
+    _fields_ = [
+        ("model", C.c_int), ("cs", C.c_double), ("aplus", C.c_double), ("beta", C.c_double),
+        ("mlp", C.c_void_p),
+        ("in_shift", C.c_float * 10), ("in_scale", C.c_float * 10),
+        ("out_shift", C.c_float * 6), ("out_scale", C.c_float * 6),
+    ]
+
+
 class CfhRun(C.Structure):
     _fields_ = [
         ("re", C.c_double), ("ctrlu", C.c_double), ("ctrlw", C.c_double), ("lx", C.c_double),
@@ -151,6 +161,21 @@ SYMBOLS = {
     "cfg_launch_count": (C.c_longlong, [_VP]),
     "cfg_stream": (_VP, [_VP]),
     "cfg_xz_c2r_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _VP, _VP, _VP]),
+    "cfg_set_les": (C.c_int, [_VP, C.c_void_p]),
+    "cfg_les_features": (C.c_int, [_VP, _VP]),
+    "cfg_les_stresses": (C.c_int, [_VP, _VP]),
+    "cfg_les_fallbacks": (C.c_int, [_VP, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong)]),
+    "cfg_mlp_nparams": (C.c_int, []),
+    "cfg_mlp_create": (C.c_int, [C.c_int, C.POINTER(_VP)]),
+    "cfg_mlp_destroy": (None, [_VP]),
+    "cfg_mlp_set_params": (C.c_int, [_VP, _VP]),
+    "cfg_mlp_get_params": (C.c_int, [_VP, _VP]),
+    "cfg_mlp_forward": (C.c_int, [_VP, _VP, _VP, C.c_longlong, _VP]),
+    "cfg_mlp_accumulate_grad": (C.c_int, [_VP, _VP, _VP, _VP, C.c_int, _VP]),
+    "cfg_mlp_get_grads": (C.c_int, [_VP, _VP, _VP]),
+    "cfg_mlp_zero_grads": (C.c_int, [_VP, _VP]),
+    "cfg_mlp_adam_step": (C.c_int, [_VP, C.c_float, C.c_float, C.c_float, C.c_float, _VP]),
+    "cfg_mlp_status": (C.c_int, [_VP]),
     "cfg_profile_enable": (C.c_int, [_VP, C.c_int]),
     "cfg_profile_read": (C.c_int, [_VP, C.c_int, C.c_char_p, C.c_int, C.POINTER(C.c_int), _DP]),
     "cfg_partition": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _VP, _VP, _VP, _VP, _VP, _VP]),
@@ -519,6 +544,41 @@ class ChannelFlow:
     def wait_io(self):
         self._chk(self.L.cfg_wait_io(self.h))
 
+    def set_les(self, model, cs=0.1, aplus=25.0, beta=0.0, mlp=None, in_shift=None, in_scale=None,
+                out_shift=None, out_scale=None):
+        """LES mode: model 0 off, 1 eddy viscosity (Smagorinsky cs, van
+        Driest aplus), 2 the learned closure (an Mlp) with the eddy
+        viscosity as its per-point fallback (beta: admitted backscatter as a
+        fraction of the eddy viscosity's dissipation).  The shifts and scales
+        normalise the 10 features and map the 6 outputs back."""
+        l = CfgLes()
+        l.model, l.cs, l.aplus, l.beta = int(model), cs, aplus, beta
+        l.mlp = mlp.h.value if mlp is not None else None
+        for name, n, default in (("in_shift", 10, 0.0), ("in_scale", 10, 1.0), ("out_shift", 6, 0.0),
+                                 ("out_scale", 6, 1.0)):
+            v = locals()[name]
+            arr = getattr(l, name)
+            for i in range(n):
+                arr[i] = float(default if v is None else v[i])
+        self._les_mlp = mlp          # keep the network alive while the context uses it
+        self._chk(self.L.cfg_set_les(self.h, C.byref(l)))
+
+    def les_features(self, ptr):
+        """The closure's features of the current state into a device buffer
+        of (ny-1)*nz2*nx2*10 floats (model 2 must be set)."""
+        self._chk(self.L.cfg_les_features(self.h, ptr))
+
+    def les_stresses(self):
+        """The last subgrid stresses, (ny+1, 6, nz2, nx2) FP64."""
+        S = np.zeros((self.ny + 1, 6, self.grid.nz2, self.grid.nx2))
+        self._chk(self.L.cfg_les_stresses(self.h, S.ctypes.data))
+        return S
+
+    def les_fallbacks(self):
+        f, n = C.c_ulonglong(), C.c_ulonglong()
+        self._chk(self.L.cfg_les_fallbacks(self.h, C.byref(f), C.byref(n)))
+        return f.value, n.value
+
     def set_jet(self, jet):
         """crossflow = 1 with a CfgJet (jet_profile every substep), or None."""
         self._chk(self.L.cfg_set_jet(self.h, C.byref(jet) if jet is not None else None))
@@ -621,6 +681,118 @@ def arnoldi_eigs(flow, tend, nev=12, ncv=25, tol=1e-8, maxiter=None, v0=None):
     lam = (np.log(np.abs(mu) + np.finfo(np.float64).eps) + 1j * np.arctan2(mu.imag, mu.real)) / T
     order = np.argsort(-np.abs(mu))
     return mu[order], lam[order], vec[:, order]
+
+
+def stability_columns(nx, nz):
+    """The Fourier columns (kx index a, kz index b) of a real nx x nz field
+    that carry a free complex amplitude: 1 <= a < nx/2 with every kz but the
+    Nyquist one, and a = 0 with 1 <= b < nz/2 (its kz < 0 partners are the
+    conjugates).  Mean and Nyquist columns are left out."""
+    cols = [(a, b) for a in range(1, nx // 2) for b in range(nz) if b != nz // 2]
+    cols += [(0, b) for b in range(1, nz // 2)]
+    return np.array(cols, dtype=np.int64)
+
+
+def arnoldi_columns(flow, tend, ncv=60, nev=10, seed=3, restarts=4, keep=None, tol=1e-9):
+    """Leading eigenvalues of the propagator Phi_T (T = tend*dt) about a
+    parallel baseflow U(y), by Arnoldi run on every Fourier column at once.
+
+    The linearized operator about a profile U(y) (PFC/pass1_linearized.f90,
+    PFC/arnoldi.f90:485-567) does not couple Fourier columns, so its spectrum
+    is the union of the columns' spectra.  Each column (stability_columns)
+    gets its own Krylov basis of up to ncv vectors of (ny+1)*3 complex
+    amplitudes, Gram-Schmidt orthogonalised twice in FP64 on the host; one
+    GPU matvec (cfg_arnoldi_matvec) on the physical field that superposes all
+    columns' current vectors advances every column's iteration.  Between
+    cycles each column keeps its `keep` (default ncv/2) leading Schur vectors
+    (a Krylov-Schur restart, Stewart 2001), `restarts` cycles in all.
+    Returns (mu, lam, residual, column) for the nev eigenvalues of largest
+    modulus among the Ritz values whose Arnoldi residual estimate is below
+    tol |mu|: mu the propagator eigenvalue, lam = (log|mu| + i arg mu)/T,
+    residual the explicit ||Phi x - mu x|| / ||x|| of its Ritz vector (one
+    more matvec per Ritz rank), column its (kx index, kz index)."""
+    import scipy.linalg as sl
+    nx, nz, n1 = flow.nx, flow.nz, flow.ny + 1
+    cols = stability_columns(nx, nz)
+    ncol, n = len(cols), n1 * 3
+    ncv = min(ncv, n)
+    keep = keep or ncv // 2
+    a, b = cols[:, 0], cols[:, 1]
+    rng = np.random.default_rng(seed)
+
+    def embed(V):
+        """(ncol, n) column vectors -> real physical field (nx, nz, ny+1, 3)."""
+        Ch = np.zeros((nz, nx // 2 + 1, n), complex)
+        Ch[b, a] = V
+        k0 = a == 0
+        Ch[(-b[k0]) % nz, 0] = np.conj(V[k0])
+        X = np.fft.irfft2(Ch, s=(nz, nx), axes=(0, 1))       # (nz, nx, n)
+        return np.asfortranarray(X.transpose(1, 0, 2).reshape(nx, nz, n1, 3, order="C"))
+
+    def extract(X):
+        Xz = np.ascontiguousarray(np.asarray(X).reshape(nx, nz, n, order="C").transpose(1, 0, 2))
+        return np.fft.rfft2(Xz, axes=(0, 1))[b, a]
+
+    def apply(V):
+        return extract(flow.arnoldi_matvec(embed(V), tend))
+
+    T = tend * flow.scalars()["dt"]
+    Vb = np.zeros((ncol, ncv + 1, n), complex)
+    H = np.zeros((ncol, ncv + 1, ncv), complex)
+    v = rng.standard_normal((ncol, n)) + 1j * rng.standard_normal((ncol, n))
+    Vb[:, 0] = v / np.linalg.norm(v, axis=1, keepdims=True)
+    j0 = 0
+    for cycle in range(max(1, restarts)):
+        for j in range(j0, ncv):
+            w = apply(Vb[:, j])
+            for _ in range(2):
+                h = np.einsum("cjn,cn->cj", Vb[:, :j + 1].conj(), w)
+                w = w - np.einsum("cjn,cj->cn", Vb[:, :j + 1], h)
+                H[:, :j + 1, j] += h
+            nrm = np.linalg.norm(w, axis=1)
+            H[:, j + 1, j] = nrm
+            Vb[:, j + 1] = w / np.maximum(nrm, 1e-300)[:, None]
+        if cycle == restarts - 1:
+            break
+        # Krylov-Schur restart: the keep leading Schur vectors of each column
+        Hn = np.zeros_like(H)
+        Vn = np.zeros_like(Vb)
+        for c in range(ncol):
+            ev = np.linalg.eigvals(H[c, :ncv, :ncv])
+            thr = np.sort(np.abs(ev))[::-1][keep - 1]
+            S, Q, _ = sl.schur(H[c, :ncv, :ncv], output="complex", sort=lambda z, t=thr: abs(z) >= t * (1 - 1e-12))
+            Vn[c, :keep] = Q[:, :keep].T @ Vb[c, :ncv]
+            Hn[c, :keep, :keep] = S[:keep, :keep]
+            Hn[c, keep, :keep] = H[c, ncv, ncv - 1] * Q[ncv - 1, :keep]
+            Vn[c, keep] = Vb[c, ncv]
+        Vb, H, j0 = Vn, Hn, keep
+    theta, Y = np.linalg.eig(H[:, :ncv, :ncv])
+    # the nev largest over all columns' converged Ritz values (Arnoldi
+    # residual estimate |h_{m+1,m} y_m| below tol relative to |theta|)
+    est = np.abs(H[:, ncv, ncv - 1])[:, None] * np.abs(Y[:, ncv - 1, :])
+    mag = np.where(est <= tol * np.abs(theta), np.abs(theta), -1.0)
+    flat = np.argsort(-mag, axis=None)[:nev]
+    ci, ri = np.unravel_index(flat, theta.shape)
+    mu = theta[ci, ri]
+    X = np.einsum("kjn,kj->kn", Vb[ci, :ncv], Y[ci, :, ri])
+    res = np.zeros(nev)
+    # explicit residuals, one matvec per set of distinct columns
+    todo = list(range(nev))
+    while todo:
+        batch, seen = [], set()
+        for k in todo:
+            if ci[k] not in seen:
+                seen.add(ci[k])
+                batch.append(k)
+        V = np.zeros((ncol, n), complex)
+        for k in batch:
+            V[ci[k]] = X[k]
+        W = apply(V)
+        for k in batch:
+            res[k] = np.linalg.norm(W[ci[k]] - mu[k] * X[k]) / np.linalg.norm(X[k])
+        todo = [k for k in todo if k not in batch]
+    lam = (np.log(np.abs(mu)) + 1j * np.angle(mu)) / T
+    return mu, lam, res, cols[ci]
 
 
 PARTITION_KEYS = ("nx_proc", "x_start", "nz_proc", "z_start", "nz_small_proc", "z_small_start")
@@ -815,6 +987,71 @@ class Rank(ChannelFlow):
         if err:
             raise err[0]
         self._chk(r)
+
+
+class Mlp:
+    """The learned subgrid-stress closure network on the tensor cores
+    (cfg_mlp_*): 10 -> 64 -> 64 -> 64 -> 6, GELU, BF16 operands, FP32
+    accumulation.  Data arguments are device pointers (e.g. torch tensors'
+    data_ptr()); stream is a cudaStream_t value (None: the default stream)."""
+
+    def __init__(self, device=0, params=None):
+        self.L = load_library()
+        self.nparams = self.L.cfg_mlp_nparams()
+        h = _VP()
+        r = self.L.cfg_mlp_create(device, C.byref(h))
+        if r != 0:
+            raise ChanflowError(f"cfg_mlp_create failed ({r})")
+        self.h = h
+        if params is not None:
+            self.set_params(params)
+
+    def _chk(self, r):
+        if r != 0:
+            raise ChanflowError(f"cfg_mlp call failed ({r})")
+
+    def set_params(self, params):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        if p.size != self.nparams:
+            raise ChanflowError(f"expected {self.nparams} parameters, got {p.size}")
+        self._chk(self.L.cfg_mlp_set_params(self.h, p.ctypes.data))
+
+    def get_params(self):
+        p = np.zeros(self.nparams, np.float32)
+        self._chk(self.L.cfg_mlp_get_params(self.h, p.ctypes.data))
+        return p
+
+    def forward(self, x_ptr, y_ptr, n, stream=None):
+        self._chk(self.L.cfg_mlp_forward(self.h, x_ptr, y_ptr, int(n), stream))
+
+    def accumulate_grad(self, x_ptr, t_ptr, idx_ptr, batch, stream=None):
+        self._chk(self.L.cfg_mlp_accumulate_grad(self.h, x_ptr, t_ptr, idx_ptr, int(batch), stream))
+
+    def grads(self):
+        g = np.zeros(self.nparams, np.float32)
+        loss = C.c_float()
+        self._chk(self.L.cfg_mlp_get_grads(self.h, g.ctypes.data, C.byref(loss)))
+        return g, loss.value
+
+    def zero_grads(self, stream=None):
+        self._chk(self.L.cfg_mlp_zero_grads(self.h, stream))
+
+    def adam_step(self, lr, beta1=0.9, beta2=0.999, eps=1e-8, stream=None):
+        self._chk(self.L.cfg_mlp_adam_step(self.h, lr, beta1, beta2, eps, stream))
+
+    def status(self):
+        return self.L.cfg_mlp_status(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.cfg_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Ensemble:

@@ -28,6 +28,7 @@
 #include "arnoldi.cuh"
 #include "io.cuh"
 #include "jet.cuh"
+#include "les.cuh"
 #include "pass2v2.h"
 #include "planes.cuh"
 #include "restart.h"
@@ -226,6 +227,17 @@ struct cfg_ctx {
   unsigned long long** cfl_peers = nullptr;   // the other ranks' cflbits
   int n_cfl_peers = 0;
   std::vector<void*> ipc_open;   // other processes' buffers mapped by cfg_rank_connect
+  // LES mode (cfg_set_les): subgrid stresses S[ny+1][6][nz2][nx2] (storage
+  // precision) added by the flux kernel; the learned closure's features and
+  // outputs (FP32) and its fallback counter
+  bool les_on = false;
+  LesDev les{};
+  cfg_mlp* les_mlp = nullptr;
+  void* les_S = nullptr;
+  float* les_F = nullptr;
+  float* les_Y = nullptr;
+  unsigned long long* les_nfall = nullptr;
+  unsigned long long les_points = 0;
 };
 
 // slab of one rank (cfg_group_create); one rank: the whole grid
@@ -489,6 +501,11 @@ struct Impl {
         prof_begin(c, "k_xinv");
         if (p1_fast_launch(3, g.nx2, f32, a) != 0) return fail(c, CFG_E_CUDA, "k_xinv_r launch");
         CKL();
+        if (c->les_on && !lin) {
+          const int r = les_stresses(c, c->les_F);
+          if (r) return r;
+          a.sgs = c->les_S;
+        }
         prof_begin(c, "k_flux");
         if (p1_fast_launch(4, g.nx2, f32, a) != 0) return fail(c, CFG_E_CUDA, "k_flux_r launch");
       } else if (c->fast_x) {
@@ -531,6 +548,44 @@ struct Impl {
       CKL();
     }
     return CFG_OK;
+  }
+
+  // the LES mode's subgrid stresses from the physical planes P (after
+  // k_xinv_r): eddy viscosity, and for model 2 the network and the checks
+  static int les_stresses(cfg_ctx* c, float* F) {
+    const Geom& g = c->g;
+    dim3 gr((g.nx2 + 127) / 128, g.nz2, g.ny - 1);
+    prof_begin(c, "k_les_sgs");
+    k_les_sgs<T><<<gr, 128, 0, c->st>>>((const T*)c->P, (T*)c->les_S, F, g, c->gd, c->les, c->d_um_dy);
+    CKL();
+    if (c->les.model == 2 && F == c->les_F) {
+      prof_begin(c, "k_mlp_fwd");
+      if (cfg_mlp_forward(c->les_mlp, c->les_F, c->les_Y, (long long)c->les_points, c->st) != CFG_OK)
+        return fail(c, CFG_E_CUDA, "closure network launch");
+      c->launches++;
+      prof_begin(c, "k_les_blend");
+      k_les_blend<T><<<gr, 128, 0, c->st>>>((const T*)c->P, (T*)c->les_S, c->les_Y, g, c->gd, c->les, c->d_um_dy,
+                                            c->les_nfall);
+      CKL();
+    }
+    return CFG_OK;
+  }
+
+  // the closure's input features of the current state into F (device):
+  // the inverse transforms and the feature kernel, without a step
+  static int les_features(cfg_ctx* c, float* F) {
+    const Geom& g = c->g;
+    const bool f32 = sizeof(T) == 4;
+    P1Launch a{};
+    a.vel = c->vel; a.T1 = c->T1; a.g = g; a.twx = c->twx; a.twz = c->twz; a.gd = c->gd; a.YB1 = c->fYB1;
+    a.st = c->st; a.P = c->P; a.FZR = c->flux_zr; a.sc = c->scat;
+    if (p1_fast_launch(0, g.nz2, f32, a) != 0) return fail(c, CFG_E_CUDA, "k_zinv_r launch");
+    c->launches++;
+    a.g = c->gP;
+    a.gd = c->gd_all;
+    if (p1_fast_launch(3, g.nx2, f32, a) != 0) return fail(c, CFG_E_CUDA, "k_xinv_r launch");
+    c->launches++;
+    return les_stresses(c, F);
   }
 
   template <int MM>
@@ -1012,7 +1067,8 @@ void cfg_destroy(cfg_ctx* c) {
   void* bufs[] = {c->dgrid, c->fringe, c->vel, c->cru, c->prs, c->mvel64, c->mcru64, c->T1, c->T2, c->P, c->rhs2_tbl, c->rhs2_tbl64, c->jst, c->pp_wy, c->pp_sy, c->pp_acc, c->cbc,
                   c->sc, c->d_um_dy, c->cflp, c->cflbits, c->l2acc, c->divbits, c->plist, c->pw_H,
                   c->pw_phys, c->pw_phys2, c->pw_in, c->stage, c->twx, c->twz, c->twxs, c->twzs,
-                  c->wl_fast, c->wl_prec, c->scat_tab, c->cfl_peers};
+                  c->wl_fast, c->wl_prec, c->scat_tab, c->cfl_peers, c->les_S, c->les_F, c->les_Y,
+                  c->les_nfall};
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
@@ -1381,6 +1437,97 @@ int cfg_small_c2r(cfg_ctx* c, const double* cdata, double* data, int nplanes) {
   CKL();
   CK(cudaMemcpyAsync(data, c->stage, sizeof(double) * nout, cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
+  return CFG_OK;
+}
+
+int cfg_set_les(cfg_ctx* c, const cfg_les* l) {
+  if (!c) return CFG_E_ARG;
+  if (c->nranks > 1) return single_only(c, "cfg_set_les");
+  cudaSetDevice(c->dev);
+  if (!l || l->model == 0) {
+    c->les_on = false;
+    return CFG_OK;
+  }
+  if (l->model != 1 && l->model != 2) return fail(c, CFG_E_ARG, "cfg_set_les: model %d", l->model);
+  if (!c->split_x) return fail(c, CFG_E_ARG, "cfg_set_les: needs the register-FFT x stage (nx2 of 24 .. 576)");
+  if (l->model == 2 && !l->mlp) return fail(c, CFG_E_ARG, "cfg_set_les: model 2 needs the network");
+  if (!(l->cs >= 0.0) || !(l->aplus > 0.0) || !(l->beta >= 0.0)) return fail(c, CFG_E_ARG, "cfg_set_les: cs, aplus, beta");
+  for (int i = 0; i < 10; ++i)
+    if (!(l->in_scale[i] != 0.0f) && l->model == 2) return fail(c, CFG_E_ARG, "cfg_set_les: in_scale[%d] = 0", i);
+  const Geom& g = c->g;
+  const size_t cs = (size_t)g.nz2 * g.nx2;
+  const size_t tsz = c->mixed ? sizeof(float) : sizeof(double);
+  c->les_points = (unsigned long long)(g.ny - 1) * cs;
+  if (!c->les_S) {
+    if (cudaMalloc(&c->les_S, tsz * 6 * cs * g.ny1) != cudaSuccess || cudaMalloc(&c->les_nfall, 8) != cudaSuccess)
+      return fail(c, CFG_E_NOMEM, "LES stresses");
+    CK(cudaMemsetAsync(c->les_S, 0, tsz * 6 * cs * g.ny1, c->st));   // wall planes stay zero
+  }
+  if (l->model == 2 && !c->les_F) {
+    if (cudaMalloc(&c->les_F, sizeof(float) * 10 * c->les_points) != cudaSuccess ||
+        cudaMalloc(&c->les_Y, sizeof(float) * 6 * c->les_points) != cudaSuccess)
+      return fail(c, CFG_E_NOMEM, "LES closure buffers");
+  }
+  CK(cudaMemsetAsync(c->les_nfall, 0, 8, c->st));
+  LesDev& d = c->les;
+  d.model = l->model;
+  d.cs = l->cs;
+  d.aplus = l->aplus;
+  d.beta = l->beta;
+  d.dx = c->p.lx / g.nx;
+  d.dz = c->p.lz / g.nz;
+  d.hx = c->p.lx / g.nx2;
+  d.hz = c->p.lz / g.nz2;
+  d.re = c->p.re;
+  for (int i = 0; i < 10; ++i) {
+    d.in_shift[i] = l->in_shift[i];
+    d.in_scale[i] = l->model == 2 ? l->in_scale[i] : 1.0f;
+  }
+  for (int i = 0; i < 6; ++i) {
+    d.out_shift[i] = l->out_shift[i];
+    d.out_scale[i] = l->out_scale[i];
+  }
+  c->les_mlp = l->mlp;
+  CK(cudaStreamSynchronize(c->st));
+  c->les_on = true;
+  return CFG_OK;
+}
+
+int cfg_les_features(cfg_ctx* c, float* features) {
+  if (!c || !features) return CFG_E_ARG;
+  if (!c->les_on || c->les.model != 2) return fail(c, CFG_E_STATE, "cfg_les_features: set the LES model 2 first");
+  cudaSetDevice(c->dev);
+  return DISPATCH(c, les_features(c, features));
+}
+
+int cfg_les_stresses(cfg_ctx* c, double* S) {
+  if (!c || !S) return CFG_E_ARG;
+  if (!c->les_S) return fail(c, CFG_E_STATE, "cfg_les_stresses: no LES model set");
+  cudaSetDevice(c->dev);
+  const Geom& g = c->g;
+  const size_t n = (size_t)g.ny1 * 6 * g.nz2 * g.nx2;
+  if (c->mixed) {
+    std::vector<float> h(n);
+    CK(cudaMemcpyAsync(h.data(), c->les_S, n * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    for (size_t i = 0; i < n; ++i) S[i] = h[i];
+  } else {
+    CK(cudaMemcpyAsync(S, c->les_S, n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+  }
+  return CFG_OK;
+}
+
+int cfg_les_fallbacks(cfg_ctx* c, unsigned long long* fallbacks, unsigned long long* points) {
+  if (!c) return CFG_E_ARG;
+  cudaSetDevice(c->dev);
+  unsigned long long h = 0;
+  if (c->les_nfall) {
+    CK(cudaMemcpyAsync(&h, c->les_nfall, 8, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+  }
+  if (fallbacks) *fallbacks = h;
+  if (points) *points = c->les_points;
   return CFG_OK;
 }
 

@@ -25,6 +25,7 @@ struct P1Launch {
   void* P;              // physical planes (split x stage)
   int FZR;              // z rows per k_flux_r block (2 or 4)
   Scatter sc;           // transposes of a multi-rank run (n == 0: one rank)
+  const void* sgs;      // LES subgrid stresses [ny+1][6][nz2][nx2] for k_flux_r, or null
   cudaStream_t st;
 };
 

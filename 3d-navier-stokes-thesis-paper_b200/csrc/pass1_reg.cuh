@@ -624,11 +624,19 @@ __global__ void __launch_bounds__(256) k_xinv_r(const cplx_t<T>* __restrict__ T1
 // on ZR rows of z from the physical planes k-1, k, k+1, then the forward x
 // transform and the Hermitian unpacking into T2 -- the same arithmetic and
 // output as k_xflux_r (PFC/pass1.f90:134-226, PFC/transform.f90:287-315).
-template <typename T, int NX2, int ZR, int NT, bool LIN>
+// MODE 0: the nonlinear products; 1: the linearized products about the
+// baseflow (PFC/pass1_linearized.f90:135-509); 2: the nonlinear products plus
+// the subgrid stresses of the LES mode, S[pl][6][nz2][nx2] on the yh planes
+// (components 11, 22, 33, 12, 13, 23; zero on the walls), added to the
+// momentum fluxes at the same points (y-plane values interpolated as the
+// velocities are: half sums for the u and w equations, iu for the v one).
+template <typename T, int NX2, int ZR, int NT, int MODE>
 __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT == 256 ? 1 : 3)) k_flux_r(const T* __restrict__ P, cplx_t<T>* __restrict__ T2, Geom g,
                                                const cplx_t<T>* __restrict__ twx, GridDev gd,
                                                const T* __restrict__ fringe, int has_fringe,
-                                               unsigned long long* __restrict__ cflbits, int do_cfl, Scatter sc) {
+                                               unsigned long long* __restrict__ cflbits, int do_cfl, Scatter sc,
+                                               const T* __restrict__ S) {
+  constexpr bool LIN = MODE == 1, SGS = MODE == 2;
   using C = cplx_t<T>;
   constexpr int N1 = Split<NX2>::N1, N2 = Split<NX2>::N2, PITCH = N2 + 1, SEQ = SeqPitch<NX2>::V;
   constexpr int N = NX2;
@@ -672,8 +680,10 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT
   const T* Pp = P0 + pstride;
   const size_t cs = (size_t)NZ2 * N;
   T ma = 0, mb = 0, mc = 0;
-  // fluxes of one point (r, x) into the packed sequences
-  auto point = [&](T U, T V, T W, T Up, T Vp, T Wp, T Um, T Vm, T Wm, T fr, int r, int x) {
+  // fluxes of one point (r, x) into the packed sequences; tau: the subgrid
+  // stresses of the point (SGS mode): 11, 22, 33, 12, 13, 23 at yh plane k,
+  // then 12, 23 at plane k-1 and 12, 22, 23 at plane k+1
+  auto point = [&](T U, T V, T W, T Up, T Vp, T Wp, T Um, T Vm, T Wm, T fr, int r, int x, const T* tau) {
   T fpu0, fpw0, fpu, fpw, xfu, zfu, xfw, zfw;
   if (!LIN) {
     if (k == 2) { fpu0 = Vm * Um; fpw0 = Vm * Wm; }
@@ -681,6 +691,12 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT
     if (k < ny) { fpu = V * half * (U + Up); fpw = V * half * (W + Wp); }
     else { fpu = V * Up; fpw = V * Wp; }
     xfu = U * U; zfu = W * U; xfw = U * W; zfw = W * W;
+    if (SGS) {
+      xfu += tau[0]; zfu += tau[4]; xfw += tau[4]; zfw += tau[2];
+      // y-plane k-1 (zero on the bottom wall) and y-plane k (zero on the top one)
+      if (k > 2) { fpu0 += half * (tau[6] + tau[3]); fpw0 += half * (tau[7] + tau[5]); }
+      if (k < ny) { fpu += half * (tau[3] + tau[8]); fpw += half * (tau[5] + tau[10]); }
+    }
   } else {
     if (k == 2) { fpu0 = Bm[1] * Um + Vm * Bm[0]; fpw0 = Bm[1] * Wm + Vm * Bm[2]; }
     else {
@@ -707,6 +723,12 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT
       fp0 = t0 * t0; fp = t1 * t1;
       xfv = V * (iu1 * U + iu2 * Up);
       zfv = V * (iu1 * W + iu2 * Wp);
+      if (SGS) {
+        xfv += iu1 * tau[3] + iu2 * tau[8];
+        zfv += iu1 * tau[5] + iu2 * tau[10];
+        fp0 += tau[1];
+        fp += tau[9];
+      }
     } else {
       const T t0 = half * (Vm + V), b0v = half * (Bm[1] + B0[1]);
       const T t1 = half * (V + Vp), b1v = half * (B0[1] + Bp[1]);
@@ -747,8 +769,22 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT
     V2 fr;
     if (has_fringe) fr = __ldg(reinterpret_cast<const V2*>(fringe + (size_t)(z0 + r) * N + x));
     else { fr.x = (T)0; fr.y = (T)0; }
-    point(U.x, V.x, W.x, Up.x, Vp.x, Wp.x, Um.x, Vm.x, Wm.x, fr.x, r, x);
-    point(U.y, V.y, W.y, Up.y, Vp.y, Wp.y, Um.y, Vm.y, Wm.y, fr.y, r, x + 1);
+    T ta[11], tb[11];
+    if (SGS) {
+      // S planes k-1, k, k+1 are S indices k-2, k-1, k (six components each)
+      const size_t ss = (size_t)6 * NZ2 * N, so = (size_t)(k - 1) * ss + (size_t)(z0 + r) * N + x;
+      const int c0[11] = {0, 1, 2, 3, 4, 5, 3, 5, 3, 1, 5};
+      const int pd[11] = {0, 0, 0, 0, 0, 0, -1, -1, 1, 1, 1};
+#pragma unroll
+      for (int q = 0; q < 11; ++q) {
+        const V2 v = __ldg(reinterpret_cast<const V2*>(S + (size_t)((long long)so + (long long)pd[q] * (long long)ss) +
+                                                       (size_t)c0[q] * NZ2 * N));
+        ta[q] = v.x;
+        tb[q] = v.y;
+      }
+    }
+    point(U.x, V.x, W.x, Up.x, Vp.x, Wp.x, Um.x, Vm.x, Wm.x, fr.x, r, x, ta);
+    point(U.y, V.y, W.y, Up.y, Vp.y, Wp.y, Um.y, Vm.y, Wm.y, fr.y, r, x + 1, tb);
   }
   if (do_cfl) {
 #pragma unroll

@@ -397,15 +397,18 @@ def run_ensemble(args):
 
 
 def run_arnoldi(args):
+    """Configuration C3: 10 leading eigenvalues of the T = 1 propagator about
+    laminar Poiseuille flow at Re 2900 on 64x65x64, Krylov dimension 60 per
+    Fourier column (chanflow.arnoldi_columns: the linearized operator does
+    not couple columns; one GPU matvec advances every column's Arnoldi),
+    FP64 and mixed precision, with explicit residuals and their agreement."""
     import __graft_entry__
     cf = __graft_entry__.load_package()
-    from chanflow_b200.chanflow import arnoldi_eigs
+    from chanflow_b200.chanflow import arnoldi_columns
     nx, ny, nz, tend = 64, 65, 64, 100
     grid = cf.Grid(nx, ny, nz, lx=4 * np.pi, lz=2 * np.pi, stretch=STRETCH)
-    n = nx * nz * (ny + 1) * 3
-    v0 = np.random.default_rng(3).standard_normal(n)
     out = {}
-    for name, prec, tol in (("fp64", cf.FP64, 1e-8), ("mixed", cf.MIXED, 1e-6)):
+    for name, prec, tol in (("fp64", cf.FP64, 1e-9), ("mixed", cf.MIXED, 1e-5)):
         f = cf.ChannelFlow(grid, re=2900.0, dt=0.01, fix_mass=0, precision=prec)
         base = np.zeros((ny + 1, 3), order="F")
         base[:, 0] = 1 - grid.yh ** 2
@@ -419,111 +422,46 @@ def run_arnoldi(args):
 
         f.arnoldi_matvec = counted
         t0 = time.perf_counter()
-        try:
-            mu, lam, _ = arnoldi_eigs(f, tend, nev=10, ncv=60, tol=tol, v0=v0, maxiter=args.arnoldi_maxiter)
-            ok = True
-        except Exception as e:  # no convergence within maxiter: report what converged
-            ok = False
-            out[name + "_error"] = type(e).__name__
-            mu = np.asarray(getattr(e, "eigenvalues", np.array([])))
-            mu = mu[np.argsort(-np.abs(mu))] if mu.size else mu
-            T = tend * 0.01
-            lam = (np.log(np.abs(mu) + np.finfo(np.float64).eps) + 1j * np.arctan2(mu.imag, mu.real)) / T
-        out[name] = {"converged": ok, "matvecs": calls[0], "s": time.perf_counter() - t0,
+        mu, lam, res, cols = arnoldi_columns(f, tend, ncv=60, nev=10, restarts=args.arnoldi_maxiter, tol=tol)
+        out[name] = {"matvecs": calls[0], "s": time.perf_counter() - t0,
                      "mu": [[float(z.real), float(z.imag)] for z in mu],
-                     "lambda": [[float(z.real), float(z.imag)] for z in lam]}
+                     "lambda": [[float(z.real), float(z.imag)] for z in lam],
+                     "residual": [float(r) for r in res], "column_kx_kz": cols.tolist()}
         f.close()
-    if out["fp64"]["mu"] and out["mixed"]["mu"]:
-        a = np.array([complex(*z) for z in out["fp64"]["mu"]])
-        b = np.array([complex(*z) for z in out["mixed"]["mu"]])
-        out["leading_rel_diff"] = float(abs(b[0] - a[0]) / abs(a[0]))
-        out["max_rel_diff_nearest"] = float(max(np.abs(b - m).min() / abs(m) for m in a))
+    a = np.array([complex(*z) for z in out["fp64"]["mu"]])
+    b = np.array([complex(*z) for z in out["mixed"]["mu"]])
+    out["max_rel_diff_mixed_fp64"] = float(max(np.abs(b - m).min() / abs(m) for m in a))
+    out["fp64_max_residual"] = float(max(out["fp64"]["residual"]))
     line = {"metric": "Arnoldi eigenvalues (C3)", "config": {"workload": "linearized channel about Poiseuille, "
-            "Re 2900, 64x65x64, T = 1 (100 steps of dt 0.01), Krylov 60, nev 10, seeded start vector"},
+            "Re 2900, 64x65x64, T = 1 (100 steps of dt 0.01), Krylov 60 per Fourier column, nev 10, "
+            "seeded start vectors; mean and Nyquist columns excluded"},
             "n_gpus": 1, "data": "synthetic (seeded)", "result": out}
     print(json.dumps(line), flush=True)
     return 0
 
 
-def pinned_state(torch, flow):
-    """Pinned host copies of the flow's data1, data2, data4 (reference
-    layouts, interleaved complex FP64) filled with its current state."""
-    s1, s2, s4 = flow.shapes()
-    pin = [torch.empty(int(np.prod(s)) * 2, dtype=torch.float64, pin_memory=True) for s in (s1, s2, s4)]
-    d1, d2, d4 = flow.download_state()
-    for t, a in zip(pin, (d1, d2, d4)):
-        t.numpy()[:] = np.asfortranarray(a).ravel(order="F").view(np.float64)
-    return pin
-
-
-def host_round_trip_steps(flow, ptr, n):
-    """n steps of a host-owned state through the C ABI: upload data1, data2,
-    data4 from pinned host memory, one time step, download them again."""
-    L = flow.L
-    for _ in range(n):
-        flow._chk(L.cfg_upload_state(flow.h, ptr[0], ptr[1], ptr[2]))
-        flow.timestep(1)
-        flow._chk(L.cfg_download_state(flow.h, ptr[0], ptr[1], ptr[2]))
-
-
-def e2e_overlapped(torch, cf, nx, ny, nz, dev, n):
-    """Two independent domains, each driven by its own host thread through
-    the same host round trip per step as the serial e2e: one domain's uploads
-    and downloads overlap the other's step and its copies in the other
-    direction (the C calls release the interpreter lock).  Device time from
-    events on both streams, first start to last end."""
-    import threading
-    flows = [make_flow(cf, nx, ny, nz, cf.MIXED, dev) for _ in range(2)]
-    pins = [pinned_state(torch, f) for f in flows]
-    streams = [torch.cuda.ExternalStream(f.stream_ptr()) for f in flows]
-    for f in flows:
-        host_round_trip_steps(f, [t.data_ptr() for t in pins[flows.index(f)]], 1)   # warm-up
-        f.synchronize()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in flows]
-    for (e0, _), st in zip(ev, streams):
-        e0.record(st)
-    th = [threading.Thread(target=host_round_trip_steps, args=(f, [t.data_ptr() for t in pin], n))
-          for f, pin in zip(flows, pins)]
-    for t in th:
-        t.start()
-    for t in th:
-        t.join()
-    for (_, e1), st in zip(ev, streams):
-        e1.record(st)
-    for _, e1 in ev:
-        e1.synchronize()
-    ms = max(ev[0][0].elapsed_time(e1) for _, e1 in ev)
-    nbytes = sum(t.numel() * 8 for t in pins[0])
-    for f in flows:
-        f.close()
-    return ms, nbytes
-
-
-def error_vs_fp64(cf, nx, ny, nz, dev, steps):
-    """Relative L2 difference of the mixed-precision velocity (data1) from
-    the FP64 path's after `steps` steps from the same seeded initial field:
-    over the whole field and over its perturbation (every Fourier column
-    except the kx = kz = 0 mean), with the change of the FP64 field over the
-    run beside them."""
-    a = make_flow(cf, nx, ny, nz, cf.FP64, dev)
-    b = make_flow(cf, nx, ny, nz, cf.MIXED, dev)
-    d0 = a.download_state()[0]
-    a.timestep(steps)
-    b.timestep(steps)
-    da, db = a.download_state()[0], b.download_state()[0]
-    st = (a.status(), b.status())
-    a.close()
-    b.close()
-
-    def rel(x, y):
-        return float(np.linalg.norm(x - y) / np.linalg.norm(y))
-
-    pa, pb, p0 = da.copy(), db.copy(), d0.copy()
-    for arr in (pa, pb, p0):
-        arr[0, 0] = 0
-    return {"steps": steps, "whole_field": rel(db, da), "perturbation": rel(pb, pa),
-            "fp64_change_whole": rel(da, d0), "fp64_change_perturbation": rel(pa, p0), "status": list(st),
-            "field": "data1 (u, v, w), relative L2; perturbation = all columns but kx = kz = 0"}
+def run_les(args):
+    """Configuration C4: the learned-closure LES against plain GPU DNS."""
+    import importlib
+    import __graft_entry__
+    __graft_entry__.load_package()
+    lc = importlib.import_module("chanflow_b200.les_closure")
+    t0 = time.time()
+    out = lc.run_c4(nx=args.les_nx, ny=args.les_ny, nz=args.les_nx, re=args.les_re, spinup=args.les_spinup,
+                    nsnap=args.les_nsnap, train_iters=args.les_train_iters, les_spin=args.les_time / 2,
+                    les_avg=args.les_time / 2, log=lambda m: print(m, file=sys.stderr, flush=True))
+    learned = out["les"]["learned"]
+    line = {"metric": "NN-LES speedup at equal U+ error (C4)",
+            "value": out["speedup_per_time_unit"]["learned"], "unit": "x (DNS ms per time unit / LES ms per time unit)",
+            "higher_is_better": True, "n_gpus": 1, "dtype": "f32 solver, bf16 network (f32 accumulation)",
+            "data": "synthetic: this solver's DNS from seeded noise, box-filtered", "vs_baseline": None,
+            "config": {"workload": f"LES {args.les_nx // 3}x{(args.les_ny - 1) // 3 + 1}x{args.les_nx // 3} with the "
+                                   f"learned closure vs DNS {args.les_nx}x{args.les_ny}x{args.les_nx}, Re {args.les_re:g}, "
+                                   "filter 3x in x, z"},
+            "mean_profile_max_rel_err": learned.get("mean_profile_max_rel_err"), "result": out,
+            "wall_s": time.time() - t0}
+    print(json.dumps(line), flush=True)
+    return 0
 
 
 def run_ours(args):
@@ -710,7 +648,15 @@ def main():
     ap.add_argument("--slab", type=int, default=0, help="one field in P slab ranks (one process)")
     ap.add_argument("--ensemble", type=int, default=0, help="configuration C5 with M members (one GPU)")
     ap.add_argument("--arnoldi", action="store_true", help="configuration C3 (Arnoldi eigenvalues)")
-    ap.add_argument("--arnoldi-maxiter", type=int, default=60)
+    ap.add_argument("--arnoldi-maxiter", type=int, default=6, help="Krylov-Schur cycles of the C3 run")
+    ap.add_argument("--les", action="store_true", help="configuration C4 (learned-closure LES vs DNS)")
+    ap.add_argument("--les-nx", type=int, default=384)
+    ap.add_argument("--les-ny", type=int, default=193)
+    ap.add_argument("--les-re", type=float, default=10350.0)
+    ap.add_argument("--les-spinup", type=float, default=60.0)
+    ap.add_argument("--les-nsnap", type=int, default=40)
+    ap.add_argument("--les-train-iters", type=int, default=3000)
+    ap.add_argument("--les-time", type=float, default=40.0)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -722,6 +668,8 @@ def main():
         return run_ensemble(args)
     if args.arnoldi:
         return run_arnoldi(args)
+    if args.les:
+        return run_les(args)
     return run_ours(args)
 
 

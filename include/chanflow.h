@@ -380,6 +380,74 @@ int cfg_ensemble_synchronize(cfg_ensemble *e);
 void *cfg_ensemble_stream(cfg_ensemble *e);
 void cfg_ensemble_destroy(cfg_ensemble *e);
 
+/* Learned subgrid-stress closure network (the LES mode of the reference's
+ * subgrid = 1 runs, PFC/main_mpi.f90:10-13,74-78, whose modules are not in
+ * the reference): a perceptron 10 -> 64 -> 64 -> 64 -> 6 with GELU on the
+ * hidden layers, BF16 weights and activations and FP32 accumulation on the
+ * sm_100 tensor cores (tcgen05, accumulators in tensor memory).  Inputs per
+ * point: the 9 resolved velocity-gradient components and the wall distance,
+ * normalised by the caller; outputs: the 6 subgrid-stress components
+ * (11, 22, 33, 12, 13, 23), normalised.
+ *
+ * Parameters: cfg_mlp_nparams() FP32 values, W0[64][10] b0[64] W1[64][64]
+ * b1[64] W2[64][64] b2[64] W3[6][64] b3[6] (y = W x + b per layer).
+ * cfg_mlp_set_params also clears the gradient and the Adam moments.
+ *
+ * cfg_mlp_forward: x device [n][10] FP32 -> y device [n][6] FP32, on stream.
+ * cfg_mlp_accumulate_grad: one batch of training samples, rows idx[0..batch)
+ *   of x [.][10] and targets t [.][6] (device): adds the gradient of the
+ *   mean-square loss (mean over batch x 6) and the loss itself to the
+ *   network's accumulators.  cfg_mlp_get_grads copies them to the host
+ *   (synchronises); cfg_mlp_adam_step applies one Adam update (bias
+ *   corrected) from them and clears them; cfg_mlp_zero_grads clears them.
+ * cfg_mlp_status: CFG_E_STATE if a kernel gave up waiting for the tensor
+ *   cores (a bounded wait), else CFG_OK.  Needs an sm_100 device
+ *   (CFG_E_ARG otherwise). */
+typedef struct cfg_mlp cfg_mlp;
+int cfg_mlp_nparams(void);
+int cfg_mlp_create(int device, cfg_mlp **out);
+void cfg_mlp_destroy(cfg_mlp *m);
+int cfg_mlp_set_params(cfg_mlp *m, const float *params);
+int cfg_mlp_get_params(cfg_mlp *m, float *params);
+int cfg_mlp_forward(cfg_mlp *m, const float *x, float *y, long long n, void *stream);
+int cfg_mlp_accumulate_grad(cfg_mlp *m, const float *x, const float *t, const int *idx, int batch, void *stream);
+int cfg_mlp_get_grads(cfg_mlp *m, float *grads, float *loss);
+int cfg_mlp_zero_grads(cfg_mlp *m, void *stream);
+int cfg_mlp_adam_step(cfg_mlp *m, float lr, float beta1, float beta2, float eps, void *stream);
+int cfg_mlp_status(cfg_mlp *m);
+
+/* LES mode (the reference's subgrid = 1 branch, PFC/main_mpi.f90:74-78; its
+ * model modules are not in the reference): subgrid stresses added to the
+ * momentum fluxes of every nonlinear step.
+ *   model 1: eddy viscosity, Smagorinsky constant cs with van Driest damping
+ *     (1 - exp(-y+/aplus)), filter width (lx/nx * dy * lz/nz)^(1/3), u_tau
+ *     from the mean wall shear;
+ *   model 2: the learned closure (mlp, cfg_mlp_*) on the features
+ *     (G_ij = du_i/dx_j row by row and 1 - |y|, in the lower half-channel's
+ *     frame) normalised as (f - in_shift) / in_scale, its outputs mapped as
+ *     out_shift + out_scale * y; it falls back to model 1 at every point whose
+ *     stress tensor is not realizable or whose backscatter -tau:S is below
+ *     -beta times the eddy viscosity's dissipation.
+ * Needs the register-FFT x stage and one rank (CFG_E_ARG otherwise).  The
+ * network stays owned by the caller and must outlive the context's steps.
+ * cfg_les_features writes the model-2 features of the current state
+ * (device, [(ny-1) * nz2 * nx2][10], planes 2..ny, z2, x2 fastest) without a
+ * step; cfg_les_fallbacks returns the fallback count since cfg_set_les and
+ * the points per substep (synchronises); cfg_les_stresses below. */
+typedef struct cfg_les {
+  int model;
+  double cs, aplus, beta;
+  cfg_mlp *mlp;
+  float in_shift[10], in_scale[10], out_shift[6], out_scale[6];
+} cfg_les;
+int cfg_set_les(cfg_ctx *c, const cfg_les *les);
+int cfg_les_features(cfg_ctx *c, float *features);
+int cfg_les_fallbacks(cfg_ctx *c, unsigned long long *fallbacks, unsigned long long *points);
+/* the subgrid stresses of the last nonlinear step (or cfg_les_features
+ * call), host [ny+1][6][nz2][nx2] FP64, yh planes 1..ny+1, components 11,
+ * 22, 33, 12, 13, 23 (synchronises) */
+int cfg_les_stresses(cfg_ctx *c, double *S);
+
 /* cfg_xz_c2r_noalloc -- no counterpart in the reference.  The inverse x-z
  * transform of one plane (the semantics of cfg_xz_c2r /
  * xz_fft_complex_to_real) for callers that cannot allocate device memory:

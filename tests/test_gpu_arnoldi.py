@@ -58,3 +58,28 @@ def test_leading_eigenvalue_mixed_matches_fp64(cf, orc):
     a, b = mus
     assert abs(a.imag) < 1e-8 and a.real < -1.0, a
     assert abs(b - a) / abs(a) < 1e-5, (a, b)
+
+
+def test_column_arnoldi_gpu_matches_oracle(cf, orc):
+    """arnoldi_columns with the GPU propagator (16x17x16, Re 2900, T = 0.5):
+    FP64 leading eigenvalues equal the oracle's dense column spectra to
+    1e-10 with explicit residuals below 1e-8; mixed precision equals FP64 to
+    1e-5."""
+    import test_stability_columns as tsc
+    op = tsc.OracleOperator(orc, cf)
+    mu_o, _, _, cols_o = cf.chanflow.arnoldi_columns(op, 50, ncv=30, nev=10, restarts=4)
+    grid = cf.Grid(16, 17, 16, lx=4 * np.pi, lz=2 * np.pi, stretch=1.5)
+    base = np.zeros((18, 3), order="F")
+    base[:, 0] = 1 - grid.yh ** 2
+    mus = {}
+    for name, prec, tol in (("fp64", cf.FP64, 1e-9), ("mixed", cf.MIXED, 1e-5)):
+        f = cf.ChannelFlow(grid, re=2900.0, dt=0.01, fix_mass=0, precision=prec)
+        f.set_baseflow(base)
+        mu, lam, res, cols = cf.chanflow.arnoldi_columns(f, 50, ncv=30, nev=10, restarts=4, tol=tol)
+        mus[name] = (mu, res)
+        f.close()
+    mu64, res64 = mus["fp64"]
+    assert np.abs(np.abs(mu64) - np.abs(mu_o)).max() < 1e-10
+    assert res64.max() < 1e-8, res64
+    mum, _ = mus["mixed"]
+    assert np.abs(np.abs(mum) - np.abs(mu64)).max() < 1e-5 * np.abs(mu64).max()

@@ -92,10 +92,13 @@ def test_initial_field(cf, orc, prec):
     assert rel(flow.scalars()["d_um_dy"], o.d_um_dy) < 1e-12
 
 
-@pytest.mark.parametrize("prec,tol", [(0, 1e-10), (1, 1e-5)])
-def test_config_c1_100_steps(cf, orc, prec, tol):
+@pytest.mark.parametrize("prec,tol,ptol", [(0, 1e-10, 1e-10), (1, 1e-5, 3e-5)])
+def test_config_c1_100_steps(cf, orc, prec, tol, ptol):
     """Config C1: 32x33x32, Re 2500, stretch 1.5, laminar + 1e-3 k^-2 noise,
-    constant flux, dt 0.005, 100 steps."""
+    constant flux, dt 0.005, 100 steps.  The perturbation (every Fourier
+    column but the mean) is gated on its own: FP64 1e-10 (measured on a B200
+    2.6e-14), mixed 3e-5 (measured 5.6e-6; FP32 transforms carry the mean
+    with the noise, see test_gpu_metric_config.py)."""
     grid, flow, o = make(cf, orc, 32, 33, 32, prec=prec)
     o.init_field(10, seed=1, ampl=1e-3)
     flow.define_initial_field(10, seed=1, ampl=1e-3)
@@ -107,7 +110,7 @@ def test_config_c1_100_steps(cf, orc, prec, tol):
     # the perturbation (non-mean part) is also checked on its own
     pert = d1.copy(); pert[0, 0] = 0
     opert = o.data1.copy(); opert[0, 0] = 0
-    assert rel(pert, opert) < 100 * tol
+    assert rel(pert, opert) < ptol, rel(pert, opert)
     sc = flow.scalars()
     t, dt, pg = o.scalars()
     assert abs(sc["t_total"] - t) < 1e-12
@@ -200,3 +203,34 @@ def test_cfl_abort_is_a_status(cf, orc):
     flow.define_initial_field(10, seed=3, ampl=1e-2)
     flow.timestep(1)
     assert flow.status() == -4
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_adaptive_dt_against_oracle(cf, orc, prec):
+    """dt_flag = 1 (PFC/pass1.f90:107-124): after each step's first substep
+    dt moves toward cfl_max/cfl (dt_temp = dt*cfl_max/cfl, dt = min(dt_temp,
+    dt + (dt_temp - dt)*dt/(1 + dt))).  From 0.005 the rule raises dt to ~0.1
+    in 20 steps at 32x33x32; the dt sequence and the state follow the oracle:
+    FP64 dt to 1e-12, state 1e-10 (measured 1.4e-15, 1.1e-15); mixed dt to
+    1e-6, state 1e-5 whole and 1e-4 perturbation (measured 4.5e-8, 4.2e-8,
+    2.9e-5)."""
+    grid, flow, o = make(cf, orc, 32, 33, 32, prec=prec, dt_flag=1)
+    o.init_field(10, seed=1, ampl=1e-3)
+    flow.define_initial_field(10, seed=1, ampl=1e-3)
+    gd, od = [], []
+    for _ in range(20):
+        o.timestep(1)
+        flow.timestep(1)
+        od.append(o.scalars()[1])
+        gd.append(flow.scalars()["dt"])
+    od, gd = np.array(od), np.array(gd)
+    assert od[-1] > 10 * od[0]          # the rule did adapt dt
+    assert np.abs(gd / od - 1).max() < (1e-12 if prec == 0 else 1e-6)
+    d1, _, _ = flow.download_state()
+    assert rel(d1, o.data1) < (1e-10 if prec == 0 else 1e-5)
+    p1, po = d1.copy(), o.data1.copy()
+    p1[0, 0] = 0
+    po[0, 0] = 0
+    assert rel(p1, po) < (1e-10 if prec == 0 else 1e-4)
+    assert abs(flow.scalars()["t_total"] - o.scalars()[0]) < 1e-12 * o.scalars()[0]
+    assert flow.status() == 0

@@ -11,9 +11,12 @@ Pins:
 - the oracle DNS started from that mode (laminar + 1e-4 mode, fix_mass 0,
   the reference's stretch 2.75, dt = 2 (2 pi / 0.24989154) / tend as
   PFC/setup.f90:1386-1388 sets it) grows the mode's energy (ke of
-  PFC/pass2.f90:113-117) at 2 alpha c_i, to the second-order accuracy of
-  its y differences: within 0.6 % at ny = 193 and, Richardson-extrapolated
-  from ny = 97 and 193, within 0.1 %.
+  PFC/pass2.f90:113-117) at 2 alpha c_i to the accuracy of its second-order
+  y differences: within 0.6 % at ny = 193 and, Richardson-extrapolated from
+  ny = 97 and 193, within 0.1 % (measured 0.51 % and 0.04 %; the DNS mean
+  also drifts slowly, by ~2e-5 over the run, from 1 - yh^2 toward the
+  discrete steady profile, which moves the rate by a fraction of that
+  error).
 """
 import importlib
 
