@@ -17,6 +17,45 @@ template <typename C> __host__ __device__ __forceinline__ C csub(C a, C b) { ret
 template <typename C> __host__ __device__ __forceinline__ C cmul(C a, C b) { return mk<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
 template <typename C> __host__ __device__ __forceinline__ C cconj(C a) { return mk<C>(a.x, -a.y); }
 template <typename C, typename T> __host__ __device__ __forceinline__ C cscale(T s, C a) { return mk<C>(s * a.x, s * a.y); }
+
+// FP32 complex additions, subtractions and real scalings as one packed
+// two-lane instruction (add/sub/mul.rn.f32x2, sm_100): the same IEEE results
+// as the two scalar operations, half the issued instructions.
+#if !defined(CFD_NO_F32X2)
+template <> __host__ __device__ __forceinline__ float2 cadd<float2>(float2 a, float2 b) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+  float2 r;
+  asm("{.reg .b64 pa, pb, pr;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+      "add.rn.f32x2 pr, pa, pb;\n\tmov.b64 {%0, %1}, pr;}"
+      : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+#else
+  return mk<float2>(a.x + b.x, a.y + b.y);
+#endif
+}
+template <> __host__ __device__ __forceinline__ float2 csub<float2>(float2 a, float2 b) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+  float2 r;
+  asm("{.reg .b64 pa, pb, pr;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+      "sub.rn.f32x2 pr, pa, pb;\n\tmov.b64 {%0, %1}, pr;}"
+      : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+#else
+  return mk<float2>(a.x - b.x, a.y - b.y);
+#endif
+}
+template <> __host__ __device__ __forceinline__ float2 cscale<float2, float>(float s, float2 a) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+  float2 r;
+  asm("{.reg .b64 pa, ps, pr;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 ps, {%4, %4};\n\t"
+      "mul.rn.f32x2 pr, ps, pa;\n\tmov.b64 {%0, %1}, pr;}"
+      : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(s));
+  return r;
+#else
+  return mk<float2>(s * a.x, s * a.y);
+#endif
+}
+#endif
 // (i*k) * a for real k
 template <typename C, typename T> __host__ __device__ __forceinline__ C cimul(T k, C a) { return mk<C>(-k * a.y, k * a.x); }
 template <typename C> __host__ __device__ __forceinline__ C czero() { return mk<C>(0, 0); }

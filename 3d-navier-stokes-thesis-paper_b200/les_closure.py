@@ -254,7 +254,7 @@ def run_c4(nx=384, ny=193, nz=384, factor=3, re=10350.0, stretch=1.5, ampl=0.5, 
                   "ms_per_time_unit": e0.elapsed_time(e1) / sc["t_total"]}
     log(f"DNS spin-up: {nsteps} steps to t = {sc['t_total']:.2f}, {dns_ms:.3f} ms/step, dt {sc['dt']:.4g}")
     probe = FeatureProbe(gl, re, device=device, cs=cs)
-    feats, targs, evs, states = [], [], [], []
+    feats, targs, evs, states, retau = [], [], [], [], []
     Uf, Rf = 0.0, 0.0
     for s in range(nsnap):
         if s:
@@ -269,6 +269,9 @@ def run_c4(nx=384, ny=193, nz=384, factor=3, re=10350.0, stretch=1.5, ampl=0.5, 
             states.append(les_d1)
         U, R = profile_stats(les_d1, gl)
         Uf, Rf = Uf + U / nsnap, Rf + R / nsnap
+        dud = dns.scalars()["d_um_dy"]
+        retau.append(math.sqrt(0.5 * (abs(dud[0]) + abs(dud[-1])) / re) * re)
+    out["dns"]["re_tau_snapshots"] = [round(v, 2) for v in retau]
     out["dns"]["status_end"] = dns.status()
     out["dns"]["t_end"] = dns.scalars()["t_total"]
     dns.close()

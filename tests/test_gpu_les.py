@@ -68,7 +68,7 @@ def features_np(o, P, k, in_shift, in_scale):
 
 def test_learned_closure_matches_restatement(cf, orc):
     import torch
-    grid, flow, o = setup_pair(cf, orc, 0, nx=24, ny=17, nz=24)
+    grid, flow, o = setup_pair(cf, orc, 0, nx=32, ny=17, nz=32)
     p = mo.init_params(21)
     net = cf.Mlp(0, p)
     in_shift = np.zeros(10)

@@ -232,5 +232,6 @@ def test_adaptive_dt_against_oracle(cf, orc, prec):
     p1[0, 0] = 0
     po[0, 0] = 0
     assert rel(p1, po) < (1e-10 if prec == 0 else 1e-4)
-    assert abs(flow.scalars()["t_total"] - o.scalars()[0]) < 1e-12 * o.scalars()[0]
+    # t_total sums the dt sequence: FP64 to round-off, mixed to its dt bar
+    assert abs(flow.scalars()["t_total"] - o.scalars()[0]) < (1e-12 if prec == 0 else 1e-6) * o.scalars()[0]
     assert flow.status() == 0

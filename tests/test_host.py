@@ -182,6 +182,7 @@ def test_headers_compile_as_c99(tmp_path):
 
 
 RUN_BIN = os.path.join(ROOT, "3d-navier-stokes-thesis-paper_b200", "lib", "chanflow_run")
+GOLD = os.path.join(ROOT, "tests", "golden")
 
 
 @pytest.mark.skipif(not os.path.exists(RUN_BIN), reason="chanflow_run not built")
@@ -194,6 +195,10 @@ def test_run_program_arguments(tmp_path):
     assert subprocess.run([RUN_BIN], capture_output=True).returncode == 2
     r = subprocess.run([RUN_BIN, str(tmp_path / "missing.dat")], capture_output=True, text=True)
     assert r.returncode == 1 and "cannot open" in r.stderr
+    # --restart with read_vel = 0 in flow.dat is refused (the file would be ignored)
+    r = subprocess.run([RUN_BIN, os.path.join(GOLD, "flow_c1.dat"), "--restart", str(tmp_path / "x.out")],
+                       capture_output=True, text=True)
+    assert r.returncode == 2 and "read_vel = 0" in r.stderr
 
 
 def test_group_splits_and_gathers_kx_slabs(cf):
