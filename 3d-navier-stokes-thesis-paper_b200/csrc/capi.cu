@@ -230,6 +230,10 @@ struct cfg_ctx {
   // LES mode (cfg_set_les): subgrid stresses S[ny+1][6][nz2][nx2] (storage
   // precision) added by the flux kernel; the learned closure's features and
   // outputs (FP32) and its fallback counter
+  // mean split of the mixed path's nonlinear products (k_zinv_r drops the
+  // mean column, k_flux_r adds its products from mean_base, FP64 (ny+1, 3))
+  bool mean_split = false;
+  double* mean_base = nullptr;
   bool les_on = false;
   LesDev les{};
   cfg_mlp* les_mlp = nullptr;
@@ -357,6 +361,14 @@ static cudaError_t allow_smem(K kernel) {
   return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
 }
 
+// the real parts of the mean column (kx = kz = 0) of the velocity as the
+// (ny+1, 3) FP64 profile the mean-split flux kernel reads: from the FP64 side
+// copy m64 when given, else from the FP32 state
+__global__ void k_mean_base(const double2* __restrict__ m64, const float2* __restrict__ v32, double* __restrict__ base,
+                            int ny1) {
+  for (int i = threadIdx.x; i < 3 * ny1; i += blockDim.x) base[i] = m64 ? m64[i].x : (double)v32[i].x;
+}
+
 template <typename T>
 struct Impl {
   using C = cplx_t<T>;
@@ -441,6 +453,15 @@ struct Impl {
       cudaGetLastError();
       c->split_x = false;
     }
+    // mixed precision, one rank, register transforms: the FP32 transforms
+    // carry the fluctuation only and the mean's products come from its FP64
+    // copy (CHANFLOW_NO_MEAN_SPLIT=1 keeps the whole velocity in the
+    // transforms)
+    c->mean_split = f32 && c->split_x && c->fast_z && c->nranks == 1 && !getenv("CHANFLOW_NO_MEAN_SPLIT");
+    if (c->mean_split && cudaMalloc(&c->mean_base, sizeof(double) * 3 * (size_t)g.ny1) != cudaSuccess) {
+      cudaGetLastError();
+      c->mean_split = false;
+    }
     c->use_rhs2 = rhs2_supported(g.ny1) && !getenv("CHANFLOW_RHS_V1");
     // 16 lanes per wavenumber exists for FP32 only (the FP64 kernel and its
     // coefficient table stay at 32)
@@ -478,7 +499,15 @@ struct Impl {
     a.P = c->P;
     a.FZR = c->flux_zr;
     a.sc = c->scat;
+    a.split = (c->mean_split && !lin && !c->les_on) ? 1 : 0;
     if (phase == 1) {
+      if (a.split) {
+        // the current mean velocity (the FP64 side copy when it holds it)
+        prof_begin(c, "k_mean_base");
+        k_mean_base<<<1, 256, 0, c->st>>>(c->mean64_valid ? c->mvel64 : nullptr, (const float2*)c->vel, c->mean_base,
+                                         g.ny1);
+        CKL();
+      }
       c->mean64_valid = false;
       if (do_cfl) CK(cudaMemsetAsync(c->cflbits, 0, sizeof(unsigned long long) * 3 * g.ny1, c->st));
       dim3 g1(g.nxh, (g.ny1 + c->YB1 - 1) / c->YB1);
@@ -506,6 +535,7 @@ struct Impl {
           if (r) return r;
           a.sgs = c->les_S;
         }
+        if (a.split) a.gd.baseflow = c->mean_base;
         prof_begin(c, "k_flux");
         if (p1_fast_launch(4, g.nx2, f32, a) != 0) return fail(c, CFG_E_CUDA, "k_flux_r launch");
       } else if (c->fast_x) {
@@ -1068,7 +1098,7 @@ void cfg_destroy(cfg_ctx* c) {
                   c->sc, c->d_um_dy, c->cflp, c->cflbits, c->l2acc, c->divbits, c->plist, c->pw_H,
                   c->pw_phys, c->pw_phys2, c->pw_in, c->stage, c->twx, c->twz, c->twxs, c->twzs,
                   c->wl_fast, c->wl_prec, c->scat_tab, c->cfl_peers, c->les_S, c->les_F, c->les_Y,
-                  c->les_nfall};
+                  c->les_nfall, c->mean_base};
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);

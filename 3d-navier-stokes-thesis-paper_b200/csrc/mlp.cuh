@@ -1,6 +1,6 @@
 // mlp.cuh -- the learned subgrid-stress closure's network on the 5th-generation
 // tensor cores (sm_100a tcgen05): a 10 -> 64 -> 64 -> 64 -> 6 perceptron with
-// GELU on the three hidden layers, BF16 weights and activations, FP32
+// GELU (tanh form) on the three hidden layers, BF16 weights and activations, FP32
 // accumulation in tensor memory (TMEM).
 //
 // One CTA of 128 threads (4 warps) handles a tile of 128 points: thread t owns
@@ -137,10 +137,25 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
 }
 
 // ---------------------------------------------------------------- activation
-// GELU(z) = z * Phi(z) and its derivative Phi(z) + z * phi(z)
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+// GELU in its tanh form (Hendrycks & Gimpel 2016):
+//   g(z) = z (1 + t) / 2,  t = tanh(c (z + a z^3)),  c = sqrt(2/pi), a = 0.044715,
+//   g'(z) = (1 + t) / 2 + z (1 - t^2) c (1 + 3 a z^2) / 2,
+// with the hardware tanh approximation (tanh.approx.f32, relative error below
+// 2^-10, under the BF16 rounding the activations get next)
+__device__ __forceinline__ float tanh_hw(float u) {
+  float t;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
+  return t;
+}
+constexpr float kGeluC = 0.7978845608028654f, kGeluA = 0.044715f;
+__device__ __forceinline__ float gelu(float z) {
+  const float t = tanh_hw(kGeluC * z * fmaf(kGeluA * z, z, 1.0f));
+  return 0.5f * z * (1.0f + t);
+}
 __device__ __forceinline__ float gelu_d(float z) {
-  return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * __expf(-0.5f * z * z);
+  const float z2 = z * z;
+  const float t = tanh_hw(kGeluC * z * fmaf(kGeluA, z2, 1.0f));
+  return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * kGeluC * fmaf(3.0f * kGeluA, z2, 1.0f);
 }
 
 // 8 BF16 values as one 16-byte unit

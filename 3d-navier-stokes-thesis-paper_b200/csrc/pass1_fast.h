@@ -26,6 +26,7 @@ struct P1Launch {
   int FZR;              // z rows per k_flux_r block (2 or 4)
   Scatter sc;           // transposes of a multi-rank run (n == 0: one rank)
   const void* sgs;      // LES subgrid stresses [ny+1][6][nz2][nx2] for k_flux_r, or null
+  int split;            // mean split: k_zinv_r drops the mean column, k_flux_r adds it from gd.baseflow
   cudaStream_t st;
 };
 

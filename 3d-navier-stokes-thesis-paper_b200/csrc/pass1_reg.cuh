@@ -55,7 +55,8 @@ template <typename T> struct ZRawPad {   // 32 bytes between component blocks
 template <typename T, int NZ2>
 __global__ void __launch_bounds__(288, sizeof(T) == 4 ? 3 : 1) k_zinv_r(const cplx_t<T>* __restrict__ vel,
                                                 cplx_t<T>* __restrict__ T1, Geom g,
-                                                const cplx_t<T>* __restrict__ twz, int YB, Scatter sc) {
+                                                const cplx_t<T>* __restrict__ twz, int YB, Scatter sc,
+                                                int split) {
   using C = cplx_t<T>;
   constexpr int N1 = Split<NZ2>::N1, N2 = Split<NZ2>::N2, PITCH = N2 + 1, SEQ = SeqPitch<NZ2>::V;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -90,6 +91,12 @@ __global__ void __launch_bounds__(288, sizeof(T) == 4 ? 3 : 1) k_zinv_r(const cp
   load_tw2<T, NZ2>(tw, twz);
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   __syncthreads();
+  if (split && g.kx0 + kx == 0) {
+    // mean split: the kx = kz = 0 column leaves the physical fields (the
+    // flux kernel adds the mean's products from its FP64 copy)
+    for (int i = threadIdx.x; i < 3 * YB; i += blockDim.x) raw[(i / YB) * RS + (i % YB)] = czero<C>();
+    __syncthreads();
+  }
   const T half = (T)0.5;
   const bool halve_x = (g.nx2 > g.nx) && (g.kx0 + kx == g.nxh_all - 1) && (NZ2 > NZ);
   // stage 1: consecutive threads take consecutive sequences (planes fastest)
@@ -625,7 +632,12 @@ __global__ void __launch_bounds__(256) k_xinv_r(const cplx_t<T>* __restrict__ T1
 // transform and the Hermitian unpacking into T2 -- the same arithmetic and
 // output as k_xflux_r (PFC/pass1.f90:134-226, PFC/transform.f90:287-315).
 // MODE 0: the nonlinear products; 1: the linearized products about the
-// baseflow (PFC/pass1_linearized.f90:135-509); 2: the nonlinear products plus
+// baseflow (PFC/pass1_linearized.f90:135-509); 3: the nonlinear products of
+// a field split into its plane mean B (gd.baseflow, FP64) and the rest u
+// (the physical planes, mean column removed): (B + u)(B + u) - B B = the
+// linearized products plus u u, the mean-mean products being constant in x
+// and z (their divergence is the y derivative of B_i V, zero without net
+// transpiration), the fringe and CFL on B + u; 2: the nonlinear products plus
 // the subgrid stresses of the LES mode, S[pl][6][nz2][nx2] on the yh planes
 // (components 11, 22, 33, 12, 13, 23; zero on the walls), added to the
 // momentum fluxes at the same points (y-plane values interpolated as the
@@ -636,7 +648,8 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT
                                                const T* __restrict__ fringe, int has_fringe,
                                                unsigned long long* __restrict__ cflbits, int do_cfl, Scatter sc,
                                                const T* __restrict__ S) {
-  constexpr bool LIN = MODE == 1, SGS = MODE == 2;
+  constexpr bool LIN = MODE == 1, SGS = MODE == 2, SPLIT = MODE == 3;
+  constexpr bool HASB = LIN || SPLIT;
   using C = cplx_t<T>;
   constexpr int N1 = Split<NX2>::N1, N2 = Split<NX2>::N2, PITCH = N2 + 1, SEQ = SeqPitch<NX2>::V;
   constexpr int N = NX2;
@@ -665,7 +678,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT
   const T tu = (T)gd.target[(k - 1)], tv = (T)gd.target[(ny + 1) + (k - 1)];
   const T tw_ = (T)gd.target[2 * (ny + 1) + (k - 1)];
   T B0[3] = {0, 0, 0}, Bm[3] = {0, 0, 0}, Bp[3] = {0, 0, 0};
-  if (LIN) {
+  if (HASB) {
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
       B0[q] = (T)gd.baseflow[q * (ny + 1) + k - 1];
@@ -684,7 +697,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT
   // stresses of the point (SGS mode): 11, 22, 33, 12, 13, 23 at yh plane k,
   // then 12, 23 at plane k-1 and 12, 22, 23 at plane k+1
   auto point = [&](T U, T V, T W, T Up, T Vp, T Wp, T Um, T Vm, T Wm, T fr, int r, int x, const T* tau) {
-  T fpu0, fpw0, fpu, fpw, xfu, zfu, xfw, zfw;
+  T fpu0 = 0, fpw0 = 0, fpu = 0, fpw = 0, xfu = 0, zfu = 0, xfw = 0, zfw = 0;
   if (!LIN) {
     if (k == 2) { fpu0 = Vm * Um; fpw0 = Vm * Wm; }
     else { fpu0 = Vm * half * (Um + U); fpw0 = Vm * half * (Wm + W); }
@@ -697,27 +710,30 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT
       if (k > 2) { fpu0 += half * (tau[6] + tau[3]); fpw0 += half * (tau[7] + tau[5]); }
       if (k < ny) { fpu += half * (tau[3] + tau[8]); fpw += half * (tau[5] + tau[10]); }
     }
-  } else {
-    if (k == 2) { fpu0 = Bm[1] * Um + Vm * Bm[0]; fpw0 = Bm[1] * Wm + Vm * Bm[2]; }
+  }
+  if (HASB) {
+    if (k == 2) { fpu0 += Bm[1] * Um + Vm * Bm[0]; fpw0 += Bm[1] * Wm + Vm * Bm[2]; }
     else {
-      fpu0 = Bm[1] * half * (Um + U) + Vm * half * (Bm[0] + B0[0]);
-      fpw0 = Bm[1] * half * (Wm + W) + Vm * half * (Bm[2] + B0[2]);
+      fpu0 += Bm[1] * half * (Um + U) + Vm * half * (Bm[0] + B0[0]);
+      fpw0 += Bm[1] * half * (Wm + W) + Vm * half * (Bm[2] + B0[2]);
     }
     if (k < ny) {
-      fpu = B0[1] * half * (U + Up) + V * half * (B0[0] + Bp[0]);
-      fpw = B0[1] * half * (W + Wp) + V * half * (B0[2] + Bp[2]);
+      fpu += B0[1] * half * (U + Up) + V * half * (B0[0] + Bp[0]);
+      fpw += B0[1] * half * (W + Wp) + V * half * (B0[2] + Bp[2]);
     } else {
-      fpu = B0[1] * Up + V * Bp[0];
-      fpw = B0[1] * Wp + V * Bp[2];
+      fpu += B0[1] * Up + V * Bp[0];
+      fpw += B0[1] * Wp + V * Bp[2];
     }
-    xfu = two * B0[0] * U; zfu = B0[2] * U + W * B0[0];
-    xfw = B0[2] * U + W * B0[0]; zfw = two * B0[2] * W;
+    xfu += two * B0[0] * U; zfu += B0[2] * U + W * B0[0];
+    xfw += B0[2] * U + W * B0[0]; zfw += two * B0[2] * W;
   }
-  const T dyu = dhk * (fpu - fpu0) + fr * (U - tu);
-  const T dyw = dhk * (fpw - fpw0) + fr * (W - tw_);
+  // the fringe acts on the whole velocity (its mean included when split)
+  const T Uf = SPLIT ? U + B0[0] : U, Wf = SPLIT ? W + B0[2] : W, Vf = SPLIT ? V + B0[1] : V;
+  const T dyu = dhk * (fpu - fpu0) + fr * (Uf - tu);
+  const T dyw = dhk * (fpw - fpw0) + fr * (Wf - tw_);
   T xfv = 0, dyv = 0, zfv = 0;
   if (veq) {
-    T fp0, fp;
+    T fp0 = 0, fp = 0;
     if (!LIN) {
       const T t0 = half * (Vm + V), t1 = half * (V + Vp);
       fp0 = t0 * t0; fp = t1 * t1;
@@ -729,14 +745,15 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT
         fp0 += tau[1];
         fp += tau[9];
       }
-    } else {
+    }
+    if (HASB) {
       const T t0 = half * (Vm + V), b0v = half * (Bm[1] + B0[1]);
       const T t1 = half * (V + Vp), b1v = half * (B0[1] + Bp[1]);
-      fp0 = two * t0 * b0v; fp = two * t1 * b1v;
-      xfv = B0[1] * (iu1 * U + iu2 * Up) + V * (iu1 * B0[0] + iu2 * Bp[0]);
-      zfv = B0[1] * (iu1 * W + iu2 * Wp) + V * (iu1 * B0[2] + iu2 * Bp[2]);
+      fp0 += two * t0 * b0v; fp += two * t1 * b1v;
+      xfv += B0[1] * (iu1 * U + iu2 * Up) + V * (iu1 * B0[0] + iu2 * Bp[0]);
+      zfv += B0[1] * (iu1 * W + iu2 * Wp) + V * (iu1 * B0[2] + iu2 * Bp[2]);
     }
-    dyv = dnk * (fp - fp0) + fr * (V - tv);
+    dyv = dnk * (fp - fp0) + fr * (Vf - tv);
   }
   const int pxx = px(x);
   (void)zfu;
@@ -745,9 +762,15 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT
   FP[(4 * r + 2) * SEQ + pxx] = mk<C>(xfv, dyv);
   FP[(4 * r + 3) * SEQ + pxx] = mk<C>(zfw, zfv);
     if (do_cfl) {
-      ma = fmax(ma, fabs(U + Up));
-      mb = fmax(mb, fabs(V));
-      mc = fmax(mc, fabs(W + Wp));
+      if (SPLIT) {
+        ma = fmax(ma, fabs(U + Up + B0[0] + Bp[0]));
+        mb = fmax(mb, fabs(V + B0[1]));
+        mc = fmax(mc, fabs(W + Wp + B0[2] + Bp[2]));
+      } else {
+        ma = fmax(ma, fabs(U + Up));
+        mb = fmax(mb, fabs(V));
+        mc = fmax(mc, fabs(W + Wp));
+      }
     }
   };
   // two neighbouring x per thread and 8- or 16-byte loads (x even, rows of

@@ -220,7 +220,7 @@ def advance_to(flow, t_end, chunk=10):
 
 def run_c4(nx=384, ny=193, nz=384, factor=3, re=10350.0, stretch=1.5, ampl=0.5, seed=4, spinup=60.0,
            nsnap=40, snap_dt=0.5, cfl=0.5, train_iters=3000, batch=4096, lr=2e-3, les_spin=20.0, les_avg=20.0,
-           cs=0.1, beta=0.0, device=0, log=print):
+           cs=0.1, beta=0.0, device=0, log=print, artifact=None):
     """Configuration C4 end to end: DNS from the turbulent-profile initial
     field (which_test 4 plus seeded noise) at nx x ny x nz, nsnap snapshots
     snap_dt apart after `spinup` time units, box-filtered by `factor` in x
@@ -229,7 +229,9 @@ def run_c4(nx=384, ny=193, nz=384, factor=3, re=10350.0, stretch=1.5, ampl=0.5, 
     last against the eddy viscosity, and LES runs (no model, eddy viscosity,
     learned closure) from the first filtered snapshot against the filtered
     DNS mean profile and resolved Reynolds stresses.  All steps mixed
-    precision with adaptive dt (cfl_max = cfl).  Returns a dict of results."""
+    precision with adaptive dt (cfl_max = cfl).  artifact: an .npz path where
+    the a-posteriori inputs are saved (les_from_artifact reruns them).
+    Returns a dict of results."""
     import time
     import torch
     out = {"config": dict(nx=nx, ny=ny, nz=nz, factor=factor, re=re, stretch=stretch, ampl=ampl, spinup=spinup,
@@ -303,14 +305,34 @@ def run_c4(nx=384, ny=193, nz=384, factor=3, re=10350.0, stretch=1.5, ampl=0.5, 
                        "nn_corr_12": corr(pred, 3), "ev_corr_12": corr(ev, 3), "points": int(th.shape[0])}
     log(f"a priori: deviatoric error NN {out['a_priori']['nn_deviatoric_rel_err']:.3f}, "
         f"eddy viscosity {out['a_priori']['ev_deviatoric_rel_err']:.3f}")
-    # a posteriori: LES from the first filtered snapshot
+    if artifact:
+        # what the a-posteriori runs need, to rerun them without the DNS
+        np.savez_compressed(artifact, state=states[0], Uf=Uf, Rf=Rf, params=net.get_params(), mi=mi, si=si, mo=mo,
+                            so=so, grid=np.array([gl.nx, gl.ny, gl.nz]), stretch=stretch, re=re,
+                            dns_ms_per_time_unit=out["dns"]["ms_per_time_unit"])
+    out["les"] = les_runs(gl, re, states[0], Uf, Rf, net, (mi, si, mo, so), cfl, les_spin, les_avg, cs, beta,
+                          device, log)
+    out["speedup_per_time_unit"] = {k: out["dns"]["ms_per_time_unit"] / v["ms_per_time_unit"]
+                                    for k, v in out["les"].items()}
+    out["filtered_dns"] = {"U": Uf.tolist(), "uv": Rf[3].tolist()}
+    net.close()
+    return out
+
+
+def les_runs(gl, re, state, Uf, Rf, net, norm, cfl=0.5, les_spin=20.0, les_avg=20.0, cs=0.1, beta=0.0, device=0,
+             log=print, models=(("none", 0), ("eddy_viscosity", 1), ("learned", 2))):
+    """LES on grid gl from the filtered state, one run per closure: les_spin
+    time units, then statistics every 0.5 time units over les_avg, against
+    the filtered DNS mean profile Uf and stresses Rf."""
+    import torch
+    mi, si, mo, so = norm
     Ucl = float(np.max(Uf))
     les = {}
-    for name, model in (("none", 0), ("eddy_viscosity", 1), ("learned", 2)):
+    for name, model in models:
         f = ChannelFlow(gl, re=re, dt=0.005, fix_mass=1, dt_flag=1, cfl_max=cfl, precision=MIXED, device=device)
-        f.upload_state(states[0], None, None)
+        f.upload_state(state, None, None)
         sc = f.scalars()
-        f.set_scalars(0.0, sc["dt"], sc["p_grad"], wall_gradient(states[0], gl))
+        f.set_scalars(0.0, sc["dt"], sc["p_grad"], wall_gradient(state, gl))
         f.remove_initial_divergence()
         f.compute_initial_pressure(0)
         if model:
@@ -344,8 +366,20 @@ def run_c4(nx=384, ny=193, nz=384, factor=3, re=10350.0, stretch=1.5, ampl=0.5, 
         les[name] = res
         log(f"LES {name}: {res}")
         f.close()
-    out["les"] = les
-    out["speedup_per_time_unit"] = {k: out["dns"]["ms_per_time_unit"] / v["ms_per_time_unit"] for k, v in les.items()}
-    out["filtered_dns"] = {"U": Uf.tolist(), "uv": Rf[3].tolist()}
-    net.close()
-    return out
+    return les
+
+
+def les_from_artifact(path, device=0, log=print, **kw):
+    """les_runs from an artifact run_c4 saved: the filtered initial state,
+    the filtered DNS statistics, the trained network and its normalisation."""
+    a = np.load(path)
+    nx, ny, nz = (int(v) for v in a["grid"])
+    gl = Grid(nx, ny, nz, lx=4 * np.pi, lz=2 * np.pi, stretch=float(a["stretch"]))
+    net = Mlp(device, a["params"])
+    try:
+        les = les_runs(gl, float(a["re"]), a["state"], a["Uf"], a["Rf"], net, (a["mi"], a["si"], a["mo"], a["so"]),
+                       device=device, log=log, **kw)
+    finally:
+        net.close()
+    dms = float(a["dns_ms_per_time_unit"])
+    return les, {k: dms / v["ms_per_time_unit"] for k, v in les.items()}

@@ -440,6 +440,88 @@ def run_arnoldi(args):
     return 0
 
 
+def run_mlp(args):
+    """The closure network's tensor-core kernels alone: forward over n points
+    and one training batch (forward + backward + gradient accumulation),
+    timed with CUDA events; achieved FLOP/s against the measured bf16 peak
+    (algorithmic: 2 x 9216 multiply-adds per point forward, 3x that to train)."""
+    import importlib
+    import torch
+    import __graft_entry__
+    cf = __graft_entry__.load_package()
+    lc = importlib.import_module("chanflow_b200.les_closure")
+    n, B, reps = args.mlp_points, args.mlp_batch, max(3, args.steps)
+    net = cf.Mlp(0, lc.init_params(1))
+    x = torch.randn(n, 10, device="cuda")
+    y = torch.empty(n, 6, device="cuda")
+    t = torch.randn(n, 6, device="cuda")
+    idx = torch.randint(0, n, (B,), device="cuda", dtype=torch.int32)
+    for _ in range(args.warmup):
+        net.forward(x.data_ptr(), y.data_ptr(), n)
+        net.accumulate_grad(x.data_ptr(), t.data_ptr(), idx.data_ptr(), B)
+    torch.cuda.synchronize()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    e[0].record()
+    for _ in range(reps):
+        net.forward(x.data_ptr(), y.data_ptr(), n)
+    e[1].record()
+    for _ in range(reps):
+        net.accumulate_grad(x.data_ptr(), t.data_ptr(), idx.data_ptr(), B)
+    e[2].record()
+    e[2].synchronize()
+    fwd_ms, trn_ms = e[0].elapsed_time(e[1]) / reps, e[1].elapsed_time(e[2]) / reps
+    macs = 10 * 64 + 64 * 64 * 2 + 64 * 6
+    pk, kind = peaks()
+    peak = float(pk.get("bf16_tflops", PEAKS_FALLBACK["bf16_tflops"]))
+    fwd = 2 * macs * n / (fwd_ms / 1e3) / 1e12
+    trn = 6 * macs * B / (trn_ms / 1e3) / 1e12
+    line = {"metric": "closure network TFLOP/s (tensor cores)", "value": fwd, "unit": "TFLOP/s", "n_gpus": 1,
+            "higher_is_better": True, "dtype": "bf16 (f32 accumulation)", "data": "synthetic (random inputs)",
+            "config": {"workload": f"MLP 10-64-64-64-6 GELU forward over {n} points, training batch {B}"},
+            "roofline": {"bound": "tensor", "achieved": fwd, "peak": peak, "unit": "TFLOP/s", "frac": fwd / peak,
+                         "peak_kind": kind, "kernel": "k_mlp_fwd"},
+            "forward_ms": fwd_ms, "train_batch_ms": trn_ms, "train_tflops": trn, "status": net.status()}
+    print(json.dumps(line), flush=True)
+    net.close()
+    return 0
+
+
+def run_les_step(args):
+    """One LES step at configuration C4's LES grid (128x65x128) with the
+    learned closure (random weights: every point runs the network and the
+    checks) against the same grid with the eddy viscosity and without a
+    model; CUDA-event times per step and per kernel."""
+    import importlib
+    import torch
+    import __graft_entry__
+    cf = __graft_entry__.load_package()
+    lc = importlib.import_module("chanflow_b200.les_closure")
+    grid = cf.Grid(128, 65, 128, lx=4 * np.pi, lz=2 * np.pi, stretch=STRETCH)
+    out = {}
+    for name, model in (("none", 0), ("eddy_viscosity", 1), ("learned", 2)):
+        f = cf.ChannelFlow(grid, re=args.les_re, dt=0.005, precision=cf.MIXED)
+        f.define_initial_field(4, seed=4, ampl=0.3)
+        net = None
+        if model:
+            net = cf.Mlp(0, lc.init_params(2)) if model == 2 else None
+            f.set_les(model, cs=0.1, mlp=net, in_shift=np.zeros(10), in_scale=np.ones(10), out_shift=np.zeros(6),
+                      out_scale=np.full(6, 1e-3))
+        f.timestep(args.warmup)
+        ms, _, _ = timed_steps(torch, f, args.steps)
+        _, _, prof = timed_steps(torch, f, 2, profile=True)
+        out[name] = {"ms_per_step": ms / args.steps, "status": f.status(),
+                     "kernels_ms": {k: v[1] / max(v[0], 1) for k, v in (prof or {}).items()}}
+        f.close()
+        if net is not None:
+            net.close()
+    line = {"metric": "LES step time at 128x65x128 (C4 LES grid)", "value": out["learned"]["ms_per_step"],
+            "unit": "ms/step", "higher_is_better": False, "n_gpus": 1, "dtype": "f32 (bf16 network)",
+            "data": "synthetic (seeded field, random network)", "config": {"workload": "LES 128x65x128, Re "
+                                                                           f"{args.les_re:g}"}, "result": out}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_les(args):
     """Configuration C4: the learned-closure LES against plain GPU DNS."""
     import importlib
@@ -449,7 +531,8 @@ def run_les(args):
     t0 = time.time()
     out = lc.run_c4(nx=args.les_nx, ny=args.les_ny, nz=args.les_nx, re=args.les_re, spinup=args.les_spinup,
                     nsnap=args.les_nsnap, train_iters=args.les_train_iters, les_spin=args.les_time / 2,
-                    les_avg=args.les_time / 2, log=lambda m: print(m, file=sys.stderr, flush=True))
+                    les_avg=args.les_time / 2, beta=args.les_beta, artifact=args.les_artifact,
+                    log=lambda m: print(m, file=sys.stderr, flush=True))
     learned = out["les"]["learned"]
     line = {"metric": "NN-LES speedup at equal U+ error (C4)",
             "value": out["speedup_per_time_unit"]["learned"], "unit": "x (DNS ms per time unit / LES ms per time unit)",
@@ -502,7 +585,7 @@ def run_ours(args):
         _, _, prof = timed_steps(torch, flow, kp, profile=True)
         results[prec_name] = {"ms_total": ms_max, "launches": sum_over_ranks(nlaunch), "prof": prof, "tiles": tiles,
                               "prof_steps": kp, "clocks": cl, "status": st, "div": div, "q": q}
-        if prec_name == "mixed":
+        if prec_name == "mixed" and not args.no_e2e:
             # end to end through the public API with host buffers: every step
             # uploads data1/data2/data4 from pinned host memory, advances one
             # step and downloads data1/data2/data4 (a host-owned state).
@@ -530,9 +613,9 @@ def run_ours(args):
     # the same e2e with two domains whose host round trips overlap (two host
     # threads); every rank does the same
     ke = max(1, min(K, args.e2e_steps))
-    ms_ov, nb_ov = e2e_overlapped(torch, cf, nx, ny, nz, dev, ke)
+    ms_ov, nb_ov = e2e_overlapped(torch, cf, nx, ny, nz, dev, ke) if not args.no_e2e else (float("nan"), 0)
     ms_ov = max_over_ranks(ms_ov)
-    results["e2e_overlapped"] = {
+    results["e2e_overlapped"] = None if args.no_e2e else {
         "value": throughput(world, 2 * units, ke, ms_ov), "unit": UNIT,
         "h2d_bytes_per_step": nb_ov, "d2h_bytes_per_step": nb_ov,
         "how": "two independent domains per GPU, one host thread each, every domain step uploads, steps and "
@@ -650,6 +733,11 @@ def main():
     ap.add_argument("--arnoldi", action="store_true", help="configuration C3 (Arnoldi eigenvalues)")
     ap.add_argument("--arnoldi-maxiter", type=int, default=6, help="Krylov-Schur cycles of the C3 run")
     ap.add_argument("--les", action="store_true", help="configuration C4 (learned-closure LES vs DNS)")
+    ap.add_argument("--mlp", action="store_true", help="the closure network's tensor-core kernels alone")
+    ap.add_argument("--mlp-points", type=int, default=2400000)
+    ap.add_argument("--mlp-batch", type=int, default=65536)
+    ap.add_argument("--les-step", action="store_true", help="LES step times at the C4 LES grid")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end legs (profiling runs)")
     ap.add_argument("--les-nx", type=int, default=384)
     ap.add_argument("--les-ny", type=int, default=193)
     ap.add_argument("--les-re", type=float, default=10350.0)
@@ -657,6 +745,8 @@ def main():
     ap.add_argument("--les-nsnap", type=int, default=40)
     ap.add_argument("--les-train-iters", type=int, default=3000)
     ap.add_argument("--les-time", type=float, default=40.0)
+    ap.add_argument("--les-beta", type=float, default=0.0, help="admitted backscatter of the learned closure")
+    ap.add_argument("--les-artifact", default=None, help="save the a-posteriori inputs (.npz) here")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -670,6 +760,10 @@ def main():
         return run_arnoldi(args)
     if args.les:
         return run_les(args)
+    if args.mlp:
+        return run_mlp(args)
+    if args.les_step:
+        return run_les_step(args)
     return run_ours(args)
 
 

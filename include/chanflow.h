@@ -382,9 +382,10 @@ void cfg_ensemble_destroy(cfg_ensemble *e);
 
 /* Learned subgrid-stress closure network (the LES mode of the reference's
  * subgrid = 1 runs, PFC/main_mpi.f90:10-13,74-78, whose modules are not in
- * the reference): a perceptron 10 -> 64 -> 64 -> 64 -> 6 with GELU on the
- * hidden layers, BF16 weights and activations and FP32 accumulation on the
- * sm_100 tensor cores (tcgen05, accumulators in tensor memory).  Inputs per
+ * the reference): a perceptron 10 -> 64 -> 64 -> 64 -> 6 with GELU (tanh
+ * form, hardware tanh) on the hidden layers, BF16 weights and activations
+ * and FP32 accumulation on the sm_100 tensor cores (tcgen05, accumulators in
+ * tensor memory).  Inputs per
  * point: the 9 resolved velocity-gradient components and the wall distance,
  * normalised by the caller; outputs: the 6 subgrid-stress components
  * (11, 22, 33, 12, 13, 23), normalised.

@@ -2,7 +2,7 @@
 INFRASTRUCTURE ONLY: the checker of the tensor-core kernels of
 3d-navier-stokes-thesis-paper_b200/csrc/mlp.cu (forward, backward, Adam).
 
-The network: 10 -> 64 -> 64 -> 64 -> 6, GELU (the erf form) on the hidden
+The network: 10 -> 64 -> 64 -> 64 -> 6, GELU (tanh form) on the hidden
 layers, y = W x + b per layer; parameters as one flat FP32 vector
 W0[64][10] b0[64] W1[64][64] b1[64] W2[64][64] b2[64] W3[6][64] b3[6].
 Loss: the mean over the batch and the 6 outputs of (y - t)^2.
@@ -46,15 +46,17 @@ def bf16(a):
     return u.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
-_erf = np.vectorize(math.erf, otypes=[np.float64])
+C_GELU, A_GELU = math.sqrt(2.0 / math.pi), 0.044715
 
 
 def gelu(z):
-    return 0.5 * z * (1.0 + _erf(z / math.sqrt(2.0)))
+    """GELU in its tanh form (Hendrycks & Gimpel 2016), exact tanh."""
+    return 0.5 * z * (1.0 + np.tanh(C_GELU * (z + A_GELU * z ** 3)))
 
 
 def gelu_d(z):
-    return 0.5 * (1.0 + _erf(z / math.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / math.sqrt(2.0 * math.pi)
+    t = np.tanh(C_GELU * (z + A_GELU * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * C_GELU * (1.0 + 3.0 * A_GELU * z * z)
 
 
 def init_params(seed=0):

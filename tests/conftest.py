@@ -34,3 +34,23 @@ def has_gpu():
         return torch.cuda.is_available()
     except Exception:
         return False
+
+
+import contextlib  # noqa: E402
+
+
+@contextlib.contextmanager
+def whole_velocity_transforms(on=True):
+    """Contexts created inside keep the whole velocity (mean included) in the
+    FP32 transforms, as multi-rank runs do, instead of the single-context
+    mean split (CHANFLOW_NO_MEAN_SPLIT is read at cfg_create)."""
+    old = os.environ.get("CHANFLOW_NO_MEAN_SPLIT")
+    if on:
+        os.environ["CHANFLOW_NO_MEAN_SPLIT"] = "1"
+    try:
+        yield
+    finally:
+        if old is None:
+            os.environ.pop("CHANFLOW_NO_MEAN_SPLIT", None)
+        else:
+            os.environ["CHANFLOW_NO_MEAN_SPLIT"] = old

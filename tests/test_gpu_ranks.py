@@ -12,6 +12,8 @@ import socket
 import numpy as np
 import pytest
 
+from conftest import whole_velocity_transforms
+
 pytestmark = pytest.mark.gpu
 
 
@@ -61,7 +63,8 @@ def test_two_processes_match_single_context(cf, tmp_path, prec, dt_flag, ordered
     import multiprocessing as mp
     grid = cf.Grid(32, 33, 32, stretch=1.5)
     d1 = cf.initial_field(grid, 10, seed=11, ampl=5e-2)
-    f = cf.ChannelFlow(grid, re=2500.0, dt=0.004, precision=prec, dt_flag=dt_flag)
+    with whole_velocity_transforms():   # as the ranks of a multi-rank run
+        f = cf.ChannelFlow(grid, re=2500.0, dt=0.004, precision=prec, dt_flag=dt_flag)
     f.upload_state(d1, d1.transpose(2, 3, 0, 1).copy(), None)
     f.remove_initial_divergence()
     f.compute_initial_pressure()
