@@ -593,8 +593,9 @@ struct Impl {
       if (cfg_mlp_forward(c->les_mlp, c->les_F, c->les_Y, (long long)c->les_points, c->st) != CFG_OK)
         return fail(c, CFG_E_CUDA, "closure network launch");
       c->launches++;
+      prof_end(c);
       prof_begin(c, "k_les_blend");
-      k_les_blend<T><<<gr, 128, 0, c->st>>>((const T*)c->P, (T*)c->les_S, c->les_Y, g, c->gd, c->les, c->d_um_dy,
+      k_les_blend<T><<<gr, 128, 0, c->st>>>(c->les_F, (T*)c->les_S, c->les_Y, g, c->gd, c->les, c->d_um_dy,
                                             c->les_nfall);
       CKL();
     }

@@ -108,18 +108,29 @@ __global__ void __launch_bounds__(128) k_les_sgs(const T* __restrict__ P, T* __r
 
 // model 2: the network's stresses Y[(k-2) nz2 nx2 + z nx2 + x][6] where they
 // pass the checks, the eddy viscosity's (already in S) elsewhere; counts the
-// fallbacks into *nfall.  Same grid as k_les_sgs.
+// fallbacks into *nfall.  The gradient comes back from the features F (the
+// normalisation and the mirroring undone), not from the planes.  Same grid
+// as k_les_sgs.
 template <typename T>
-__global__ void __launch_bounds__(128) k_les_blend(const T* __restrict__ P, T* __restrict__ S, const float* __restrict__ Y,
-                                                   Geom g, GridDev gd, LesDev les, const double* __restrict__ d_um_dy,
+__global__ void __launch_bounds__(128) k_les_blend(const float* __restrict__ F, T* __restrict__ S,
+                                                   const float* __restrict__ Y, Geom g, GridDev gd, LesDev les,
+                                                   const double* __restrict__ d_um_dy,
                                                    unsigned long long* __restrict__ nfall) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x, z = blockIdx.y, k = 2 + blockIdx.z;
   bool fall = false;
   if (x < g.nx2) {
+    const size_t pt = ((size_t)(k - 2) * g.nz2 + z) * g.nx2 + x;
+    const float* f = F + pt * 10;
+    const double sgn = gd.yh[k - 1] > 0.0 ? -1.0 : 1.0;
     double G[9], Sd[6];
-    les_gradient<T>(P, g, gd, les, k, z, x, G);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) G[i] = (double)f[i] * les.in_scale[i] + les.in_shift[i];
+    G[1] *= sgn;
+    G[3] *= sgn;
+    G[5] *= sgn;
+    G[7] *= sgn;
     const double nut = les_strain_nut(G, gd, les, d_um_dy, g.ny, k, Sd);
-    const float* y = Y + (((size_t)(k - 2) * g.nz2 + z) * g.nx2 + x) * 6;
+    const float* y = Y + pt * 6;
     double t[6];
 #pragma unroll
     for (int c = 0; c < 6; ++c) t[c] = les.out_shift[c] + les.out_scale[c] * (double)y[c];

@@ -8,7 +8,6 @@
 //     sides); every solve multiplies by reciprocals;
 //   - the outputs are staged in shared memory and stored coalesced.
 #pragma once
-#include "bulk.cuh"
 #include "cfd_common.cuh"
 #include "pass1.cuh"
 #include "pass1_reg.cuh"
@@ -157,18 +156,6 @@ __device__ __forceinline__ cplx_t<T> d2c_t(const cplx_t<T>* s, const T* __restri
 // even (16-byte aligned columns for FP32 complex)
 __host__ __device__ __forceinline__ int rhs2_ld(int n1) { return (n1 + 1) & ~1; }
 
-// Whether a launch stages and writes its columns with bulk copies: storage in
-// the arithmetic precision, columns contiguous (ld == n1) of a multiple of 16
-// bytes.
-template <typename T, typename S>
-__host__ __device__ __forceinline__ bool rhs2_bulk(int n1, int ld) {
-#if defined(CFD_NO_BULK_RHS2)
-  return false;
-#else
-  return sizeof(S) == sizeof(T) && ld == n1 && (n1 * (int)sizeof(cplx_t<T>)) % 16 == 0;
-#endif
-}
-
 // Shared memory per wavenumber: eight columns
 //   0-2 cru (u,v,w), overwritten by the new velocity cv;  3 pressure;
 //   4 pressure correction;  5-7 nonlinear term, overwritten by the next cru.
@@ -207,24 +194,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 5 : 1) k_rhs2(cplx_t<S>*
   CS* gprs = prs + (size_t)w * n1;
 
   // ---- asynchronous staging of the seven input columns: cru (u,v,w), p, NL (u,v,w)
-  // Storage = arithmetic precision with contiguous 16-byte columns: three
-  // bulk copies per wavenumber (cru, p, NL; the three components of a field
-  // are adjacent in memory) issued by the group's first lane and completed
-  // on the group's mbarrier.
-  __shared__ __align__(8) uint64_t s_bar[8];
-  if (valid && rhs2_bulk<T, S>(n1, LD)) {
-    const int gidx = warp * GPW + grp, colb = (int)(n1 * sizeof(C));
-    const unsigned gmask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << (grp * G));
-    if (gl == 0) {
-      bar_init(&s_bar[gidx], 1);
-      bar_expect_tx(&s_bar[gidx], (uint32_t)(7 * colb));
-      bulk_load(S_, gcru, 3 * colb, &s_bar[gidx]);
-      bulk_load(S_ + 3 * LD, gprs, colb, &s_bar[gidx]);
-      bulk_load(S_ + 5 * LD, gvel, 3 * colb, &s_bar[gidx]);
-    }
-    __syncwarp(gmask);
-    if (!bar_wait(&s_bar[gidx], 0)) atomicExch(&const_cast<DevScalars*>(sc)->status, -6);
-  } else if (valid && sizeof(S) != sizeof(T)) {
+  if (valid && sizeof(S) != sizeof(T)) {
     // widening copy (mixed storage, FP64 arithmetic)
 #pragma unroll
     for (int col = 0; col < 7; ++col) {
@@ -444,19 +414,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 5 : 1) k_rhs2(cplx_t<S>*
     }
   }
   __syncwarp();
-  if (valid && rhs2_bulk<T, S>(n1, LD)) {
-    // the outputs as three bulk stores: data1 <- cv, data2 <- accumulator, data4 <- p
-    const int colb = (int)(n1 * sizeof(C));
-    const unsigned gmask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << (((threadIdx.x & 31) / G) * G));
-    fence_proxy_async();
-    __syncwarp(gmask);
-    if (gl == 0) {
-      bulk_store(gvel, sV, 3 * colb);
-      bulk_store(gcru, (rk < 3) ? sN : sV, 3 * colb);
-      bulk_store(gprs, sP, colb);
-      bulk_commit_wait();
-    }
-  } else if (valid) {
+  if (valid) {
     const C* acc = (rk < 3) ? sN : sV;
     for (int q = 0; q < 3; ++q)
       for (int j = gl; j < n1; j += G) {

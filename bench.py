@@ -547,6 +547,87 @@ def run_les(args):
     return 0
 
 
+def pinned_state(torch, flow):
+    """Pinned host copies of the flow's data1, data2, data4 (reference
+    layouts, interleaved complex FP64) filled with its current state."""
+    s1, s2, s4 = flow.shapes()
+    pin = [torch.empty(int(np.prod(s)) * 2, dtype=torch.float64, pin_memory=True) for s in (s1, s2, s4)]
+    d1, d2, d4 = flow.download_state()
+    for t, a in zip(pin, (d1, d2, d4)):
+        t.numpy()[:] = np.asfortranarray(a).ravel(order="F").view(np.float64)
+    return pin
+
+
+def host_round_trip_steps(flow, ptr, n):
+    """n steps of a host-owned state through the C ABI: upload data1, data2,
+    data4 from pinned host memory, one time step, download them again."""
+    L = flow.L
+    for _ in range(n):
+        flow._chk(L.cfg_upload_state(flow.h, ptr[0], ptr[1], ptr[2]))
+        flow.timestep(1)
+        flow._chk(L.cfg_download_state(flow.h, ptr[0], ptr[1], ptr[2]))
+
+
+def e2e_overlapped(torch, cf, nx, ny, nz, dev, n):
+    """Two independent domains, each driven by its own host thread through
+    the same host round trip per step as the serial e2e: one domain's uploads
+    and downloads overlap the other's step and its copies in the other
+    direction (the C calls release the interpreter lock).  Device time from
+    events on both streams, first start to last end."""
+    import threading
+    flows = [make_flow(cf, nx, ny, nz, cf.MIXED, dev) for _ in range(2)]
+    pins = [pinned_state(torch, f) for f in flows]
+    streams = [torch.cuda.ExternalStream(f.stream_ptr()) for f in flows]
+    for f in flows:
+        host_round_trip_steps(f, [t.data_ptr() for t in pins[flows.index(f)]], 1)   # warm-up
+        f.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in flows]
+    for (e0, _), st in zip(ev, streams):
+        e0.record(st)
+    th = [threading.Thread(target=host_round_trip_steps, args=(f, [t.data_ptr() for t in pin], n))
+          for f, pin in zip(flows, pins)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    for (_, e1), st in zip(ev, streams):
+        e1.record(st)
+    for _, e1 in ev:
+        e1.synchronize()
+    ms = max(ev[0][0].elapsed_time(e1) for _, e1 in ev)
+    nbytes = sum(t.numel() * 8 for t in pins[0])
+    for f in flows:
+        f.close()
+    return ms, nbytes
+
+
+def error_vs_fp64(cf, nx, ny, nz, dev, steps):
+    """Relative L2 difference of the mixed-precision velocity (data1) from
+    the FP64 path's after `steps` steps from the same seeded initial field:
+    over the whole field and over its perturbation (every Fourier column
+    except the kx = kz = 0 mean), with the change of the FP64 field over the
+    run beside them."""
+    a = make_flow(cf, nx, ny, nz, cf.FP64, dev)
+    b = make_flow(cf, nx, ny, nz, cf.MIXED, dev)
+    d0 = a.download_state()[0]
+    a.timestep(steps)
+    b.timestep(steps)
+    da, db = a.download_state()[0], b.download_state()[0]
+    st = (a.status(), b.status())
+    a.close()
+    b.close()
+
+    def rel(x, y):
+        return float(np.linalg.norm(x - y) / np.linalg.norm(y))
+
+    pa, pb, p0 = da.copy(), db.copy(), d0.copy()
+    for arr in (pa, pb, p0):
+        arr[0, 0] = 0
+    return {"steps": steps, "whole_field": rel(db, da), "perturbation": rel(pb, pa),
+            "fp64_change_whole": rel(da, d0), "fp64_change_perturbation": rel(pa, p0), "status": list(st),
+            "field": "data1 (u, v, w), relative L2; perturbation = all columns but kx = kz = 0"}
+
+
 def run_ours(args):
     import torch
     import __graft_entry__
@@ -566,7 +647,7 @@ def run_ours(args):
         flow = make_flow(cf, nx, ny, nz, prec, dev)
         # launch tiles tuned on this grid (outside the timed region; the
         # state is restored, results do not depend on the tiles)
-        tiles = flow.autotune(3)
+        tiles = flow.autotune(3) if not args.no_autotune else None
         clocks = Clocks(dev) if prec_name == "mixed" else None
         flow.timestep(W)
         flow.synchronize()
@@ -688,7 +769,7 @@ def run_ours(args):
             "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 (f64 mean mode and |k|<4 solves)", "data": "synthetic (seeded initial field)",
             "config": dict(workload_config(nx, ny, nz, "mixed"),
-                           tiles={k: list(v["tiles"]) for k, v in results.items() if "tiles" in v}),
+                           tiles={k: list(v["tiles"]) for k, v in results.items() if v and v.get("tiles")}),
             "roofline": best,
             "roofline_step": {"bound": "hbm", "achieved": step_bytes / (ms_step / 1e3) / 1e9, "peak": hbm,
                               "unit": "GB/s", "frac": step_bytes / (ms_step / 1e3) / 1e9 / hbm,
@@ -738,6 +819,7 @@ def main():
     ap.add_argument("--mlp-batch", type=int, default=65536)
     ap.add_argument("--les-step", action="store_true", help="LES step times at the C4 LES grid")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end legs (profiling runs)")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default tiles (profiling runs)")
     ap.add_argument("--les-nx", type=int, default=384)
     ap.add_argument("--les-ny", type=int, default=193)
     ap.add_argument("--les-re", type=float, default=10350.0)

@@ -65,3 +65,25 @@ def test_throughput_is_whole_job_on_the_slowest_rank():
     import bench
     # 4 replicas of 12.648 Mpts, 10 steps, slowest rank 36 ms
     assert abs(bench.throughput(4, 12.648, 10, 36.0) - 4 * 12.648 * 10 / 0.036) < 1e-9
+
+
+def test_bench_functions_resolve_their_globals():
+    """Every global name a function of bench.py reads is defined at module
+    level or a builtin (a function lost in an edit fails here, not on a GPU)."""
+    import builtins
+    import symtable
+    path = os.path.join(ROOT, "bench.py")
+    top = symtable.symtable(open(path).read(), path, "exec")
+    defined = {s.get_name() for s in top.get_symbols() if s.is_assigned() or s.is_imported()}
+    missing = []
+
+    def walk(t):
+        for ch in t.get_children():
+            for s in ch.get_symbols():
+                name = s.get_name()
+                if s.is_global() and s.is_referenced() and name not in defined and not hasattr(builtins, name):
+                    missing.append((ch.get_name(), name))
+            walk(ch)
+
+    walk(top)
+    assert not missing, missing

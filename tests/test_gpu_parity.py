@@ -97,8 +97,9 @@ def test_config_c1_100_steps(cf, orc, prec, tol, ptol):
     """Config C1: 32x33x32, Re 2500, stretch 1.5, laminar + 1e-3 k^-2 noise,
     constant flux, dt 0.005, 100 steps.  The perturbation (every Fourier
     column but the mean) is gated on its own: FP64 1e-10 (measured on a B200
-    2.6e-14), mixed 3e-5 (measured 5.6e-6; FP32 transforms carry the mean
-    with the noise, see test_gpu_metric_config.py)."""
+    2.6e-14), mixed 3e-5 (measured 5.6e-6 with the whole velocity in the FP32
+    transforms; the mean split keeps it lower, see
+    test_gpu_metric_config.py)."""
     grid, flow, o = make(cf, orc, 32, 33, 32, prec=prec)
     o.init_field(10, seed=1, ampl=1e-3)
     flow.define_initial_field(10, seed=1, ampl=1e-3)
