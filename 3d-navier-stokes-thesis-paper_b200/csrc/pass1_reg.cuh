@@ -686,6 +686,15 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT
       Bp[q] = (T)gd.baseflow[q * (ny + 1) + k];
     }
   }
+  // the mean's half sums onto the y planes k-1 and k and its iu-weighted
+  // values (mean split)
+  T hBm[3], hBp[3], iuB[3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    hBm[q] = half * (Bm[q] + B0[q]);
+    hBp[q] = half * (B0[q] + Bp[q]);
+    iuB[q] = iu1 * B0[q] + iu2 * Bp[q];
+  }
   // rows of planes k-1 (index k-2), k, k+1 for component c and row r
   const size_t pstride = (size_t)3 * NZ2 * N;
   const T* Pm = P + (size_t)(k - 2) * pstride + (size_t)z0 * N;
@@ -698,7 +707,18 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT
   // then 12, 23 at plane k-1 and 12, 22, 23 at plane k+1
   auto point = [&](T U, T V, T W, T Up, T Vp, T Wp, T Um, T Vm, T Wm, T fr, int r, int x, const T* tau) {
   T fpu0 = 0, fpw0 = 0, fpu = 0, fpw = 0, xfu = 0, zfu = 0, xfw = 0, zfw = 0;
-  if (!LIN) {
+  if (SPLIT) {
+    // (B + u)(B + u) - B B factored: the fluctuation's products and the
+    // mean's in one pass (block constants hold the mean's half sums)
+    if (k == 2) { fpu0 = (Vm + Bm[1]) * Um + Vm * Bm[0]; fpw0 = (Vm + Bm[1]) * Wm + Vm * Bm[2]; }
+    else { fpu0 = (Vm + Bm[1]) * (half * (Um + U)) + Vm * hBm[0]; fpw0 = (Vm + Bm[1]) * (half * (Wm + W)) + Vm * hBm[2]; }
+    if (k < ny) { fpu = (V + B0[1]) * (half * (U + Up)) + V * hBp[0]; fpw = (V + B0[1]) * (half * (W + Wp)) + V * hBp[2]; }
+    else { fpu = (V + B0[1]) * Up + V * Bp[0]; fpw = (V + B0[1]) * Wp + V * Bp[2]; }
+    xfu = U * (U + two * B0[0]);
+    zfu = U * (W + B0[2]) + W * B0[0];
+    xfw = zfu;
+    zfw = W * (W + two * B0[2]);
+  } else if (!LIN) {
     if (k == 2) { fpu0 = Vm * Um; fpw0 = Vm * Wm; }
     else { fpu0 = Vm * half * (Um + U); fpw0 = Vm * half * (Wm + W); }
     if (k < ny) { fpu = V * half * (U + Up); fpw = V * half * (W + Wp); }
@@ -711,7 +731,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT
       if (k < ny) { fpu += half * (tau[3] + tau[8]); fpw += half * (tau[5] + tau[10]); }
     }
   }
-  if (HASB) {
+  if (LIN) {
     if (k == 2) { fpu0 += Bm[1] * Um + Vm * Bm[0]; fpw0 += Bm[1] * Wm + Vm * Bm[2]; }
     else {
       fpu0 += Bm[1] * half * (Um + U) + Vm * half * (Bm[0] + B0[0]);
@@ -734,7 +754,13 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT
   T xfv = 0, dyv = 0, zfv = 0;
   if (veq) {
     T fp0 = 0, fp = 0;
-    if (!LIN) {
+    if (SPLIT) {
+      const T t0 = half * (Vm + V), t1 = half * (V + Vp);
+      fp0 = t0 * (t0 + two * hBm[1]);
+      fp = t1 * (t1 + two * hBp[1]);
+      xfv = (V + B0[1]) * (iu1 * U + iu2 * Up) + V * iuB[0];
+      zfv = (V + B0[1]) * (iu1 * W + iu2 * Wp) + V * iuB[2];
+    } else if (!LIN) {
       const T t0 = half * (Vm + V), t1 = half * (V + Vp);
       fp0 = t0 * t0; fp = t1 * t1;
       xfv = V * (iu1 * U + iu2 * Up);
@@ -746,7 +772,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT
         fp += tau[9];
       }
     }
-    if (HASB) {
+    if (LIN) {
       const T t0 = half * (Vm + V), b0v = half * (Bm[1] + B0[1]);
       const T t1 = half * (V + Vp), b1v = half * (B0[1] + Bp[1]);
       fp0 += two * t0 * b0v; fp += two * t1 * b1v;

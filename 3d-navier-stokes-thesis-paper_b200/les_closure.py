@@ -307,7 +307,8 @@ def run_c4(nx=384, ny=193, nz=384, factor=3, re=10350.0, stretch=1.5, ampl=0.5, 
         f"eddy viscosity {out['a_priori']['ev_deviatoric_rel_err']:.3f}")
     if artifact:
         # what the a-posteriori runs need, to rerun them without the DNS
-        np.savez_compressed(artifact, state=states[0], Uf=Uf, Rf=Rf, params=net.get_params(), mi=mi, si=si, mo=mo,
+        np.savez_compressed(artifact, state=states[0].astype(np.complex64), Uf=Uf, Rf=Rf, params=net.get_params(),
+                            mi=mi, si=si, mo=mo,
                             so=so, grid=np.array([gl.nx, gl.ny, gl.nz]), stretch=stretch, re=re,
                             dns_ms_per_time_unit=out["dns"]["ms_per_time_unit"])
     out["les"] = les_runs(gl, re, states[0], Uf, Rf, net, (mi, si, mo, so), cfl, les_spin, les_avg, cs, beta,
@@ -377,7 +378,8 @@ def les_from_artifact(path, device=0, log=print, **kw):
     gl = Grid(nx, ny, nz, lx=4 * np.pi, lz=2 * np.pi, stretch=float(a["stretch"]))
     net = Mlp(device, a["params"])
     try:
-        les = les_runs(gl, float(a["re"]), a["state"], a["Uf"], a["Rf"], net, (a["mi"], a["si"], a["mo"], a["so"]),
+        les = les_runs(gl, float(a["re"]), np.asfortranarray(a["state"].astype(np.complex128)), a["Uf"], a["Rf"], net,
+                       (a["mi"], a["si"], a["mo"], a["so"]),
                        device=device, log=log, **kw)
     finally:
         net.close()
