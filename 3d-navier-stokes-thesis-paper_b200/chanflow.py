@@ -191,6 +191,8 @@ SYMBOLS = {
     "cfg_ensemble_timestep": (C.c_int, [_VP, C.c_int]),
     "cfg_ensemble_synchronize": (C.c_int, [_VP]),
     "cfg_ensemble_stream": (_VP, [_VP]),
+    "cfg_ensemble_set_batched": (C.c_int, [_VP, C.c_int]),
+    "cfg_ensemble_batched": (C.c_int, [_VP]),
     "cfg_ensemble_destroy": (None, [_VP]),
     "cfg_rank_record_size": (C.c_size_t, []),
     "cfg_rank_create": (C.c_int, [C.POINTER(CfgParams), C.POINTER(CfgGrid), C.c_int, C.c_int, C.POINTER(_VP)]),
@@ -1058,10 +1060,13 @@ class Ensemble:
     """cfg_ensemble: independent ChannelFlow members on one GPU advanced
     together, one CUDA graph launch per step after the first (configuration
     C5: many grids, Reynolds numbers, seeds and forcings).  autotune tunes the
-    tiles once per distinct grid.  Call synchronize() before reading a
+    tiles once per distinct grid.  batched: None keeps the library's default
+    (batched when every member allows it), True requires the batched layout
+    (one launch per kernel per class of equal grids, over a member table),
+    False one graph branch per member.  Call synchronize() before reading a
     member."""
 
-    def __init__(self, members, autotune=True):
+    def __init__(self, members, autotune=True, batched=None):
         self.L = load_library()
         self.members = list(members)
         hs = (C.c_void_p * len(self.members))(*[m.h.value for m in self.members])
@@ -1072,6 +1077,15 @@ class Ensemble:
             msg = self.L.cfg_last_error(self.members[0].h)
             raise ChanflowError(f"cfg_ensemble_create failed ({ERRORS.get(r, r)}): {msg.decode() if msg else ''}")
         self.h = h
+        if batched is not None:
+            r = self.L.cfg_ensemble_set_batched(self.h, 1 if batched else 0)
+            if r != 0:
+                self.close()
+                raise ChanflowError(f"cfg_ensemble_set_batched failed ({ERRORS.get(r, r)})")
+
+    @property
+    def batched(self):
+        return bool(self.L.cfg_ensemble_batched(self.h))
 
     def timestep(self, nsteps=1):
         r = self.L.cfg_ensemble_timestep(self.h, nsteps)

@@ -483,6 +483,29 @@ struct Impl {
     return CFG_OK;
   }
 
+  // the launch record of register-FFT pass-1 kernel `which` (0 k_zinv_r, 1
+  // k_xflux_r, 2 k_zfwd_r, 3 k_xinv_r, 4 k_flux_r) in substep rk
+  static P1Launch p1_args(const cfg_ctx* c, int rk, bool lin, int which) {
+    const Geom& g = c->g;
+    P1Launch a{};
+    a.vel = c->vel; a.T1 = c->T1; a.T2 = c->T2; a.velout = c->vel; a.g = g; a.twx = c->twx; a.twz = c->twz;
+    a.gd = c->gd; a.fringe = c->fringe; a.has_fringe = c->has_fringe; a.YB1 = c->fYB1; a.YB3 = c->fYB3;
+    a.ZR = c->fZR; a.cflbits = c->cflbits; a.do_cfl = (rk == 1); a.lin = lin ? 1 : 0; a.st = c->st;
+    a.KC = (int)std::max(2L, std::min(16L, (long)(g.ny - 1) * (g.nz2 / c->fZR) / 592));
+    a.P = c->P;
+    a.FZR = c->flux_zr;
+    a.sc = c->scat;
+    a.split = (c->mean_split && !lin && !c->les_on) ? 1 : 0;
+    if (which == 3 || which == 4) {
+      // x stage of the split path on this rank's z2 rows, all kx
+      a.g = c->gP;
+      a.gd = c->gd_all;
+      if (c->fringe) a.fringe = (const T*)c->fringe + (size_t)c->z0s * g.nx2;
+      if (which == 4 && a.split) a.gd.baseflow = c->mean_base;
+    }
+    return a;
+  }
+
   // nonlinear (PFC/pass1.f90:26-124) in three phases; a multi-rank run puts
   // a barrier between them: 1 the inverse z transform, scattered to the z2
   // slabs; 2 the x stage (inverse x, fluxes, forward x), scattered to the kx
@@ -491,15 +514,7 @@ struct Impl {
     const Geom& g = c->g;
     const int do_cfl = (rk == 1);
     const bool f32 = sizeof(T) == 4;
-    P1Launch a{};
-    a.vel = c->vel; a.T1 = c->T1; a.T2 = c->T2; a.velout = c->vel; a.g = g; a.twx = c->twx; a.twz = c->twz;
-    a.gd = c->gd; a.fringe = c->fringe; a.has_fringe = c->has_fringe; a.YB1 = c->fYB1; a.YB3 = c->fYB3;
-    a.ZR = c->fZR; a.cflbits = c->cflbits; a.do_cfl = do_cfl; a.lin = lin ? 1 : 0; a.st = c->st;
-    a.KC = (int)std::max(2L, std::min(16L, (long)(g.ny - 1) * (g.nz2 / c->fZR) / 592));
-    a.P = c->P;
-    a.FZR = c->flux_zr;
-    a.sc = c->scat;
-    a.split = (c->mean_split && !lin && !c->les_on) ? 1 : 0;
+    P1Launch a = p1_args(c, rk, lin, 0);
     if (phase == 1) {
       if (a.split) {
         // the current mean velocity (the FP64 side copy when it holds it)
@@ -523,19 +538,16 @@ struct Impl {
     if (phase == 2) {
       dim3 g2(g.nz2 / c->ZR, (g.ny - 1 + c->KC - 1) / c->KC);
       if (c->split_x) {
-        // x stage on this rank's z2 rows, all kx
-        a.g = c->gP;
-        a.gd = c->gd_all;
-        if (c->fringe) a.fringe = (const T*)c->fringe + (size_t)c->z0s * g.nx2;
+        a = p1_args(c, rk, lin, 3);
         prof_begin(c, "k_xinv");
         if (p1_fast_launch(3, g.nx2, f32, a) != 0) return fail(c, CFG_E_CUDA, "k_xinv_r launch");
         CKL();
+        a = p1_args(c, rk, lin, 4);
         if (c->les_on && !lin) {
           const int r = les_stresses(c, c->les_F);
           if (r) return r;
           a.sgs = c->les_S;
         }
-        if (a.split) a.gd.baseflow = c->mean_base;
         prof_begin(c, "k_flux");
         if (p1_fast_launch(4, g.nx2, f32, a) != 0) return fail(c, CFG_E_CUDA, "k_flux_r launch");
       } else if (c->fast_x) {
@@ -619,6 +631,36 @@ struct Impl {
     return les_stresses(c, F);
   }
 
+  // launch records of k_rhs2: the fast list (storage precision) or, prec,
+  // the mixed path's |k| < 4 list in FP64 on the side stream st2
+  static Rhs2Launch rhs2_args(const cfg_ctx* c, int rk, bool prec) {
+    const Geom& g = c->g;
+    Rhs2Launch a{};
+    a.vel = c->vel; a.cru = c->cru; a.prs = c->prs;
+    a.cbc_top = (const C*)c->cbc + 3 * (size_t)g.nw; a.cbc_bot = c->cbc;
+    a.g = g; a.gd = c->gd; a.sc = c->sc; a.rkt = c->rkt; a.rk = rk; a.re = c->p.re;
+    if (prec) {
+      a.wlist = c->wl_prec; a.nlist = c->n_prec; a.warps = 1; a.lanes = 32; a.tbl = c->rhs2_tbl64;
+      a.st = c->st2;
+    } else {
+      a.wlist = c->wl_fast; a.nlist = c->n_fast; a.warps = c->rhs2_warps; a.lanes = c->rhs2_lanes;
+      a.tbl = c->rhs2_tbl;
+      a.st = c->st;
+    }
+    return a;
+  }
+  // launch record of the mean mode (k_rhs_mean2) on the side stream st3
+  static RhsMeanLaunch mean_args(const cfg_ctx* c, int rk) {
+    const Geom& g = c->g;
+    RhsMeanLaunch m{};
+    m.vel = c->vel; m.cru = c->cru; m.prs = c->prs; m.mvel64 = c->mvel64; m.mcru64 = c->mcru64;
+    m.cbc_top = (const C*)c->cbc + 3 * (size_t)g.nw; m.cbc_bot = c->cbc;
+    m.g = g; m.gd = c->gd; m.sc = c->sc; m.d_um_dy = c->d_um_dy; m.rkt = c->rkt; m.rk = rk;
+    m.re = c->p.re; m.beta = c->p.beta; m.fix_mass = c->p.fix_mass; m.tbl64 = (const double*)c->rhs2_tbl64;
+    m.st = c->st3;
+    return m;
+  }
+
   template <int MM>
   static int rhs_m(cfg_ctx* c, int rk, int mode) {
     const Geom& g = c->g;
@@ -638,13 +680,7 @@ struct Impl {
       c->prof_stream = c->st2;
       prof_begin(c, "k_rhs_fp64");
       if (v2 && sizeof(T) == 4) {
-        Rhs2Launch a{};
-        a.vel = c->vel; a.cru = c->cru; a.prs = c->prs;
-        a.cbc_top = (const C*)c->cbc + 3 * (size_t)g.nw; a.cbc_bot = c->cbc;
-        a.g = g; a.gd = c->gd; a.sc = c->sc; a.rkt = c->rkt; a.rk = rk; a.re = c->p.re;
-        a.wlist = c->wl_prec; a.nlist = c->n_prec; a.warps = 1; a.lanes = 32; a.tbl = c->rhs2_tbl64;
-        a.st = c->st2;
-        if (rhs2_launch_prec(a) != 0) return fail(c, CFG_E_CUDA, "k_rhs2 (FP64 list) launch");
+        if (rhs2_launch_prec(rhs2_args(c, rk, true)) != 0) return fail(c, CFG_E_CUDA, "k_rhs2 (FP64 list) launch");
       } else {
         k_rhs<double, T, MM><<<c->n_prec, 32, c->sm_rhs64 / 4, c->st2>>>((C*)c->vel, (C*)c->cru, (C*)c->prs,
                                                                        (const C*)c->cbc + 3 * (size_t)g.nw,
@@ -659,13 +695,7 @@ struct Impl {
     if (g.kx0 != 0) {
       // the mean mode lives on the rank that holds kx = 0
     } else if (v2) {
-      RhsMeanLaunch m{};
-      m.vel = c->vel; m.cru = c->cru; m.prs = c->prs; m.mvel64 = c->mvel64; m.mcru64 = c->mcru64;
-      m.cbc_top = (const C*)c->cbc + 3 * (size_t)g.nw; m.cbc_bot = c->cbc;
-      m.g = g; m.gd = c->gd; m.sc = c->sc; m.d_um_dy = c->d_um_dy; m.rkt = c->rkt; m.rk = rk;
-      m.re = c->p.re; m.beta = c->p.beta; m.fix_mass = c->p.fix_mass; m.tbl64 = (const double*)c->rhs2_tbl64;
-      m.st = c->st3;
-      if (rhs_mean2_launch(sizeof(T) == 4, m) != 0) return fail(c, CFG_E_CUDA, "k_rhs_mean2 launch");
+      if (rhs_mean2_launch(sizeof(T) == 4, mean_args(c, rk)) != 0) return fail(c, CFG_E_CUDA, "k_rhs_mean2 launch");
     } else {
       k_rhs_mean<T, MM><<<1, 32, 0, c->st3>>>((C*)c->vel, (C*)c->cru, (C*)c->prs, c->mvel64, c->mcru64,
                                              (const C*)c->cbc + 3 * (size_t)g.nw, (const C*)c->cbc, g, c->gd, c->sc,
@@ -676,15 +706,8 @@ struct Impl {
     CK(cudaEventRecord(c->ev_join, c->st2));
     CK(cudaEventRecord(c->ev_join3, c->st3));
     if (c->n_fast > 0 && mode == 0 && c->use_rhs2) {
-      Rhs2Launch a{};
-      a.vel = c->vel; a.cru = c->cru; a.prs = c->prs;
-      a.cbc_top = (const C*)c->cbc + 3 * (size_t)g.nw; a.cbc_bot = c->cbc;
-      a.g = g; a.gd = c->gd; a.sc = c->sc; a.rkt = c->rkt; a.rk = rk; a.re = c->p.re;
-      a.wlist = c->wl_fast; a.nlist = c->n_fast; a.warps = c->rhs2_warps; a.lanes = c->rhs2_lanes;
-      a.tbl = c->rhs2_tbl;
-      a.st = c->st;
       prof_begin(c, "k_rhs");
-      if (rhs2_launch(sizeof(T) == 4, a) != 0) return fail(c, CFG_E_CUDA, "k_rhs2 launch");
+      if (rhs2_launch(sizeof(T) == 4, rhs2_args(c, rk, false)) != 0) return fail(c, CFG_E_CUDA, "k_rhs2 launch");
       CKL();
     } else if (c->n_fast > 0) {
       dim3 gr((c->n_fast + 3) / 4);
@@ -2652,8 +2675,135 @@ int cfg_set_tiles(cfg_ctx* c, const int* tiles) {
 // ---- ensembles: many independent contexts stepped by one graph ------------
 // Configuration C5: members of different grids, Reynolds numbers, seeds and
 // forcing on one GPU.  One time step of every member is captured once into a
-// CUDA graph (each member's work on its own branch, forked from and joined to
-// the ensemble stream), so a step of the whole ensemble is one graph launch.
+// CUDA graph, so a step of the whole ensemble is one graph launch.  Two ways
+// to lay the step out:
+//   batched (the default where every member allows it): the members fall
+//     into classes of the same grid and launch tiles, and every kernel of
+//     the step runs once per class -- blockIdx.x runs over the class's
+//     members, each member's arguments come from a table in device memory
+//     (the *_b kernels of pass1_fast.inc, pass2v2.cu and below) -- one
+//     branch of the graph per class;
+//   branches: each member's step on its own branch, forked from and joined
+//     to the ensemble stream.
+// The arithmetic is the same either way: the batched kernels run the same
+// bodies on the same arguments.
+
+// per-member arguments of the batched small kernels (mixed precision)
+struct EnsMember {
+  // substep prologue: the mean-split base and the CFL maxima
+  const double2* m64;
+  const float2* v32;
+  double* base;
+  int ny1, split;
+  unsigned long long* cflbits;
+  // boundary: the wall values, zeroed at every step
+  float2* cbc;
+  size_t ncbc;
+  // check_cfl and the dt update
+  Geom g;
+  GridDev gd;
+  DevScalars* sc;
+  double* cflp;
+  double lx, lz, cfl_max;
+  int dt_flag;
+};
+
+// per-member arguments of the batched wall jet (members with crossflow)
+struct EnsJet {
+  JetState* st;
+  JetParams jp;
+  const DevScalars* sc;
+  RkTab rkt;
+  float* phys;
+  float2 *H, *spec, *cbc;
+  GridDev gd;
+  FftPlan px, pz;
+  const float2 *twx, *twz;
+  int nx, nz, nxh;
+  size_t nw;
+  double lx, lz;
+};
+
+// k_mean_base and, at rk 1, the zeroed CFL maxima of every member; one block
+// per member
+__global__ void k_ens_prologue(const EnsMember* __restrict__ tab, int do_cfl) {
+  const EnsMember& a = tab[blockIdx.x];
+  const int n = 3 * a.ny1;
+  if (a.split)
+    for (int i = threadIdx.x; i < n; i += blockDim.x) a.base[i] = a.m64 ? a.m64[i].x : (double)a.v32[i].x;
+  if (do_cfl)
+    for (int i = threadIdx.x; i < n; i += blockDim.x) a.cflbits[i] = 0ull;
+}
+
+// the wall values zeroed (boundary without feedback); grid (blocks, members)
+__global__ void k_ens_zero_cbc(const EnsMember* __restrict__ tab) {
+  const EnsMember& a = tab[blockIdx.y];
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.ncbc; i += (size_t)gridDim.x * blockDim.x)
+    a.cbc[i] = make_float2(0.f, 0.f);
+}
+
+__global__ void k_cfl_finalize_b(const EnsMember* __restrict__ tab, int step) {
+  const EnsMember& a = tab[blockIdx.x];
+  k_cfl_finalize_body<false>(make_uint3(0, 0, 0), a.cflbits, a.g, a.gd, a.sc, a.cflp, a.lx, a.lz, a.dt_flag,
+                             a.cfl_max, step);
+}
+
+__global__ void k_ens_advance(const EnsMember* __restrict__ tab, int n) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m < n) tab[m].sc->t_total = tab[m].sc->t_total + tab[m].sc->dt;
+}
+
+__global__ void k_jet_walk_b(const EnsJet* __restrict__ tab, int rk) {
+  const EnsJet& a = tab[blockIdx.x];
+  k_jet_walk_body(make_uint3(0, 0, 0), a.st, a.jp, a.sc, a.rkt, rk, 0.0, 0.0, 1);
+}
+
+__global__ void k_jet_field_b(const EnsJet* __restrict__ tab, unsigned gx) {
+  const unsigned m = blockIdx.x / gx;
+  const EnsJet& a = tab[m];
+  k_jet_field_body<float>(make_uint3(blockIdx.x - m * gx, blockIdx.y, 0), a.phys, a.jp, a.st, a.nx, a.nz, a.lx,
+                          a.lz);
+}
+
+__global__ void k_px_fwd_b(const EnsJet* __restrict__ tab, unsigned gx) {
+  const unsigned m = blockIdx.x / gx;
+  const EnsJet& a = tab[m];
+  k_px_fwd_body<float>(make_uint3(blockIdx.x - m * gx, blockIdx.y, 0), a.phys, a.H, a.nxh, a.nz, a.nx, a.px, a.twx);
+}
+
+__global__ void k_pz_fwd_b(const EnsJet* __restrict__ tab, unsigned gx) {
+  const unsigned m = blockIdx.x / gx;
+  const EnsJet& a = tab[m];
+  const float scale = (float)(1.0 / ((double)a.nx * (double)a.nz));
+  k_pz_fwd_body<float>(make_uint3(blockIdx.x - m * gx, blockIdx.y, 0), a.H, a.spec, a.nw, (size_t)a.nz, 1, a.nxh,
+                       a.nz, a.nz, 0, scale, a.pz, a.twz);
+}
+
+__global__ void k_jet_combine_b(const EnsJet* __restrict__ tab, unsigned gx) {
+  const unsigned m = blockIdx.x / gx;
+  const EnsJet& a = tab[m];
+  k_jet_combine_body<float>(make_uint3(blockIdx.x - m * gx, 0, 0), a.spec, a.cbc, a.jp, a.gd, a.nx, a.nz, a.nxh,
+                            a.lx, a.lz);
+}
+
+// one class of a batched ensemble: members with the same grid and tiles
+struct EnsClass {
+  std::vector<int> mem, jet;   // member indices; those with the wall jet
+  cudaStream_t st = nullptr, st2 = nullptr, st3 = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_fork = nullptr, ev_j2 = nullptr, ev_j3 = nullptr, ev_done = nullptr;
+  void* dtab = nullptr;        // every table below, one allocation
+  P1Launch *zinv = nullptr, *xinv = nullptr, *zfwd = nullptr, *flux[3] = {};
+  Rhs2Launch *r2[3] = {}, *r2p[3] = {};
+  RhsMeanLaunch* rm[3] = {};
+  EnsMember* sm = nullptr;
+  EnsJet* jt = nullptr;
+  // the first member's records: launch shapes, on the class's streams
+  P1Launch h_zinv{}, h_xinv{}, h_zfwd{}, h_flux[3] = {};
+  Rhs2Launch h_r2[3] = {}, h_r2p[3] = {};
+  RhsMeanLaunch h_rm[3] = {};
+  int nx = 0, nz = 0, nxh = 0, nx2 = 0, nz2 = 0;
+  size_t ncbc = 0;
+};
 
 struct cfg_ensemble {
   std::vector<cfg_ctx*> m;
@@ -2664,18 +2814,289 @@ struct cfg_ensemble {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   std::vector<long long> launches_per_step;
+  bool batched = false;        // step layout of the next capture
+  bool last_batched = false;   // layout of the last enqueued step
+  std::vector<EnsClass> cls;   // batched: the classes (built on first use)
 };
+
+static void ens_free_classes(cfg_ensemble* e) {
+  for (EnsClass& k : e->cls) {
+    if (k.dtab) cudaFree(k.dtab);
+    for (cudaEvent_t v : {k.ev_start, k.ev_fork, k.ev_j2, k.ev_j3, k.ev_done})
+      if (v) cudaEventDestroy(v);
+    for (cudaStream_t v : {k.st, k.st2, k.st3})
+      if (v) cudaStreamDestroy(v);
+  }
+  e->cls.clear();
+}
+
+static void ens_drop_graph(cfg_ensemble* e) {
+  if (e->exec) cudaGraphExecDestroy(e->exec);
+  if (e->graph) cudaGraphDestroy(e->graph);
+  e->exec = nullptr;
+  e->graph = nullptr;
+}
 
 void cfg_ensemble_destroy(cfg_ensemble* e) {
   if (!e) return;
   cudaSetDevice(e->dev);
   if (e->st) cudaStreamSynchronize(e->st);
-  if (e->exec) cudaGraphExecDestroy(e->exec);
-  if (e->graph) cudaGraphDestroy(e->graph);
+  ens_drop_graph(e);
+  ens_free_classes(e);
   for (cudaEvent_t v : e->ev_done) cudaEventDestroy(v);
   if (e->ev_fork) cudaEventDestroy(e->ev_fork);
   if (e->st) cudaStreamDestroy(e->st);
   delete e;
+}
+
+// whether a member's step can run in the batched layout
+static bool ens_batchable(const cfg_ctx* c) {
+  return c->mixed && c->nranks == 1 && c->g.kx0 == 0 && c->split_x && c->fast_z && c->use_rhs2 && c->rhs2_tbl64 &&
+         c->n_fast > 0 && !c->les_on && c->p.ctrlu == 0.0 && c->p.ctrlw == 0.0 && !c->prof_on;
+}
+
+// same class: everything that sets a batched launch's shape or kernel
+static bool ens_same_class(const cfg_ctx* a, const cfg_ctx* b) {
+  const Geom &x = a->g, &y = b->g;
+  return x.nx == y.nx && x.ny == y.ny && x.nz == y.nz && x.nx2 == y.nx2 && x.nz2 == y.nz2 && x.nxh == y.nxh &&
+         x.ny1 == y.ny1 && x.nw == y.nw && a->gP.nz2 == b->gP.nz2 && a->fYB1 == b->fYB1 && a->fYB3 == b->fYB3 &&
+         a->flux_zr == b->flux_zr && a->rhs2_warps == b->rhs2_warps && a->rhs2_lanes == b->rhs2_lanes &&
+         a->mean_split == b->mean_split && a->n_fast == b->n_fast && a->n_prec == b->n_prec;
+}
+
+// the classes, their streams and their member tables
+static int ens_build_classes(cfg_ensemble* e) {
+  using I = Impl<float>;
+  ens_free_classes(e);
+  for (int i = 0; i < (int)e->m.size(); ++i) {
+    bool placed = false;
+    for (EnsClass& k : e->cls)
+      if (ens_same_class(e->m[k.mem[0]], e->m[i])) {
+        k.mem.push_back(i);
+        placed = true;
+        break;
+      }
+    if (!placed) {
+      e->cls.emplace_back();
+      e->cls.back().mem.push_back(i);
+    }
+  }
+  for (EnsClass& k : e->cls) {
+    for (int i : k.mem)
+      if (e->m[i]->crossflow) k.jet.push_back(i);
+    bool ok = true;
+    for (cudaStream_t* v : {&k.st, &k.st2, &k.st3})
+      ok = ok && cudaStreamCreateWithFlags(v, cudaStreamNonBlocking) == cudaSuccess;
+    for (cudaEvent_t* v : {&k.ev_start, &k.ev_fork, &k.ev_j2, &k.ev_j3, &k.ev_done})
+      ok = ok && cudaEventCreateWithFlags(v, cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) return CFG_E_CUDA;
+    const int n = (int)k.mem.size(), nj = (int)k.jet.size();
+    std::vector<P1Launch> zinv(n), xinv(n), zfwd(n), flux(3 * n);
+    std::vector<Rhs2Launch> r2(3 * n), r2p(3 * n);
+    std::vector<RhsMeanLaunch> rm(3 * n);
+    std::vector<EnsMember> sm(n);
+    std::vector<EnsJet> jt(nj);
+    for (int q = 0; q < n; ++q) {
+      const cfg_ctx* c = e->m[k.mem[q]];
+      zinv[q] = I::p1_args(c, 1, false, 0);
+      xinv[q] = I::p1_args(c, 1, false, 3);
+      zfwd[q] = I::p1_args(c, 1, false, 2);
+      for (int rk = 1; rk <= 3; ++rk) {
+        flux[(rk - 1) * n + q] = I::p1_args(c, rk, false, 4);
+        r2[(rk - 1) * n + q] = I::rhs2_args(c, rk, false);
+        r2p[(rk - 1) * n + q] = I::rhs2_args(c, rk, true);
+        rm[(rk - 1) * n + q] = I::mean_args(c, rk);
+      }
+      EnsMember& a = sm[q];
+      a.m64 = c->mvel64;
+      a.v32 = (const float2*)c->vel;
+      a.base = c->mean_base;
+      a.ny1 = c->g.ny1;
+      a.split = (c->mean_split && !c->les_on) ? 1 : 0;
+      a.cflbits = c->cflbits;
+      a.cbc = (float2*)c->cbc;
+      a.ncbc = 6 * (size_t)c->g.nw;
+      a.g = c->g;
+      a.gd = c->gd;
+      a.sc = c->sc;
+      a.cflp = c->cflp;
+      a.lx = c->p.lx;
+      a.lz = c->p.lz;
+      a.cfl_max = c->p.cfl_max;
+      a.dt_flag = c->p.dt_flag;
+    }
+    for (int q = 0; q < nj; ++q) {
+      const cfg_ctx* c = e->m[k.jet[q]];
+      EnsJet& a = jt[q];
+      a.st = c->jst;
+      a.jp = c->jp;
+      a.sc = c->sc;
+      a.rkt = c->rkt;
+      a.phys = (float*)c->pw_phys;
+      a.H = (float2*)c->pw_H;
+      a.spec = (float2*)c->pw_in;
+      a.cbc = (float2*)c->cbc;
+      a.gd = c->gd;
+      a.px = c->pxs;
+      a.pz = c->pzs;
+      a.twx = (const float2*)c->twxs;
+      a.twz = (const float2*)c->twzs;
+      a.nx = c->g.nx;
+      a.nz = c->g.nz;
+      a.nxh = c->g.nxh;
+      a.nw = (size_t)c->g.nw;
+      a.lx = c->p.lx;
+      a.lz = c->p.lz;
+    }
+    // one device allocation, 256-byte aligned pieces
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+      const size_t o = off;
+      off += (bytes + 255) & ~(size_t)255;
+      return o;
+    };
+    const size_t o_zinv = take(sizeof(P1Launch) * n), o_xinv = take(sizeof(P1Launch) * n),
+                 o_zfwd = take(sizeof(P1Launch) * n), o_flux = take(sizeof(P1Launch) * 3 * n),
+                 o_r2 = take(sizeof(Rhs2Launch) * 3 * n), o_r2p = take(sizeof(Rhs2Launch) * 3 * n),
+                 o_rm = take(sizeof(RhsMeanLaunch) * 3 * n), o_sm = take(sizeof(EnsMember) * n),
+                 o_jt = take(sizeof(EnsJet) * (nj > 0 ? nj : 1));
+    if (cudaMalloc(&k.dtab, off) != cudaSuccess) {
+      cudaGetLastError();
+      k.dtab = nullptr;
+      return CFG_E_NOMEM;
+    }
+    char* b = (char*)k.dtab;
+    auto put = [&](size_t o, const void* src, size_t bytes) {
+      return bytes == 0 || cudaMemcpy(b + o, src, bytes, cudaMemcpyHostToDevice) == cudaSuccess;
+    };
+    ok = put(o_zinv, zinv.data(), sizeof(P1Launch) * n) && put(o_xinv, xinv.data(), sizeof(P1Launch) * n) &&
+         put(o_zfwd, zfwd.data(), sizeof(P1Launch) * n) && put(o_flux, flux.data(), sizeof(P1Launch) * 3 * n) &&
+         put(o_r2, r2.data(), sizeof(Rhs2Launch) * 3 * n) && put(o_r2p, r2p.data(), sizeof(Rhs2Launch) * 3 * n) &&
+         put(o_rm, rm.data(), sizeof(RhsMeanLaunch) * 3 * n) && put(o_sm, sm.data(), sizeof(EnsMember) * n) &&
+         put(o_jt, jt.data(), sizeof(EnsJet) * nj);
+    if (!ok) return CFG_E_CUDA;
+    k.zinv = (P1Launch*)(b + o_zinv);
+    k.xinv = (P1Launch*)(b + o_xinv);
+    k.zfwd = (P1Launch*)(b + o_zfwd);
+    for (int r = 0; r < 3; ++r) {
+      k.flux[r] = (P1Launch*)(b + o_flux) + r * n;
+      k.r2[r] = (Rhs2Launch*)(b + o_r2) + r * n;
+      k.r2p[r] = (Rhs2Launch*)(b + o_r2p) + r * n;
+      k.rm[r] = (RhsMeanLaunch*)(b + o_rm) + r * n;
+      k.h_flux[r] = flux[r * n];
+      k.h_flux[r].st = k.st;
+      k.h_r2[r] = r2[r * n];
+      k.h_r2[r].st = k.st;
+      k.h_r2p[r] = r2p[r * n];
+      k.h_r2p[r].st = k.st2;
+      k.h_rm[r] = rm[r * n];
+      k.h_rm[r].st = k.st3;
+    }
+    k.sm = (EnsMember*)(b + o_sm);
+    k.jt = (EnsJet*)(b + o_jt);
+    k.h_zinv = zinv[0];
+    k.h_zinv.st = k.st;
+    k.h_xinv = xinv[0];
+    k.h_xinv.st = k.st;
+    k.h_zfwd = zfwd[0];
+    k.h_zfwd.st = k.st;
+    const cfg_ctx* c0 = e->m[k.mem[0]];
+    k.nx = c0->g.nx;
+    k.nz = c0->g.nz;
+    k.nxh = c0->g.nxh;
+    k.nx2 = c0->g.nx2;
+    k.nz2 = c0->g.nz2;
+    k.ncbc = 6 * (size_t)c0->g.nw;
+  }
+  return CFG_OK;
+}
+
+// one time step of one class: the sequence of step_enqueue (boundary, three
+// nonlinear + rhs substeps, t_total += dt), each kernel once for all members
+static int ens_class_enqueue(cfg_ensemble* e, EnsClass& k) {
+  const int n = (int)k.mem.size(), nj = (int)k.jet.size();
+  cfg_ctx* c0 = e->m[k.mem[0]];
+  int launches = 0;
+  auto ck = [&](bool ok, const char* what) { return ok && cudaGetLastError() == cudaSuccess ? 0 : fail(c0, CFG_E_CUDA, "%s", what); };
+  const unsigned zb = (unsigned)std::min<size_t>(64, (k.ncbc + 255) / 256);
+  k_ens_zero_cbc<<<dim3(zb, n), 256, 0, k.st>>>(k.sm);
+  ++launches;
+  if (int r = ck(true, "batched boundary")) return r;
+  for (int rk = 1; rk <= 3; ++rk) {
+    k_ens_prologue<<<n, 256, 0, k.st>>>(k.sm, rk == 1);
+    ++launches;
+    if (int r = ck(true, "batched substep prologue")) return r;
+    if (int r = ck(p1_fast_launch_batch(0, k.nz2, true, k.h_zinv, k.zinv, n) == 0, "batched k_zinv_r")) return r;
+    if (int r = ck(p1_fast_launch_batch(3, k.nx2, true, k.h_xinv, k.xinv, n) == 0, "batched k_xinv_r")) return r;
+    if (int r = ck(p1_fast_launch_batch(4, k.nx2, true, k.h_flux[rk - 1], k.flux[rk - 1], n) == 0, "batched k_flux_r"))
+      return r;
+    if (int r = ck(p1_fast_launch_batch(2, k.nz2, true, k.h_zfwd, k.zfwd, n) == 0, "batched k_zfwd_r")) return r;
+    launches += 4;
+    if (rk == 1) {
+      k_cfl_finalize_b<<<n, 256, 0, k.st>>>(k.sm, c0->step);
+      ++launches;
+      if (int r = ck(true, "batched k_cfl_finalize")) return r;
+    }
+    if (nj > 0) {
+      // the wall jet of this substep (PFC/pass2.f90:41-43)
+      k_jet_walk_b<<<nj, 32, 0, k.st>>>(k.jt, rk);
+      k_jet_field_b<<<dim3(k.nz * nj, 3), 128, 0, k.st>>>(k.jt, (unsigned)k.nz);
+      const unsigned gxx = (unsigned)(k.nz + 1) / 2;
+      k_px_fwd_b<<<dim3(gxx * nj, 3), 128, sizeof(float2) * 3 * k.nx, k.st>>>(k.jt, gxx);
+      k_pz_fwd_b<<<dim3((unsigned)k.nxh * nj, 3), 128, sizeof(float2) * 3 * k.nz, k.st>>>(k.jt, (unsigned)k.nxh);
+      const unsigned gxc = (unsigned)((k.ncbc / 6 + 255) / 256);
+      k_jet_combine_b<<<gxc * nj, 256, 0, k.st>>>(k.jt, gxc);
+      launches += 5;
+      if (int r = ck(true, "batched wall jet")) return r;
+    }
+    // the FP64 |k| < 4 list and the mean mode beside the main kernel
+    if (int r = ck(cudaEventRecord(k.ev_fork, k.st) == cudaSuccess &&
+                       cudaStreamWaitEvent(k.st2, k.ev_fork, 0) == cudaSuccess &&
+                       cudaStreamWaitEvent(k.st3, k.ev_fork, 0) == cudaSuccess,
+                   "batched fork"))
+      return r;
+    if (k.h_r2p[rk - 1].nlist > 0) {
+      if (int r = ck(rhs2_launch_prec_batch(k.h_r2p[rk - 1], k.r2p[rk - 1], n) == 0, "batched k_rhs2 (FP64 list)"))
+        return r;
+      ++launches;
+    }
+    if (int r = ck(rhs_mean2_launch_batch(true, k.h_rm[rk - 1], k.rm[rk - 1], n) == 0, "batched k_rhs_mean2")) return r;
+    if (int r = ck(rhs2_launch_batch(true, k.h_r2[rk - 1], k.r2[rk - 1], n) == 0, "batched k_rhs2")) return r;
+    launches += 2;
+    if (int r = ck(cudaEventRecord(k.ev_j2, k.st2) == cudaSuccess && cudaEventRecord(k.ev_j3, k.st3) == cudaSuccess &&
+                       cudaStreamWaitEvent(k.st, k.ev_j2, 0) == cudaSuccess &&
+                       cudaStreamWaitEvent(k.st, k.ev_j3, 0) == cudaSuccess,
+                   "batched join"))
+      return r;
+  }
+  k_ens_advance<<<(n + 63) / 64, 64, 0, k.st>>>(k.sm, n);
+  ++launches;
+  if (int r = ck(true, "batched advance time")) return r;
+  // the members' host bookkeeping, as step_enqueue keeps it (the batched
+  // launches are shared: each member is credited with its share)
+  for (int q = 0; q < n; ++q) {
+    cfg_ctx* c = e->m[k.mem[q]];
+    c->step = c->step < 0 ? 1 : c->step + 1;
+    c->mean64_valid = true;
+    c->launches += (launches + q) / n;
+  }
+  return CFG_OK;
+}
+
+static int ens_batched_enqueue(cfg_ensemble* e) {
+  if (e->cls.empty()) {
+    const int r = ens_build_classes(e);
+    if (r) return r;
+  }
+  if (cudaEventRecord(e->ev_fork, e->st) != cudaSuccess) return CFG_E_CUDA;
+  for (EnsClass& k : e->cls) {
+    if (cudaStreamWaitEvent(k.st, e->ev_fork, 0) != cudaSuccess) return CFG_E_CUDA;
+    const int r = ens_class_enqueue(e, k);
+    if (r) return r;
+    if (cudaEventRecord(k.ev_done, k.st) != cudaSuccess || cudaStreamWaitEvent(e->st, k.ev_done, 0) != cudaSuccess)
+      return CFG_E_CUDA;
+  }
+  return CFG_OK;
 }
 
 int cfg_ensemble_create(int n, cfg_ctx* const* members, int autotune, cfg_ensemble** out) {
@@ -2693,6 +3114,8 @@ int cfg_ensemble_create(int n, cfg_ctx* const* members, int autotune, cfg_ensemb
             cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming) == cudaSuccess;
   for (int i = 0; i < n && ok; ++i) ok = cudaEventCreateWithFlags(&e->ev_done[i], cudaEventDisableTiming) == cudaSuccess;
   if (!ok) { cfg_ensemble_destroy(e); return CFG_E_CUDA; }
+  e->batched = true;
+  for (int i = 0; i < n; ++i) e->batched = e->batched && ens_batchable(members[i]);
   if (autotune) {
     // one trial run per distinct grid and precision; the others take its tiles
     for (int i = 0; i < n; ++i) {
@@ -2719,9 +3142,15 @@ int cfg_ensemble_create(int n, cfg_ctx* const* members, int autotune, cfg_ensemb
   return CFG_OK;
 }
 
-// one step of every member on its own stream, forked from and joined to the
-// ensemble stream (eagerly, or under stream capture)
+// one step of the ensemble (eagerly, or under stream capture): batched, or
+// every member on its own stream, forked from and joined to the ensemble
+// stream.  A batched step needs every member's FP64 mean copy current (it is
+// after any whole step).
 static int ensemble_enqueue(cfg_ensemble* e) {
+  bool batched = e->batched;
+  for (const cfg_ctx* c : e->m) batched = batched && c->mean64_valid;
+  e->last_batched = batched;
+  if (batched) return ens_batched_enqueue(e);
   if (cudaEventRecord(e->ev_fork, e->st) != cudaSuccess) return CFG_E_CUDA;
   for (size_t i = 0; i < e->m.size(); ++i) {
     cfg_ctx* c = e->m[i];
@@ -2741,9 +3170,14 @@ int cfg_ensemble_timestep(cfg_ensemble* e, int nsteps) {
   int r;
   if (!e->exec && nsteps > 0) {
     // the first step runs eagerly (it also sets every kernel's shared-memory
-    // limit), the second is captured
+    // limit; a second one when the first could not run batched), the next
+    // one is captured
     if ((r = ensemble_enqueue(e))) return r;
     --nsteps;
+    if (e->batched && !e->last_batched && nsteps > 0) {
+      if ((r = ensemble_enqueue(e))) return r;
+      --nsteps;
+    }
     if (nsteps == 0) return CFG_OK;
     std::vector<long long> before(e->m.size());
     for (size_t i = 0; i < e->m.size(); ++i) before[i] = e->m[i]->launches;
@@ -2786,6 +3220,23 @@ int cfg_ensemble_synchronize(cfg_ensemble* e) {
 }
 
 void* cfg_ensemble_stream(cfg_ensemble* e) { return e ? (void*)e->st : nullptr; }
+
+int cfg_ensemble_set_batched(cfg_ensemble* e, int on) {
+  if (!e) return CFG_E_ARG;
+  if (on)
+    for (const cfg_ctx* c : e->m)
+      if (!ens_batchable(c)) return CFG_E_ARG;
+  cudaSetDevice(e->dev);
+  if (cudaStreamSynchronize(e->st) != cudaSuccess) return CFG_E_CUDA;
+  // the next step is captured again in the new layout; the classes are
+  // rebuilt then (tiles may have changed)
+  ens_drop_graph(e);
+  ens_free_classes(e);
+  e->batched = on != 0;
+  return CFG_OK;
+}
+
+int cfg_ensemble_batched(const cfg_ensemble* e) { return e && e->batched ? 1 : 0; }
 
 int cfg_rank_timestep(cfg_ctx* c, int nsteps, cfg_barrier_fn barrier, void* user) {
   return rank_timestep(c, nsteps, barrier, user, true);

@@ -48,8 +48,9 @@ __device__ __forceinline__ double jet_u01(uint64_t seed, long long x, int z, int
 // one warp.  use_sc: time = t_total + dt*sum(rkc(1:rk)+rkd(1:rk)),
 // incr = dt*(rkc(rk)+rkd(rk)) from the device scalars (PFC/pass2.f90:37-38);
 // otherwise the given time/incr.
-__global__ void k_jet_walk(JetState* __restrict__ st, JetParams jp, const DevScalars* __restrict__ sc,
-                           RkTab rkt, int rk, double time, double incr, int use_sc) {
+__device__ __forceinline__ void k_jet_walk_body(const uint3 bid, JetState* __restrict__ st, JetParams jp,
+                                                const DevScalars* __restrict__ sc, RkTab rkt, int rk, double time,
+                                                double incr, int use_sc) {
   const int n = threadIdx.x;
   if (use_sc) {
     double s = 0.0;
@@ -76,6 +77,11 @@ __global__ void k_jet_walk(JetState* __restrict__ st, JetParams jp, const DevSca
   st->inc[n] = inc;
 }
 
+__global__ void k_jet_walk(JetState* __restrict__ st, JetParams jp, const DevScalars* __restrict__ sc, RkTab rkt,
+                           int rk, double time, double incr, int use_sc) {
+  k_jet_walk_body(blockIdx, st, jp, sc, rkt, rk, time, incr, use_sc);
+}
+
 // |(a, b)| of a default-real complex: both parts rounded to single, the
 // modulus formed in double and rounded to single
 __device__ __forceinline__ double abs_cmplx_single(double a, double b) {
@@ -86,9 +92,10 @@ __device__ __forceinline__ double abs_cmplx_single(double a, double b) {
 // grid (nz, 3), block 128: planes 0 suction, 1 bottom jet, 2 top jet;
 // phys[p][z][x] on the nx x nz grid
 template <typename T>
-__global__ void k_jet_field(T* __restrict__ phys, JetParams jp, const JetState* __restrict__ st, int nx, int nz,
-                            double lx, double lz) {
-  const int z = blockIdx.x, p = blockIdx.y;
+__device__ __forceinline__ void k_jet_field_body(const uint3 bid, T* __restrict__ phys, JetParams jp,
+                                                 const JetState* __restrict__ st, int nx, int nz, double lx,
+                                                 double lz) {
+  const int z = bid.x, p = bid.y;
   const double pi = 3.14159265358979323846;
   const double time = st->time;
   const double zc = (double)z * lz / (double)nz;
@@ -148,14 +155,21 @@ __global__ void k_jet_field(T* __restrict__ phys, JetParams jp, const JetState* 
   }
 }
 
+template <typename T>
+__global__ void k_jet_field(T* __restrict__ phys, JetParams jp, const JetState* __restrict__ st, int nx, int nz,
+                            double lx, double lz) {
+  k_jet_field_body<T>(blockIdx, phys, jp, st, nx, nz, lx, lz);
+}
+
 // spec[p][kx][kz] (p = 0 suction, 1 bottom, 2 top) -> cbc(:,:,2) of the
 // forced walls, the other wall slots zeroed
 template <typename T>
-__global__ void k_jet_combine(const cplx_t<T>* __restrict__ spec, cplx_t<T>* __restrict__ cbc, JetParams jp,
-                              GridDev gd, int nx, int nz, int nxh, double lx, double lz) {
+__device__ __forceinline__ void k_jet_combine_body(const uint3 bid, const cplx_t<T>* __restrict__ spec,
+                                                   cplx_t<T>* __restrict__ cbc, JetParams jp, GridDev gd, int nx,
+                                                   int nz, int nxh, double lx, double lz) {
   using C = cplx_t<T>;
   const int nw = nz * nxh;
-  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  const int w = bid.x * blockDim.x + threadIdx.x;
   if (w >= nw) return;
   const int kx = w / nz, kz = w % nz;
   const double pi = 3.14159265358979323846;
@@ -184,6 +198,12 @@ __global__ void k_jet_combine(const cplx_t<T>* __restrict__ spec, cplx_t<T>* __r
     // cbc layout [bot, top][comp][kx][kz]: component 2 (v) is index 1
     cbc[((size_t)wall * 3 + 1) * nw + w] = out;
   }
+}
+
+template <typename T>
+__global__ void k_jet_combine(const cplx_t<T>* __restrict__ spec, cplx_t<T>* __restrict__ cbc, JetParams jp,
+                              GridDev gd, int nx, int nz, int nxh, double lx, double lz) {
+  k_jet_combine_body<T>(blockIdx, spec, cbc, jp, gd, nx, nz, nxh, lx, lz);
 }
 
 // ---------------------------------------------------------------------------

@@ -351,10 +351,9 @@ __global__ void __launch_bounds__(256) k_zfwd(const cplx_t<T>* __restrict__ T2,
 // --------------------------------------------------------------------------
 // check_cfl + dt adaptation (PFC/pass1.f90:202-250, 106-124): one block.
 template <bool LIN>
-__global__ void k_cfl_finalize(const unsigned long long* __restrict__ cflbits, Geom g,
-                               GridDev gd, DevScalars* sc, double* cfl, double lx,
-                               double lz, int dt_flag, double cfl_max_param,
-                               int step) {
+__device__ __forceinline__ void k_cfl_finalize_body(const uint3 bid, const unsigned long long* __restrict__ cflbits,
+                                                    Geom g, GridDev gd, DevScalars* sc, double* cfl, double lx,
+                                                    double lz, int dt_flag, double cfl_max_param, int step) {
   __shared__ double smax[256];
   const int ny = g.ny;
   const double dt = sc->dt;
@@ -395,6 +394,12 @@ __global__ void k_cfl_finalize(const unsigned long long* __restrict__ cflbits, G
       sc->dt = fmin(dt_temp, alt);
     }
   }
+}
+
+template <bool LIN>
+__global__ void k_cfl_finalize(const unsigned long long* __restrict__ cflbits, Geom g, GridDev gd, DevScalars* sc,
+                               double* cfl, double lx, double lz, int dt_flag, double cfl_max_param, int step) {
+  k_cfl_finalize_body<LIN>(blockIdx, cflbits, g, gd, sc, cfl, lx, lz, dt_flag, cfl_max_param, step);
 }
 
 }  // namespace cfd

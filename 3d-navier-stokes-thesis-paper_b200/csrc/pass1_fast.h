@@ -33,6 +33,10 @@ struct P1Launch {
 // which: 0 k_zinv_r, 1 k_xflux_r, 2 k_zfwd_r, 3 k_xinv_r, 4 k_flux_r.
 // Returns 0, or -1 when the length is not compiled in, or -2 on a launch error.
 int p1_fast_launch(int which, int n, bool f32, const P1Launch& a);
+// the same kernel for nmem members of one grid and tiles in one launch: tab
+// is the members' P1Launch array in device memory, a the first member's
+// (host) copy, which sets the launch shape and stream; which 0, 2, 3 or 4
+int p1_fast_launch_batch(int which, int n, bool f32, const P1Launch& a, const P1Launch* tab, int nmem);
 // shared memory bytes of kernel `which` at length n with its tile parameter
 // (YB for 0/2, ZR for 1 and 4, the z2 row count for 3); 0 when unsupported.
 size_t p1_fast_smem(int which, int n, bool f32, int param, int nxh, int nz);

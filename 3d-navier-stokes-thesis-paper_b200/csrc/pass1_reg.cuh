@@ -53,10 +53,9 @@ template <typename T> struct ZRawPad {   // 32 bytes between component blocks
 };
 
 template <typename T, int NZ2>
-__global__ void __launch_bounds__(288, sizeof(T) == 4 ? 3 : 1) k_zinv_r(const cplx_t<T>* __restrict__ vel,
-                                                cplx_t<T>* __restrict__ T1, Geom g,
-                                                const cplx_t<T>* __restrict__ twz, int YB, Scatter sc,
-                                                int split) {
+__device__ __forceinline__ void k_zinv_r_body(const uint3 bid, const cplx_t<T>* __restrict__ vel,
+                                              cplx_t<T>* __restrict__ T1, Geom g, const cplx_t<T>* __restrict__ twz,
+                                              int YB, Scatter sc, int split) {
   using C = cplx_t<T>;
   constexpr int N1 = Split<NZ2>::N1, N2 = Split<NZ2>::N2, PITCH = N2 + 1, SEQ = SeqPitch<NZ2>::V;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -65,8 +64,8 @@ __global__ void __launch_bounds__(288, sizeof(T) == 4 ? 3 : 1) k_zinv_r(const cp
   C* tw = reinterpret_cast<C*>(smem_raw);
   C* raw = tw + NZ2;                         // [c][kz][jj]
   C* Y = raw + 3 * RS;
-  const int kx = blockIdx.x;
-  const int j0 = blockIdx.y * YB;
+  const int kx = bid.x;
+  const int j0 = bid.y * YB;
   const int nj = min(YB, NY1 - j0);
   const int nseq = 3 * YB;
   const C* col = vel + (size_t)kx * NZ * 3 * NY1;
@@ -157,14 +156,20 @@ __global__ void __launch_bounds__(288, sizeof(T) == 4 ? 3 : 1) k_zinv_r(const cp
   }
 }
 
+template <typename T, int NZ2>
+__global__ void __launch_bounds__(288, sizeof(T) == 4 ? 3 : 1)
+k_zinv_r(const cplx_t<T>* __restrict__ vel, cplx_t<T>* __restrict__ T1, Geom g, const cplx_t<T>* __restrict__ twz,
+         int YB, Scatter sc, int split) {
+  k_zinv_r_body<T, NZ2>(blockIdx, vel, T1, g, twz, YB, sc, split);
+}
+
 // --------------------------------------------------------------------------
 // k_zfwd_r: grid (nxh, ceil(ny1/YB)), block 256.  Forward z transform, fold,
 // scale and ikz combine (PFC/transform.f90:317-333, 639-688).
 template <typename T, int NZ2>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_zfwd_r(const cplx_t<T>* __restrict__ T2,
-                                                   cplx_t<T>* __restrict__ vel, Geom g,
-                                                   const cplx_t<T>* __restrict__ twz, GridDev gd,
-                                                   int YB) {
+__device__ __forceinline__ void k_zfwd_r_body(const uint3 bid, const cplx_t<T>* __restrict__ T2,
+                                              cplx_t<T>* __restrict__ vel, Geom g, const cplx_t<T>* __restrict__ twz,
+                                              GridDev gd, int YB) {
   using C = cplx_t<T>;
   constexpr int N1 = Split<NZ2>::N1, N2 = Split<NZ2>::N2, PITCH = N2 + 1, SEQ = SeqPitch<NZ2>::V;
   constexpr int ZP = NZ2 + 1;   // pitch of the stage-2 output (spreads banks across sequences)
@@ -175,8 +180,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_zfwd_r(const cp
   C* Y = tw + NZ2;
   C* Z = Y;                      // stage 2 reads Y into registers, then overwrites it
   const int NZ = g.nz, NY1 = g.ny1, NXH = g.nxh, ny = g.ny;
-  const int kx = blockIdx.x;
-  const int j0 = 1 + blockIdx.y * YB;   // 1-based first plane
+  const int kx = bid.x;
+  const int j0 = 1 + bid.y * YB;   // 1-based first plane
   __shared__ T skz[NZ2];                 // kz of the retained rows (nz <= nz2)
   load_tw2<T, NZ2>(tw, twz);
   for (int i = threadIdx.x; i < NZ; i += blockDim.x) skz[i] = (T)gd.kz[i];
@@ -249,6 +254,13 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_zfwd_r(const cp
     }
     vel[((size_t)(kx * NZ + kz) * 3 + e) * NY1 + (j - 1)] = out;
   }
+}
+
+template <typename T, int NZ2>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2)
+k_zfwd_r(const cplx_t<T>* __restrict__ T2, cplx_t<T>* __restrict__ vel, Geom g, const cplx_t<T>* __restrict__ twz,
+         GridDev gd, int YB) {
+  k_zfwd_r_body<T, NZ2>(blockIdx, T2, vel, g, twz, gd, YB);
 }
 
 // --------------------------------------------------------------------------
@@ -558,8 +570,8 @@ template <typename T, int ZB> struct RawPitch {
 // complex FFT (the x part of xz_fft_complex_to_real_parallel,
 // PFC/transform.f90:345-368).  v of plane ny+1 is not formed: no flux reads it.
 template <typename T, int NX2, int ZB>
-__global__ void __launch_bounds__(256) k_xinv_r(const cplx_t<T>* __restrict__ T1, T* __restrict__ P, Geom g,
-                                                const cplx_t<T>* __restrict__ twx) {
+__device__ __forceinline__ void k_xinv_r_body(const uint3 bid, const cplx_t<T>* __restrict__ T1, T* __restrict__ P,
+                                              Geom g, const cplx_t<T>* __restrict__ twx) {
   using C = cplx_t<T>;
   constexpr int N1 = Split<NX2>::N1, N2 = Split<NX2>::N2, PITCH = N2 + 1, SEQ = SeqPitch<NX2>::V;
   constexpr int N = NX2, Nh = NX2 / 2, NS = ZB / 2, RP = RawPitch<T, ZB>::V;
@@ -570,7 +582,7 @@ __global__ void __launch_bounds__(256) k_xinv_r(const cplx_t<T>* __restrict__ T1
   C* tw = reinterpret_cast<C*>(smem_raw);   // [N]
   C* raw = tw + N;                          // [NXH][RP]
   C* Y = raw + NXH * RP;                    // [NS][SEQ]
-  const int z0 = blockIdx.x * ZB, c = blockIdx.y, pl = blockIdx.z;
+  const int z0 = bid.x * ZB, c = bid.y, pl = bid.z;
   if (c == 1 && pl == g.ny) return;
   const C* src = T1 + ((size_t)pl * 3 + c) * NXH * NZ2 + z0;
   for (int idx = threadIdx.x; idx < NXH * CH; idx += blockDim.x) {
@@ -627,6 +639,12 @@ __global__ void __launch_bounds__(256) k_xinv_r(const cplx_t<T>* __restrict__ T1
   }
 }
 
+template <typename T, int NX2, int ZB>
+__global__ void __launch_bounds__(256)
+k_xinv_r(const cplx_t<T>* __restrict__ T1, T* __restrict__ P, Geom g, const cplx_t<T>* __restrict__ twx) {
+  k_xinv_r_body<T, NX2, ZB>(blockIdx, T1, P, g, twx);
+}
+
 // k_flux_r: grid (nz2/ZR, ny-1), block NT.  Fluxes of plane k = 2 + blockIdx.y
 // on ZR rows of z from the physical planes k-1, k, k+1, then the forward x
 // transform and the Hermitian unpacking into T2 -- the same arithmetic and
@@ -643,11 +661,11 @@ __global__ void __launch_bounds__(256) k_xinv_r(const cplx_t<T>* __restrict__ T1
 // momentum fluxes at the same points (y-plane values interpolated as the
 // velocities are: half sums for the u and w equations, iu for the v one).
 template <typename T, int NX2, int ZR, int NT, int MODE>
-__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT == 256 ? 1 : 3)) k_flux_r(const T* __restrict__ P, cplx_t<T>* __restrict__ T2, Geom g,
-                                               const cplx_t<T>* __restrict__ twx, GridDev gd,
-                                               const T* __restrict__ fringe, int has_fringe,
-                                               unsigned long long* __restrict__ cflbits, int do_cfl, Scatter sc,
-                                               const T* __restrict__ S) {
+__device__ __forceinline__ void k_flux_r_body(const uint3 bid, const T* __restrict__ P, cplx_t<T>* __restrict__ T2,
+                                              Geom g, const cplx_t<T>* __restrict__ twx, GridDev gd,
+                                              const T* __restrict__ fringe, int has_fringe,
+                                              unsigned long long* __restrict__ cflbits, int do_cfl, Scatter sc,
+                                              const T* __restrict__ S) {
   constexpr bool LIN = MODE == 1, SGS = MODE == 2, SPLIT = MODE == 3;
   constexpr bool HASB = LIN || SPLIT;
   using C = cplx_t<T>;
@@ -664,8 +682,8 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT
   __shared__ T red[3][NW];
   __shared__ T skx[NX2 / 2 + 2];             // kx of the retained columns (nx/2+1 <= nx2/2+1)
   const int NXH = g.nxh, NZ2 = g.nz2, ny = g.ny;
-  const int z0 = blockIdx.x * ZR;
-  const int k = 2 + blockIdx.y;
+  const int z0 = bid.x * ZR;
+  const int k = 2 + bid.y;
   load_tw2<T, N>(tw, twx);
   for (int i = threadIdx.x; i < g.nxh; i += NT) skx[i] = (T)gd.kx[i];
   auto px = [](int x) { return (x / N2) * PITCH + (x % N2); };
@@ -906,6 +924,14 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT
     }
 #undef OUT
   }
+}
+
+template <typename T, int NX2, int ZR, int NT, int MODE>
+__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? (NT == 256 ? 4 : 6) : (NT == 256 ? 1 : 3))
+k_flux_r(const T* __restrict__ P, cplx_t<T>* __restrict__ T2, Geom g, const cplx_t<T>* __restrict__ twx, GridDev gd,
+         const T* __restrict__ fringe, int has_fringe, unsigned long long* __restrict__ cflbits, int do_cfl,
+         Scatter sc, const T* __restrict__ S) {
+  k_flux_r_body<T, NX2, ZR, NT, MODE>(blockIdx, P, T2, g, twx, gd, fringe, has_fringe, cflbits, do_cfl, sc, S);
 }
 
 // smem sizes (bytes) of the three kernels

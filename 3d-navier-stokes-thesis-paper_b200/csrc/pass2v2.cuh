@@ -162,20 +162,18 @@ __host__ __device__ __forceinline__ int rhs2_ld(int n1) { return (n1 + 1) & ~1; 
 // T is the arithmetic precision, S the storage precision of the state (the
 // mixed path runs its |k| < 4 list with T = double over S = float).
 template <typename T, typename S, int M, int G>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 5 : 1) k_rhs2(cplx_t<S>* __restrict__ vel, cplx_t<S>* __restrict__ cru,
-                                              cplx_t<S>* __restrict__ prs,
-                                              const cplx_t<S>* __restrict__ cbc_top,
-                                              const cplx_t<S>* __restrict__ cbc_bot, Geom g,
-                                              GridDev gd, const DevScalars* __restrict__ sc, RkTab rkt,
-                                              int rk, double re, const int* __restrict__ wlist,
-                                              int nlist, const T* __restrict__ tbl) {
+__device__ __forceinline__ void k_rhs2_body(const uint3 bid, cplx_t<S>* __restrict__ vel, cplx_t<S>* __restrict__ cru,
+                                            cplx_t<S>* __restrict__ prs, const cplx_t<S>* __restrict__ cbc_top,
+                                            const cplx_t<S>* __restrict__ cbc_bot, Geom g, GridDev gd,
+                                            const DevScalars* __restrict__ sc, RkTab rkt, int rk, double re,
+                                            const int* __restrict__ wlist, int nlist, const T* __restrict__ tbl) {
   using C = cplx_t<T>;
   using CS = cplx_t<S>;
   constexpr int GPW = 32 / G;                 // lane groups (wavenumbers) per warp
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int grp = lane / G, gl = lane % G;
-  const int widx = (blockIdx.x * (blockDim.x >> 5) + warp) * GPW + grp;
+  const int widx = (bid.x * (blockDim.x >> 5) + warp) * GPW + grp;
   const bool valid = widx < nlist;
   const int w = valid ? wlist[widx] : 1;
   const int NZ = g.nz, ny = g.ny, n1 = g.ny1;
@@ -425,20 +423,29 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 5 : 1) k_rhs2(cplx_t<S>*
   }
 }
 
+template <typename T, typename S, int M, int G>
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 5 : 1)
+k_rhs2(cplx_t<S>* __restrict__ vel, cplx_t<S>* __restrict__ cru, cplx_t<S>* __restrict__ prs,
+       const cplx_t<S>* __restrict__ cbc_top, const cplx_t<S>* __restrict__ cbc_bot, Geom g, GridDev gd,
+       const DevScalars* __restrict__ sc, RkTab rkt, int rk, double re, const int* __restrict__ wlist, int nlist,
+       const T* __restrict__ tbl) {
+  k_rhs2_body<T, S, M, G>(blockIdx, vel, cru, prs, cbc_top, cbc_bot, g, gd, sc, rkt, rk, re, wlist, nlist, tbl);
+}
+
 // Mean mode (kx = kz = 0) of the substep with the constant-mass-flux pressure
 // gradient (PFC/pass2.f90:217-263, 356-375), FP64 arithmetic, one warp of 32
 // lanes: the cru and NL columns are staged in shared memory, u and w share
 // one solve (alpha = 1), v takes the wall value.  In mixed precision the FP64
 // mean columns live in mvel64/mcru64 beside the FP32 state.
 template <typename S, int M>
-__global__ void __launch_bounds__(32) k_rhs_mean2(cplx_t<S>* __restrict__ vel, cplx_t<S>* __restrict__ cru,
-                                                  cplx_t<S>* __restrict__ prs, double2* __restrict__ mvel64,
-                                                  double2* __restrict__ mcru64,
-                                                  const cplx_t<S>* __restrict__ cbc_top,
-                                                  const cplx_t<S>* __restrict__ cbc_bot, Geom g, GridDev gd,
-                                                  DevScalars* __restrict__ sc, double* __restrict__ d_um_dy,
-                                                  RkTab rkt, int rk, double re, double beta, int fix_mass,
-                                                  const double* __restrict__ tbl) {
+__device__ __forceinline__ void k_rhs_mean2_body(const uint3 bid, cplx_t<S>* __restrict__ vel,
+                                                 cplx_t<S>* __restrict__ cru, cplx_t<S>* __restrict__ prs,
+                                                 double2* __restrict__ mvel64, double2* __restrict__ mcru64,
+                                                 const cplx_t<S>* __restrict__ cbc_top,
+                                                 const cplx_t<S>* __restrict__ cbc_bot, Geom g, GridDev gd,
+                                                 DevScalars* __restrict__ sc, double* __restrict__ d_um_dy, RkTab rkt,
+                                                 int rk, double re, double beta, int fix_mass,
+                                                 const double* __restrict__ tbl) {
   using C = double2;
   using CS = cplx_t<S>;
   constexpr int G = 32;
@@ -560,6 +567,17 @@ __global__ void __launch_bounds__(32) k_rhs_mean2(cplx_t<S>* __restrict__ vel, c
     d_um_dy[ny - 1] = dm[3] * sV[ny - 2].x + dm[4] * sV[ny - 1].x + dm[5] * sV[ny].x;
   }
   for (int j = 1 + lane; j <= ny - 2; j += G) d_um_dy[j] = gd.dn[j] * (sV[j + 1].x - sV[j].x);
+}
+
+template <typename S, int M>
+__global__ void __launch_bounds__(32)
+k_rhs_mean2(cplx_t<S>* __restrict__ vel, cplx_t<S>* __restrict__ cru, cplx_t<S>* __restrict__ prs,
+            double2* __restrict__ mvel64, double2* __restrict__ mcru64, const cplx_t<S>* __restrict__ cbc_top,
+            const cplx_t<S>* __restrict__ cbc_bot, Geom g, GridDev gd, DevScalars* __restrict__ sc,
+            double* __restrict__ d_um_dy, RkTab rkt, int rk, double re, double beta, int fix_mass,
+            const double* __restrict__ tbl) {
+  k_rhs_mean2_body<S, M>(blockIdx, vel, cru, prs, mvel64, mcru64, cbc_top, cbc_bot, g, gd, sc, d_um_dy, rkt, rk, re,
+                         beta, fix_mass, tbl);
 }
 
 template <int M> size_t rhs_mean2_smem(int n1) { return sizeof(double2) * 9 * (size_t)rhs2_ld(n1); }

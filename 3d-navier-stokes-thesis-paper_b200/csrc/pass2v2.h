@@ -29,6 +29,11 @@ int rhs2_launch(bool f32, const Rhs2Launch& a);
 // the mixed path's |k| < 4 list: FP64 arithmetic over FP32 storage, tbl the
 // FP64 table for 32 lanes
 int rhs2_launch_prec(const Rhs2Launch& a);
+// the same kernels for nmem members of one grid in one launch: tab is the
+// members' launch records in device memory, a the first member's (host)
+// copy, which sets the launch shape and stream
+int rhs2_launch_batch(bool f32, const Rhs2Launch& a, const Rhs2Launch* tab, int nmem);
+int rhs2_launch_prec_batch(const Rhs2Launch& a, const Rhs2Launch* tab, int nmem);
 
 // the mean mode (k_rhs_mean2)
 struct RhsMeanLaunch {
@@ -47,6 +52,7 @@ struct RhsMeanLaunch {
   cudaStream_t st;
 };
 int rhs_mean2_launch(bool f32, const RhsMeanLaunch& a);
+int rhs_mean2_launch_batch(bool f32, const RhsMeanLaunch& a, const RhsMeanLaunch* tab, int nmem);
 bool rhs2_supported(int ny1);
 // the lane-major grid-coefficient table the kernel reads (host side)
 size_t rhs2_table_bytes(bool f32, int ny1, int lanes);

@@ -98,14 +98,15 @@ __global__ void k_px_inv(const cplx_t<T>* __restrict__ H, T* __restrict__ phys, 
 
 // grid (zlen/2, np)
 template <typename T>
-__global__ void k_px_fwd(const T* __restrict__ phys, cplx_t<T>* __restrict__ H, int nxh, int zlen,
-                         int xlen, FftPlan px, const cplx_t<T>* __restrict__ twx) {
+__device__ __forceinline__ void k_px_fwd_body(const uint3 bid, const T* __restrict__ phys, cplx_t<T>* __restrict__ H,
+                                              int nxh, int zlen, int xlen, FftPlan px,
+                                              const cplx_t<T>* __restrict__ twx) {
   using C = cplx_t<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tw = reinterpret_cast<C*>(smem_raw);
   C* b0 = tw + xlen;
   C* b1 = b0 + xlen;
-  const int z = 2 * blockIdx.x, p = blockIdx.y;
+  const int z = 2 * bid.x, p = bid.y;
   const bool two = (z + 1 < zlen);
   for (int m = threadIdx.x; m < xlen; m += blockDim.x) tw[m] = twx[m];
   for (int k = threadIdx.x; k < xlen; k += blockDim.x)
@@ -121,17 +122,24 @@ __global__ void k_px_fwd(const T* __restrict__ phys, cplx_t<T>* __restrict__ H, 
   }
 }
 
+template <typename T>
+__global__ void k_px_fwd(const T* __restrict__ phys, cplx_t<T>* __restrict__ H, int nxh, int zlen, int xlen,
+                         FftPlan px, const cplx_t<T>* __restrict__ twx) {
+  k_px_fwd_body<T>(blockIdx, phys, H, nxh, zlen, xlen, px, twx);
+}
+
 // grid (nxh, np); out element (p, kx, kz) at out + p*osp + kx*oskx + kz*oskz
 template <typename T>
-__global__ void k_pz_fwd(const cplx_t<T>* __restrict__ H, cplx_t<T>* __restrict__ out, size_t osp,
-                         size_t oskx, size_t oskz, int nxh, int zlen, int nzout, int fold,
-                         T scale, FftPlan pz, const cplx_t<T>* __restrict__ twz) {
+__device__ __forceinline__ void k_pz_fwd_body(const uint3 bid, const cplx_t<T>* __restrict__ H,
+                                              cplx_t<T>* __restrict__ out, size_t osp, size_t oskx, size_t oskz,
+                                              int nxh, int zlen, int nzout, int fold, T scale, FftPlan pz,
+                                              const cplx_t<T>* __restrict__ twz) {
   using C = cplx_t<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tw = reinterpret_cast<C*>(smem_raw);
   C* b0 = tw + zlen;
   C* b1 = b0 + zlen;
-  const int kx = blockIdx.x, p = blockIdx.y;
+  const int kx = bid.x, p = bid.y;
   for (int m = threadIdx.x; m < zlen; m += blockDim.x) {
     tw[m] = twz[m];
     b0[m] = H[((size_t)p * nxh + kx) * zlen + m];
@@ -148,6 +156,13 @@ __global__ void k_pz_fwd(const cplx_t<T>* __restrict__ H, cplx_t<T>* __restrict_
     else v = S[off + kz];
     out[p * osp + kx * oskx + kz * oskz] = cscale(s, v);
   }
+}
+
+template <typename T>
+__global__ void k_pz_fwd(const cplx_t<T>* __restrict__ H, cplx_t<T>* __restrict__ out, size_t osp, size_t oskx,
+                         size_t oskz, int nxh, int zlen, int nzout, int fold, T scale, FftPlan pz,
+                         const cplx_t<T>* __restrict__ twz) {
+  k_pz_fwd_body<T>(blockIdx, H, out, osp, oskx, oskz, nxh, zlen, nzout, fold, scale, pz, twz);
 }
 
 // Wall-shear feedback law of boundary (PFC/read_write.f90:1483,1498,1514,1527)

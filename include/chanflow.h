@@ -366,18 +366,30 @@ int cfg_set_tiles(cfg_ctx *c, const int *tiles);
 /* An ensemble of independent contexts on one GPU (different grids,
  * Reynolds numbers, seeds, forcing): members of one run of the reference
  * each, advanced together.  cfg_ensemble_timestep runs the first step
- * eagerly and captures one step of every member into a CUDA graph (each
- * member on its own branch); every further step is one graph launch on the
- * ensemble's stream.  autotune != 0 tunes the tiles once per distinct grid.
- * The members stay owned by the caller and must outlive the ensemble; call
- * cfg_ensemble_synchronize before reading or changing a member, and do not
- * change a member's parameters (jet, baseflow, tiles) once the ensemble has
- * stepped (the graph holds them). */
+ * eagerly and captures one step of the ensemble into a CUDA graph; every
+ * further step is one graph launch on the ensemble's stream.  autotune != 0
+ * tunes the tiles once per distinct grid.  The members stay owned by the
+ * caller and must outlive the ensemble; call cfg_ensemble_synchronize before
+ * reading or changing a member, and do not change a member's parameters
+ * (jet, baseflow, fringe, tiles) once the ensemble has stepped (the graph
+ * and the member tables hold them).
+ *
+ * Step layout.  Batched (the default when every member allows it: mixed
+ * precision, one rank, the register-FFT transforms with the v2 rhs kernel,
+ * no LES, no wall feedback): the members fall into classes of the same grid
+ * and tiles, and every kernel of the step runs once per class over a table
+ * of the members' arguments in device memory.  Otherwise, or after
+ * cfg_ensemble_set_batched(e, 0): one graph branch per member.  The results
+ * are the same bit for bit.  cfg_ensemble_set_batched(e, 1) returns
+ * CFG_E_ARG when a member does not allow it; cfg_ensemble_batched tells the
+ * current layout. */
 typedef struct cfg_ensemble cfg_ensemble;
 int cfg_ensemble_create(int nmembers, cfg_ctx *const *members, int autotune, cfg_ensemble **out);
 int cfg_ensemble_timestep(cfg_ensemble *e, int nsteps);
 int cfg_ensemble_synchronize(cfg_ensemble *e);
 void *cfg_ensemble_stream(cfg_ensemble *e);
+int cfg_ensemble_set_batched(cfg_ensemble *e, int on);
+int cfg_ensemble_batched(const cfg_ensemble *e);
 void cfg_ensemble_destroy(cfg_ensemble *e);
 
 /* Learned subgrid-stress closure network (the LES mode of the reference's

@@ -2,7 +2,9 @@
 Reynolds numbers, noise seeds, jet forcing and precisions, tuned once per
 grid and advanced by one CUDA graph launch per step, must reproduce each
 member run alone with the default tiles bit for bit (the tiles change the
-schedule, never the arithmetic)."""
+schedule, never the arithmetic) -- in both step layouts: one graph branch
+per member, and batched (one launch per kernel for each class of equal
+grids, every member's arguments from a table in device memory)."""
 import numpy as np
 import pytest
 
@@ -43,6 +45,10 @@ def test_ensemble_graph_matches_members_alone(cf):
 
     ens_members = [member(cf, *m) for m in MEMBERS]
     ens = cf.Ensemble(ens_members, autotune=True)
+    # an FP64 member: the batched layout is not available
+    assert not ens.batched
+    with pytest.raises(cf.ChanflowError):
+        cf.Ensemble([member(cf, *m) for m in MEMBERS[-2:]], autotune=False, batched=True)
     ens.timestep(steps)
     ens.synchronize()
     for k, f in enumerate(ens_members):
@@ -65,3 +71,53 @@ def test_autotune_restores_state(cf):
     for a, b in zip(f.download_state(), g.download_state()):
         np.testing.assert_array_equal(a, b)
     np.testing.assert_array_equal(f.jet_forcing()[0], g.jet_forcing()[0])
+
+
+# mixed precision only: three classes (48, 64 and 96 points), jets and plain
+# members in the same class, different Reynolds numbers within a class
+BATCH_MEMBERS = [
+    (48, 49, 48, 2000.0, 1001, True, 1),
+    (48, 49, 48, 2600.0, 1002, False, 1),
+    (48, 49, 48, 2100.0, 1006, True, 1),
+    (64, 65, 64, 2300.0, 1003, True, 1),
+    (64, 65, 64, 2800.0, 1007, False, 1),
+    (96, 97, 96, 2900.0, 1004, False, 1),
+    (96, 97, 96, 2200.0, 1008, True, 1),
+]
+
+
+@pytest.mark.parametrize("autotune", [False, True])
+def test_batched_ensemble_matches_members_alone(cf, autotune):
+    steps = 6
+    alone = [member(cf, *m) for m in BATCH_MEMBERS]
+    for f in alone:
+        f.timestep(steps)
+    ref = [f.download_state() for f in alone]
+
+    ens_members = [member(cf, *m) for m in BATCH_MEMBERS]
+    ens = cf.Ensemble(ens_members, autotune=autotune)
+    assert ens.batched
+    ens.timestep(steps)
+    ens.synchronize()
+    for k, f in enumerate(ens_members):
+        got = f.download_state()
+        for a, b in zip(ref[k], got):
+            np.testing.assert_array_equal(a, b)
+        assert f.status() == 0
+        sa, sb = f.scalars(), alone[k].scalars()
+        for key in ("t_total", "dt", "p_grad", "cfl_max"):
+            assert sa[key] == sb[key], key
+        np.testing.assert_array_equal(sa["d_um_dy"], sb["d_um_dy"])
+        if BATCH_MEMBERS[k][5]:
+            np.testing.assert_array_equal(f.jet_forcing()[0], alone[k].jet_forcing()[0])
+    # the layout switch: the next steps in branches continue bit for bit
+    ens.L.cfg_ensemble_set_batched(ens.h, 0)
+    assert not ens.batched
+    ens.timestep(2)
+    ens.synchronize()
+    for f in alone:
+        f.timestep(2)
+    for k, f in enumerate(ens_members):
+        for a, b in zip(alone[k].download_state(), f.download_state()):
+            np.testing.assert_array_equal(a, b)
+    ens.close()
