@@ -463,9 +463,13 @@ struct Impl {
       c->mean_split = false;
     }
     c->use_rhs2 = rhs2_supported(g.ny1) && !getenv("CHANFLOW_RHS_V1");
-    // 16 lanes per wavenumber exists for FP32 only (the FP64 kernel and its
-    // coefficient table stay at 32)
-    c->rhs2_lanes = (f32 && getenv("CHANFLOW_RHS2_LANES") && atoi(getenv("CHANFLOW_RHS2_LANES")) == 16) ? 16 : 32;
+    // lanes per wavenumber: 16 (two wavenumbers per warp) in FP32 up to 128
+    // rows -- fewer idle rows and one cyclic-reduction level fewer than 32;
+    // 32 for taller columns (16 lanes would hold more than 8 rows each) and
+    // in FP64 (its kernel and coefficient table exist for 32 only).
+    // CHANFLOW_RHS2_LANES=16 or 32 overrides the choice in FP32.
+    c->rhs2_lanes = (f32 && g.ny1 <= 128) ? 16 : 32;
+    if (f32 && getenv("CHANFLOW_RHS2_LANES")) c->rhs2_lanes = atoi(getenv("CHANFLOW_RHS2_LANES")) == 16 ? 16 : 32;
     c->rhs2_warps = f32 ? 3 : 2;
     c->twx = make_twiddles<T>(g.nx2);
     c->twz = make_twiddles<T>(g.nz2);

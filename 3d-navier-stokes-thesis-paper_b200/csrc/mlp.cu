@@ -89,7 +89,11 @@ __device__ __forceinline__ void gelu_to_tile(uint32_t taddr, const float* sb, ui
     float z[32];
     tmem_ld32(taddr + 32 * h, z);
 #pragma unroll
-    for (int i = 0; i < 32; ++i) z[i] = gelu(z[i] + sb[32 * h + i]);
+    for (int i = 0; i < 32; i += 2) {
+      const float2 g = gelu2(add2(make_float2(z[i], z[i + 1]), make_float2(sb[32 * h + i], sb[32 * h + i + 1])));
+      z[i] = g.x;
+      z[i + 1] = g.y;
+    }
 #pragma unroll
     for (int q = 0; q < 4; ++q) dst[unit_of(p, 32 * h + 8 * q, TILE)] = pack8(z + 8 * q);
   }

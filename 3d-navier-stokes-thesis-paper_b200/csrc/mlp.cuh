@@ -147,15 +147,48 @@ __device__ __forceinline__ float tanh_hw(float u) {
   asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
   return t;
 }
-constexpr float kGeluC = 0.7978845608028654f, kGeluA = 0.044715f;
+constexpr float kGeluC = 0.7978845608028654f, kGeluA = 0.044715f, kGeluCA = kGeluC * kGeluA;
+// the tanh argument c (z + a z^3) = z (c + c a z^2)
+__device__ __forceinline__ float gelu_arg(float z) { return z * fmaf(z * z, kGeluCA, kGeluC); }
 __device__ __forceinline__ float gelu(float z) {
-  const float t = tanh_hw(kGeluC * z * fmaf(kGeluA * z, z, 1.0f));
-  return 0.5f * z * (1.0f + t);
+  const float h = 0.5f * z;
+  return fmaf(h, tanh_hw(gelu_arg(z)), h);
 }
 __device__ __forceinline__ float gelu_d(float z) {
   const float z2 = z * z;
-  const float t = tanh_hw(kGeluC * z * fmaf(kGeluA, z2, 1.0f));
+  const float t = tanh_hw(gelu_arg(z));
   return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * kGeluC * fmaf(3.0f * kGeluA, z2, 1.0f);
+}
+
+// two lanes per instruction (add/mul/fma.rn.f32x2, sm_100): the same IEEE
+// results as the scalar operations
+__device__ __forceinline__ float2 add2(float2 a, float2 b) {
+  float2 r;
+  asm("{.reg .b64 pa, pb, pr;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+      "add.rn.f32x2 pr, pa, pb;\n\tmov.b64 {%0, %1}, pr;}"
+      : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
+  float2 r;
+  asm("{.reg .b64 pa, pb, pr;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+      "mul.rn.f32x2 pr, pa, pb;\n\tmov.b64 {%0, %1}, pr;}"
+      : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+  float2 r;
+  asm("{.reg .b64 pa, pb, pc, pr;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+      "mov.b64 pc, {%6, %7};\n\tfma.rn.f32x2 pr, pa, pb, pc;\n\tmov.b64 {%0, %1}, pr;}"
+      : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+  return r;
+}
+// gelu of two values, the arithmetic of gelu() two lanes at a time
+__device__ __forceinline__ float2 gelu2(float2 z) {
+  const float2 w = fma2(mul2(z, z), make_float2(kGeluCA, kGeluCA), make_float2(kGeluC, kGeluC));
+  const float2 u = mul2(z, w);
+  const float2 h = mul2(z, make_float2(0.5f, 0.5f));
+  return fma2(h, make_float2(tanh_hw(u.x), tanh_hw(u.y)), h);
 }
 
 // 8 BF16 values as one 16-byte unit
