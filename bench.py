@@ -381,6 +381,12 @@ def run_ensemble(args):
     for f in mem:
         f.close()
     ms_b, tune_s, status, _ = graph_run(True)
+    if args.ensemble_only:
+        # the batched layout alone (for profiling its kernels)
+        print(json.dumps({"metric": "ensemble member-steps/s (C5)", "value": M / (ms_b / 1e3),
+                          "unit": "member·steps/s", "ms_per_step": ms_b, "mpts_steps_per_s": pts / (ms_b / 1e3),
+                          "status": status}), flush=True)
+        return 0
     ms_g, _, status_g, _ = graph_run(False)
     # one call per member per step (no graph), same members, default tiles
     mem = ensemble_members(cf, M)
@@ -837,6 +843,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--slab", type=int, default=0, help="one field in P slab ranks (one process)")
     ap.add_argument("--ensemble", type=int, default=0, help="configuration C5 with M members (one GPU)")
+    ap.add_argument("--ensemble-only", action="store_true", help="time the batched ensemble layout only")
     ap.add_argument("--arnoldi", action="store_true", help="configuration C3 (Arnoldi eigenvalues)")
     ap.add_argument("--arnoldi-maxiter", type=int, default=6, help="Krylov-Schur cycles of the C3 run")
     ap.add_argument("--les", action="store_true", help="configuration C4 (learned-closure LES vs DNS)")
