@@ -187,6 +187,7 @@ SYMBOLS = {
     "cfg_group_destroy": (None, [_VP]),
     "cfg_autotune": (C.c_int, [_VP, C.c_int, _VP]),
     "cfg_set_tiles": (C.c_int, [_VP, _VP]),
+    "cfg_get_tiles": (C.c_int, [_VP, _VP]),
     "cfg_ensemble_create": (C.c_int, [C.c_int, _VP, C.c_int, C.POINTER(_VP)]),
     "cfg_ensemble_timestep": (C.c_int, [_VP, C.c_int]),
     "cfg_ensemble_synchronize": (C.c_int, [_VP]),
@@ -623,6 +624,13 @@ class ChannelFlow:
     def set_tiles(self, tiles):
         t = np.ascontiguousarray(tiles, dtype=np.int32)
         self._chk(self.L.cfg_set_tiles(self.h, _p(t)))
+
+    def tiles(self):
+        """(warps per rhs block, z rows per flux block, planes per inverse and
+        forward z-transform block)."""
+        t = np.zeros(4, dtype=np.int32)
+        self._chk(self.L.cfg_get_tiles(self.h, _p(t)))
+        return [int(v) for v in t]
 
     def synchronize(self):
         self._chk(self.L.cfg_synchronize(self.h))

@@ -442,7 +442,7 @@ struct Impl {
     // split x stage: physical planes written once, fluxes read three of them
     // z rows per flux block: 4 (FP32) or 2 (FP64, half the shared memory)
     c->flux_zr = getenv("CHANFLOW_FLUX_ZR") ? atoi(getenv("CHANFLOW_FLUX_ZR")) : (f32 ? 4 : 2);
-    if (c->flux_zr != 2) c->flux_zr = 4;
+    if (c->flux_zr != 2 && !(c->flux_zr == 8 && f32)) c->flux_zr = 4;   // 8 rows: FP32 only
     // (gP: the x stage's geometry, all kx and this rank's z2 rows)
     const Geom& gp = c->gP;
     c->split_x = c->fast_x && (!getenv("CHANFLOW_FUSED_XFLUX") || c->nranks > 1) && gp.nz2 % 8 == 0 &&
@@ -2641,10 +2641,14 @@ int cfg_autotune(cfg_ctx* c, int trial_steps, int* choice) {
     if (f32) tune(&c->rhs2_warps, {2, 3, 4});
     else tune(&c->rhs2_warps, {1, 2});
   }
-  if (c->split_x) tune(&c->flux_zr, {2, 4});   // a row count that does not split fails its trial
+  // a row count that does not split, or the 8-row block outside the
+  // FP32 nonlinear products, fails its trial
+  if (c->split_x) tune(&c->flux_zr, {2, 4, 8});
   if (c->fast_z) {
-    tune(&c->fYB1, {1, 2, 3, 4});
-    tune(&c->fYB3, {1, 2, 3, 4});
+    // planes per z-transform block (a block too large for its launch fails
+    // its trial)
+    tune(&c->fYB1, {1, 2, 3, 4, 6, 8});
+    tune(&c->fYB3, {1, 2, 3, 4, 6, 8});
   }
   snap_restore(c, snap);
   CK(cudaStreamSynchronize(c->st));
@@ -2663,10 +2667,19 @@ int cfg_autotune(cfg_ctx* c, int trial_steps, int* choice) {
   return CFG_OK;
 }
 
+int cfg_get_tiles(const cfg_ctx* c, int* tiles) {
+  if (!c || !tiles) return CFG_E_ARG;
+  tiles[0] = c->rhs2_warps;
+  tiles[1] = c->flux_zr;
+  tiles[2] = c->fYB1;
+  tiles[3] = c->fYB3;
+  return CFG_OK;
+}
+
 int cfg_set_tiles(cfg_ctx* c, const int* tiles) {
   if (!c || !tiles) return CFG_E_ARG;
   const int w = tiles[0], fz = tiles[1], y1 = tiles[2], y3 = tiles[3];
-  if (w < 1 || w > 4 || (fz != 2 && fz != 4) || y1 < 1 || y1 > 4 || y3 < 1 || y3 > 4 ||
+  if (w < 1 || w > 4 || (fz != 2 && fz != 4 && !(fz == 8 && c->mixed)) || y1 < 1 || y1 > 8 || y3 < 1 || y3 > 8 ||
       (c->split_x && c->gP.nz2 % fz != 0))
     return fail(c, CFG_E_ARG, "cfg_set_tiles: unsupported tiles");
   c->rhs2_warps = w;
@@ -3103,6 +3116,97 @@ static int ens_batched_enqueue(cfg_ensemble* e) {
   return CFG_OK;
 }
 
+// The launch tiles of a batched ensemble, tuned per class on the class's
+// own batched step: coordinate descent over warps per rhs block, z rows per
+// flux block and planes per z-transform block, every member's state,
+// scalars, wall values and jet walk restored before each trial and at the
+// end.  A setting whose launch fails or that sets a device error flag is
+// skipped.
+static int ens_tune_batched(cfg_ensemble* e, int trial_steps) {
+  const int n = (int)e->m.size();
+  int r = ens_build_classes(e);
+  if (r) return r;
+  std::vector<std::vector<int>> groups;
+  for (const EnsClass& k : e->cls) groups.push_back(k.mem);
+  std::vector<TuneSnap> snaps(n);
+  std::vector<int> step0(n);
+  std::vector<long long> launches0(n);
+  for (int i = 0; i < n && !r; ++i) {
+    cfg_ctx* c = e->m[i];
+    step0[i] = c->step;
+    launches0[i] = c->launches;
+    r = snap_take(c, snaps[i]);
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (!r && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)) r = CFG_E_CUDA;
+  if (!r && cudaDeviceSynchronize() != cudaSuccess) r = CFG_E_CUDA;
+  auto trial = [&](int q) -> float {
+    for (int i : groups[q]) {
+      snap_restore(e->m[i], snaps[i]);
+      e->m[i]->step = step0[i];
+    }
+    if (cudaDeviceSynchronize() != cudaSuccess || ens_build_classes(e)) {
+      cudaGetLastError();
+      return -1.f;
+    }
+    EnsClass* k = nullptr;
+    for (EnsClass& x : e->cls)
+      if (x.mem == groups[q]) k = &x;
+    if (!k) return -1.f;
+    bool ok = ens_class_enqueue(e, *k) == CFG_OK && cudaEventRecord(e0, k->st) == cudaSuccess;
+    for (int s = 0; s < trial_steps && ok; ++s) ok = ens_class_enqueue(e, *k) == CFG_OK;
+    ok = ok && cudaEventRecord(e1, k->st) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess;
+    if (!ok) {
+      cudaGetLastError();
+      cudaDeviceSynchronize();
+      cudaGetLastError();
+      return -1.f;
+    }
+    for (int i : groups[q]) {
+      DevScalars h;
+      if (cudaMemcpy(&h, e->m[i]->sc, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess || h.status != 0) return -1.f;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    return ms;
+  };
+  for (int q = 0; q < (int)groups.size() && !r; ++q) {
+    float best = trial(q);
+    if (best < 0.f) continue;   // the class keeps its tiles
+    auto tune = [&](int cfg_ctx::*knob, std::initializer_list<int> vals) {
+      const int keep = e->m[groups[q][0]]->*knob;
+      int bestv = keep;
+      for (int v : vals) {
+        if (v == keep) continue;
+        for (int i : groups[q]) e->m[i]->*knob = v;
+        const float t = trial(q);
+        if (t >= 0.f && t < best) {
+          best = t;
+          bestv = v;
+        }
+      }
+      for (int i : groups[q]) e->m[i]->*knob = bestv;
+    };
+    tune(&cfg_ctx::rhs2_warps, {2, 3, 4});
+    tune(&cfg_ctx::flux_zr, {2, 4, 8});
+    tune(&cfg_ctx::fYB1, {1, 2, 3, 4, 6, 8});
+    tune(&cfg_ctx::fYB3, {1, 2, 3, 4, 6, 8});
+  }
+  for (int i = 0; i < n; ++i) {
+    cfg_ctx* c = e->m[i];
+    if (!snaps[i].bufs.empty()) snap_restore(c, snaps[i]);
+    c->step = step0[i];
+    c->launches = launches0[i];
+    c->mean64_valid = true;
+  }
+  if (cudaDeviceSynchronize() != cudaSuccess && !r) r = CFG_E_CUDA;
+  for (TuneSnap& sn : snaps) snap_free(sn);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  ens_free_classes(e);   // rebuilt by the first step with the chosen tiles
+  return r;
+}
+
 int cfg_ensemble_create(int n, cfg_ctx* const* members, int autotune, cfg_ensemble** out) {
   if (n < 1 || !members || !out) return CFG_E_ARG;
   *out = nullptr;
@@ -3120,7 +3224,14 @@ int cfg_ensemble_create(int n, cfg_ctx* const* members, int autotune, cfg_ensemb
   if (!ok) { cfg_ensemble_destroy(e); return CFG_E_CUDA; }
   e->batched = true;
   for (int i = 0; i < n; ++i) e->batched = e->batched && ens_batchable(members[i]);
-  if (autotune) {
+  bool tune_batched = e->batched && autotune;
+  for (int i = 0; i < n; ++i) tune_batched = tune_batched && members[i]->mean64_valid;
+  if (tune_batched) {
+    // one class per grid first (each grid's default tiles), then per class
+    // on its batched step
+    const int r = ens_tune_batched(e, 2);
+    if (r) { cfg_ensemble_destroy(e); return r; }
+  } else if (autotune) {
     // one trial run per distinct grid and precision; the others take its tiles
     for (int i = 0; i < n; ++i) {
       cfg_ctx* c = e->m[i];

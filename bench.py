@@ -355,6 +355,8 @@ def run_ensemble(args):
     cf = __graft_entry__.load_package()
     M, K, W = args.ensemble, args.steps, args.warmup
 
+    tiles = {}
+
     def graph_run(batched):
         mem = ensemble_members(cf, M)
         t0 = time.perf_counter()
@@ -371,6 +373,7 @@ def run_ensemble(args):
         ms = e0.elapsed_time(e1) / K
         status = [f.status() for f in mem]
         launches = sum(f.launch_count() for f in mem)
+        tiles.update({f"{f.nx}x{f.ny}x{f.nz}" + ("" if batched else " (branches)"): f.tiles() for f in mem})
         ens.close()
         for f in mem:
             f.close()
@@ -412,7 +415,7 @@ def run_ensemble(args):
                        "Re U[2000,3000], seeds 1000+m, jet on odd members, mixed precision, dt 0.0025",
            "members": M, "mpts_total": round(pts, 4),
            "parallelism": "one GPU, one CUDA graph per step, batched (one launch per kernel per grid class)",
-           "autotune_s": round(tune_s, 2)}
+           "autotune_s": round(tune_s, 2), "tiles": tiles}
     line = {"metric": "ensemble member-steps/s (C5)", "value": M / (ms_b / 1e3), "unit": "member·steps/s",
             "n_gpus": 1, "steps": K, "warmup": W, "ms_per_step": ms_b, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)", "config": cfg,

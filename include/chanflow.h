@@ -362,6 +362,7 @@ int cfg_rank_timestep_ordered(cfg_ctx *c, int nsteps, cfg_barrier_fn barrier, vo
  * ints) receives the tiles; cfg_set_tiles sets them directly. */
 int cfg_autotune(cfg_ctx *c, int trial_steps, int *choice);
 int cfg_set_tiles(cfg_ctx *c, const int *tiles);
+int cfg_get_tiles(const cfg_ctx *c, int *tiles);   /* the current 4 tiles */
 
 /* An ensemble of independent contexts on one GPU (different grids,
  * Reynolds numbers, seeds, forcing): members of one run of the reference

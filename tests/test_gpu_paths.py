@@ -2,7 +2,8 @@
 (environment switches read by cfg_create; the defaults are the fast paths):
 CHANFLOW_GENERIC_FFT (shared-memory Stockham FFTs in every transform),
 CHANFLOW_FUSED_XFLUX (inverse x, fluxes and forward x in one kernel),
-CHANFLOW_FLUX_ZR=2 (two z rows per flux block), CHANFLOW_RHS_V1 (the first
+CHANFLOW_FLUX_ZR=2 and =8 (two or, FP32 only, eight z rows per flux
+block), CHANFLOW_RHS_V1 (the first
 per-wavenumber solver) and CHANFLOW_RHS2_LANES=32 (one wavenumber per warp;
 the default at this grid's 34 rows in FP32 is 16 lanes, two wavenumbers per
 warp).
@@ -20,6 +21,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 SWITCHES = [("CHANFLOW_GENERIC_FFT", "1"), ("CHANFLOW_FUSED_XFLUX", "1"), ("CHANFLOW_FLUX_ZR", "2"),
+            ("CHANFLOW_FLUX_ZR", "8"),
             ("CHANFLOW_RHS_V1", "1"), ("CHANFLOW_RHS2_LANES", "32")]
 
 
