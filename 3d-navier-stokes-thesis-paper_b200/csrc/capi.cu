@@ -208,6 +208,7 @@ struct cfg_ctx {
   int rhs2_lanes = 32;
   int rhs2_warps = 3;   // warps (wavenumbers) per k_rhs2 block
   int fYB1 = 1, fYB3 = 1, fZR = 1;
+  int xinv_zb = 0;      // z2 rows per k_xinv_r block (0: 16 in FP32, 8 in FP64), tuned
   // optional per-launch CUDA-event timing on the context stream
   bool prof_on = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -441,10 +442,15 @@ struct Impl {
     if (getenv("CHANFLOW_GENERIC_FFT")) c->fast_x = c->fast_z = false;
     // split x stage: physical planes written once, fluxes read three of them
     // z rows per flux block: 4 (FP32) or 2 (FP64, half the shared memory)
+    // z2 rows per inverse-x block: the default rule unless CHANFLOW_XINV_ROWS
+    // sets 8, 16 or 24 (the tuners also try them)
+    c->xinv_zb = getenv("CHANFLOW_XINV_ROWS") ? atoi(getenv("CHANFLOW_XINV_ROWS")) : 0;
+    if (c->xinv_zb != 8 && !(f32 && (c->xinv_zb == 16 || c->xinv_zb == 24))) c->xinv_zb = 0;
     c->flux_zr = getenv("CHANFLOW_FLUX_ZR") ? atoi(getenv("CHANFLOW_FLUX_ZR")) : (f32 ? 4 : 2);
     if (c->flux_zr != 2 && !(c->flux_zr == 8 && f32)) c->flux_zr = 4;   // 8 rows: FP32 only
     // (gP: the x stage's geometry, all kx and this rank's z2 rows)
     const Geom& gp = c->gP;
+    if (c->xinv_zb && gp.nz2 % c->xinv_zb) c->xinv_zb = 0;
     c->split_x = c->fast_x && (!getenv("CHANFLOW_FUSED_XFLUX") || c->nranks > 1) && gp.nz2 % 8 == 0 &&
                  gp.nz2 % c->flux_zr == 0 && p1_fast_smem(3, g.nx2, f32, gp.nz2, gp.nxh, g.nz) <= 200 * 1024 &&
                  p1_fast_smem(4, g.nx2, f32, c->flux_zr, gp.nxh, g.nz) <= 200 * 1024;
@@ -500,6 +506,7 @@ struct Impl {
     a.FZR = c->flux_zr;
     a.sc = c->scat;
     a.split = (c->mean_split && !lin && !c->les_on) ? 1 : 0;
+    a.XZB = c->xinv_zb;
     if (which == 3 || which == 4) {
       // x stage of the split path on this rank's z2 rows, all kx
       a.g = c->gP;
@@ -2650,6 +2657,9 @@ int cfg_autotune(cfg_ctx* c, int trial_steps, int* choice) {
     tune(&c->fYB1, {1, 2, 3, 4, 6, 8});
     tune(&c->fYB3, {1, 2, 3, 4, 6, 8});
   }
+  // z2 rows per inverse-x block (not one of the four public tiles; a row
+  // count that does not divide the slab fails its trial)
+  if (c->split_x) tune(&c->xinv_zb, {8, 16, 24});
   snap_restore(c, snap);
   CK(cudaStreamSynchronize(c->st));
   snap_free(snap);
@@ -2878,7 +2888,8 @@ static bool ens_same_class(const cfg_ctx* a, const cfg_ctx* b) {
   return x.nx == y.nx && x.ny == y.ny && x.nz == y.nz && x.nx2 == y.nx2 && x.nz2 == y.nz2 && x.nxh == y.nxh &&
          x.ny1 == y.ny1 && x.nw == y.nw && a->gP.nz2 == b->gP.nz2 && a->fYB1 == b->fYB1 && a->fYB3 == b->fYB3 &&
          a->flux_zr == b->flux_zr && a->rhs2_warps == b->rhs2_warps && a->rhs2_lanes == b->rhs2_lanes &&
-         a->mean_split == b->mean_split && a->n_fast == b->n_fast && a->n_prec == b->n_prec;
+         a->mean_split == b->mean_split && a->n_fast == b->n_fast && a->n_prec == b->n_prec &&
+         a->xinv_zb == b->xinv_zb;
 }
 
 // the classes, their streams and their member tables
@@ -3191,6 +3202,7 @@ static int ens_tune_batched(cfg_ensemble* e, int trial_steps) {
     tune(&cfg_ctx::flux_zr, {2, 4, 8});
     tune(&cfg_ctx::fYB1, {1, 2, 3, 4, 6, 8});
     tune(&cfg_ctx::fYB3, {1, 2, 3, 4, 6, 8});
+    tune(&cfg_ctx::xinv_zb, {8, 16, 24});
   }
   for (int i = 0; i < n; ++i) {
     cfg_ctx* c = e->m[i];
@@ -3245,6 +3257,7 @@ int cfg_ensemble_create(int n, cfg_ctx* const* members, int autotune, cfg_ensemb
       if (first >= 0) {
         const cfg_ctx* o = e->m[first];
         const int t[4] = {o->rhs2_warps, o->flux_zr, o->fYB1, o->fYB3};
+        c->xinv_zb = o->xinv_zb;
         const int r = cfg_set_tiles(c, t);
         if (r) { cfg_ensemble_destroy(e); return r; }
       } else {

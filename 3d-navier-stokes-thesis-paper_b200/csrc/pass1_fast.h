@@ -27,6 +27,7 @@ struct P1Launch {
   Scatter sc;           // transposes of a multi-rank run (n == 0: one rank)
   const void* sgs;      // LES subgrid stresses [ny+1][6][nz2][nx2] for k_flux_r, or null
   int split;            // mean split: k_zinv_r drops the mean column, k_flux_r adds it from gd.baseflow
+  int XZB;              // z2 rows per k_xinv_r block: 8, 16 or 24 (FP32), 0 for the default
   cudaStream_t st;
 };
 

@@ -3,7 +3,8 @@
 CHANFLOW_GENERIC_FFT (shared-memory Stockham FFTs in every transform),
 CHANFLOW_FUSED_XFLUX (inverse x, fluxes and forward x in one kernel),
 CHANFLOW_FLUX_ZR=2 and =8 (two or, FP32 only, eight z rows per flux
-block), CHANFLOW_RHS_V1 (the first
+block), CHANFLOW_XINV_ROWS=24 and =8 (z rows per inverse-x block; 24 FP32
+only), CHANFLOW_RHS_V1 (the first
 per-wavenumber solver) and CHANFLOW_RHS2_LANES=32 (one wavenumber per warp;
 the default at this grid's 34 rows in FP32 is 16 lanes, two wavenumbers per
 warp).
@@ -21,7 +22,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 SWITCHES = [("CHANFLOW_GENERIC_FFT", "1"), ("CHANFLOW_FUSED_XFLUX", "1"), ("CHANFLOW_FLUX_ZR", "2"),
-            ("CHANFLOW_FLUX_ZR", "8"),
+            ("CHANFLOW_FLUX_ZR", "8"), ("CHANFLOW_XINV_ROWS", "24"), ("CHANFLOW_XINV_ROWS", "8"),
             ("CHANFLOW_RHS_V1", "1"), ("CHANFLOW_RHS2_LANES", "32")]
 
 
