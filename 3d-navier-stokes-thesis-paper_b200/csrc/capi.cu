@@ -469,13 +469,19 @@ struct Impl {
       c->mean_split = false;
     }
     c->use_rhs2 = rhs2_supported(g.ny1) && !getenv("CHANFLOW_RHS_V1");
-    // lanes per wavenumber: 16 (two wavenumbers per warp) in FP32 up to 128
-    // rows -- fewer idle rows and one cyclic-reduction level fewer than 32;
-    // 32 for taller columns (16 lanes would hold more than 8 rows each) and
-    // in FP64 (its kernel and coefficient table exist for 32 only).
-    // CHANFLOW_RHS2_LANES=16 or 32 overrides the choice in FP32.
-    c->rhs2_lanes = (f32 && g.ny1 <= 128) ? 16 : 32;
-    if (f32 && getenv("CHANFLOW_RHS2_LANES")) c->rhs2_lanes = atoi(getenv("CHANFLOW_RHS2_LANES")) == 16 ? 16 : 32;
+    // lanes per wavenumber in FP32: 8 (four wavenumbers per warp) up to 64
+    // rows, 16 (two) up to 128 -- fewer idle rows and fewer cyclic-reduction
+    // levels than 32; 32 for taller columns (fewer lanes would hold more
+    // than 8 rows each) and in FP64 (its kernel and coefficient table exist
+    // for 32 only).
+    // CHANFLOW_RHS2_LANES=8 (up to 64 rows), 16 (up to 256) or 32 overrides
+    // the choice in FP32.  Not a tuned tile: the lane count sets the
+    // reduction order of the solves, so it changes the rounding.
+    c->rhs2_lanes = !f32 ? 32 : (g.ny1 <= 64 ? 8 : (g.ny1 <= 128 ? 16 : 32));
+    if (f32 && getenv("CHANFLOW_RHS2_LANES")) {
+      const int l = atoi(getenv("CHANFLOW_RHS2_LANES"));
+      if (l == 32 || (l == 16 && g.ny1 <= 256) || (l == 8 && g.ny1 <= 64)) c->rhs2_lanes = l;
+    }
     c->rhs2_warps = f32 ? 3 : 2;
     c->twx = make_twiddles<T>(g.nx2);
     c->twz = make_twiddles<T>(g.nz2);
@@ -1129,7 +1135,8 @@ void cfg_destroy(cfg_ctx* c) {
   if (c->ev_io_done) cudaEventDestroy(c->ev_io_done);
   if (c->st_io) cudaStreamDestroy(c->st_io);
   for (void* q : c->ipc_open) cudaIpcCloseMemHandle(q);
-  void* bufs[] = {c->dgrid, c->fringe, c->vel, c->cru, c->prs, c->mvel64, c->mcru64, c->T1, c->T2, c->P, c->rhs2_tbl, c->rhs2_tbl64, c->jst, c->pp_wy, c->pp_sy, c->pp_acc, c->cbc,
+  void* bufs[] = {c->dgrid, c->fringe, c->vel, c->cru, c->prs, c->mvel64, c->mcru64, c->T1, c->T2, c->P,
+                  c->rhs2_tbl, c->rhs2_tbl64, c->jst, c->pp_wy, c->pp_sy, c->pp_acc, c->cbc,
                   c->sc, c->d_um_dy, c->cflp, c->cflbits, c->l2acc, c->divbits, c->plist, c->pw_H,
                   c->pw_phys, c->pw_phys2, c->pw_in, c->stage, c->twx, c->twz, c->twxs, c->twzs,
                   c->wl_fast, c->wl_prec, c->scat_tab, c->cfl_peers, c->les_S, c->les_F, c->les_Y,
@@ -2648,6 +2655,7 @@ int cfg_autotune(cfg_ctx* c, int trial_steps, int* choice) {
     if (f32) tune(&c->rhs2_warps, {2, 3, 4});
     else tune(&c->rhs2_warps, {1, 2});
   }
+
   // a row count that does not split, or the 8-row block outside the
   // FP32 nonlinear products, fails its trial
   if (c->split_x) tune(&c->flux_zr, {2, 4, 8});
@@ -3045,7 +3053,9 @@ static int ens_class_enqueue(cfg_ensemble* e, EnsClass& k) {
   const int n = (int)k.mem.size(), nj = (int)k.jet.size();
   cfg_ctx* c0 = e->m[k.mem[0]];
   int launches = 0;
-  auto ck = [&](bool ok, const char* what) { return ok && cudaGetLastError() == cudaSuccess ? 0 : fail(c0, CFG_E_CUDA, "%s", what); };
+  auto ck = [&](bool ok, const char* what) {
+    return ok && cudaGetLastError() == cudaSuccess ? 0 : fail(c0, CFG_E_CUDA, "%s", what);
+  };
   const unsigned zb = (unsigned)std::min<size_t>(64, (k.ncbc + 255) / 256);
   k_ens_zero_cbc<<<dim3(zb, n), 256, 0, k.st>>>(k.sm);
   ++launches;
@@ -3066,7 +3076,9 @@ static int ens_class_enqueue(cfg_ensemble* e, EnsClass& k) {
       if (int r = ck(true, "batched k_cfl_finalize")) return r;
     }
     if (nj > 0) {
-      // the wall jet of this substep (PFC/pass2.f90:41-43)
+      // the wall jet of this substep (PFC/pass2.f90:41-43); beside the
+      // nonlinear term on a side stream (from rk 2, when dt is final) it
+      // measured slower: 8.70 against 8.62 ms per 64-member step
       k_jet_walk_b<<<nj, 32, 0, k.st>>>(k.jt, rk);
       k_jet_field_b<<<dim3(k.nz * nj, 3), 128, 0, k.st>>>(k.jt, (unsigned)k.nz);
       const unsigned gxx = (unsigned)(k.nz + 1) / 2;

@@ -82,6 +82,21 @@ static int launch_g32(const Rhs2Launch& a, const Rhs2Launch* tab, int nmem) {
   }
 }
 
+// 8 lanes per wavenumber (FP32 only): M = ceil(ny1/8) <= 8
+static int launch_g8(const Rhs2Launch& a, const Rhs2Launch* tab, int nmem) {
+  const int M = (a.g.ny1 + 7) / 8;
+  switch (M < 2 ? 2 : M) {
+    case 2: return launch_m<float, 2, 8>(a, tab, nmem);
+    case 3: return launch_m<float, 3, 8>(a, tab, nmem);
+    case 4: return launch_m<float, 4, 8>(a, tab, nmem);
+    case 5: return launch_m<float, 5, 8>(a, tab, nmem);
+    case 6: return launch_m<float, 6, 8>(a, tab, nmem);
+    case 7: return launch_m<float, 7, 8>(a, tab, nmem);
+    case 8: return launch_m<float, 8, 8>(a, tab, nmem);
+    default: return -1;
+  }
+}
+
 // 16 lanes per wavenumber (FP32 only): M = ceil(ny1/16) <= 16
 static int launch_g16(const Rhs2Launch& a, const Rhs2Launch* tab, int nmem) {
   const int M = (a.g.ny1 + 15) / 16;
@@ -176,6 +191,7 @@ int rhs2_launch(bool f32, const Rhs2Launch& a) { return rhs2_launch_batch(f32, a
 int rhs2_launch_batch(bool f32, const Rhs2Launch& a, const Rhs2Launch* tab, int nmem) {
   if (tab && nmem < 1) return -1;
   if (f32 && a.lanes == 16) return launch_g16(a, tab, nmem);
+  if (f32 && a.lanes == 8) return launch_g8(a, tab, nmem);
   return f32 ? launch_g32<float>(a, tab, nmem) : launch_g32<double>(a, tab, nmem);
 }
 

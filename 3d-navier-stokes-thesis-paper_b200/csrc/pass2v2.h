@@ -19,7 +19,7 @@ struct Rhs2Launch {
   const int* wlist;
   int nlist;
   int warps;   // warps per block
-  int lanes;   // lanes per wavenumber: 32, or 16 (FP32 only)
+  int lanes;   // lanes per wavenumber: 32, or 16 or 8 (FP32 only)
   const void* tbl;   // coefficient table of rhs2_table for these lanes
   cudaStream_t st;
 };

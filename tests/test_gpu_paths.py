@@ -5,9 +5,9 @@ CHANFLOW_FUSED_XFLUX (inverse x, fluxes and forward x in one kernel),
 CHANFLOW_FLUX_ZR=2 and =8 (two or, FP32 only, eight z rows per flux
 block), CHANFLOW_XINV_ROWS=24 and =8 (z rows per inverse-x block; 24 FP32
 only), CHANFLOW_RHS_V1 (the first
-per-wavenumber solver) and CHANFLOW_RHS2_LANES=32 (one wavenumber per warp;
-the default at this grid's 34 rows in FP32 is 16 lanes, two wavenumbers per
-warp).
+per-wavenumber solver) and CHANFLOW_RHS2_LANES=32 and =16 (one and two
+wavenumbers per warp; the default at this grid's 34 rows in FP32 is 8
+lanes, four wavenumbers per warp).
 Each must give the default path's state after three steps to 1e-12 in FP64
 and 1e-5 in mixed precision (different summation orders).  The alternative
 paths keep the whole velocity in their FP32 transforms, so in mixed precision
@@ -23,7 +23,7 @@ pytestmark = pytest.mark.gpu
 
 SWITCHES = [("CHANFLOW_GENERIC_FFT", "1"), ("CHANFLOW_FUSED_XFLUX", "1"), ("CHANFLOW_FLUX_ZR", "2"),
             ("CHANFLOW_FLUX_ZR", "8"), ("CHANFLOW_XINV_ROWS", "24"), ("CHANFLOW_XINV_ROWS", "8"),
-            ("CHANFLOW_RHS_V1", "1"), ("CHANFLOW_RHS2_LANES", "32")]
+            ("CHANFLOW_RHS_V1", "1"), ("CHANFLOW_RHS2_LANES", "32"), ("CHANFLOW_RHS2_LANES", "16")]
 
 
 def run(cf, grid, env, prec):
