@@ -1554,6 +1554,7 @@ int cfg_set_les(cfg_ctx* c, const cfg_les* l) {
   for (int i = 0; i < 10; ++i) {
     d.in_shift[i] = l->in_shift[i];
     d.in_scale[i] = l->model == 2 ? l->in_scale[i] : 1.0f;
+    d.in_iscale[i] = 1.0 / (double)d.in_scale[i];
   }
   for (int i = 0; i < 6; ++i) {
     d.out_shift[i] = l->out_shift[i];

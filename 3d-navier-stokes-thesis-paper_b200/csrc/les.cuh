@@ -33,6 +33,7 @@ struct LesDev {
   double hx, hz;             // dealiased grid spacing lx/nx2, lz/nz2
   double re;
   float in_shift[10], in_scale[10], out_shift[6], out_scale[6];
+  double in_iscale[10];      // 1 / in_scale
 };
 
 // gradient of the resolved velocity at (plane k, z, x): G[3*i + j] = du_i/dx_j
@@ -61,9 +62,29 @@ __device__ __forceinline__ void les_gradient(const T* __restrict__ P, const Geom
   G[8] = (at(P0, 2, zp, x) - at(P0, 2, zm, x)) * ihz;
 }
 
+// the eddy viscosity's length of plane k, Cs Delta (1 - exp(-y+/A+)): one
+// value per plane, computed once per block (the caller's threads share k)
+__device__ __forceinline__ double les_nut_length(const GridDev& gd, const LesDev& les,
+                                                 const double* __restrict__ d_um_dy, int ny, int k) {
+  const double dy = gd.y[k - 1] - gd.y[k - 2];
+  const double delta = cbrt(les.dx * dy * les.dz);
+  const double utau = sqrt(0.5 * (fabs(d_um_dy[0]) + fabs(d_um_dy[ny - 1])) / les.re);
+  const double yplus = (1.0 - fabs(gd.yh[k - 1])) * utau * les.re;
+  return les.cs * delta * (1.0 - exp(-yplus / les.aplus));
+}
+
+// the length above shared by a block: thread 0 computes it
+__device__ __forceinline__ double les_block_length(const GridDev& gd, const LesDev& les,
+                                                   const double* __restrict__ d_um_dy, int ny, int k) {
+  __shared__ double len;
+  if (threadIdx.x == 0) len = les_nut_length(gd, les, d_um_dy, ny, k);
+  __syncthreads();
+  return len;
+}
+
 // trace-free strain rate (11, 22, 33, 12, 13, 23) and the eddy viscosity
-__device__ __forceinline__ double les_strain_nut(const double G[9], const GridDev& gd, const LesDev& les,
-                                                 const double* __restrict__ d_um_dy, int ny, int k, double Sd[6]) {
+// with the plane's length f
+__device__ __forceinline__ double les_strain_nut(const double G[9], double f, double Sd[6]) {
   const double tr = (G[0] + G[4] + G[8]) / 3.0;
   Sd[0] = G[0] - tr;
   Sd[1] = G[4] - tr;
@@ -73,11 +94,6 @@ __device__ __forceinline__ double les_strain_nut(const double G[9], const GridDe
   Sd[5] = 0.5 * (G[5] + G[7]);
   const double ss = Sd[0] * Sd[0] + Sd[1] * Sd[1] + Sd[2] * Sd[2] + 2.0 * (Sd[3] * Sd[3] + Sd[4] * Sd[4] + Sd[5] * Sd[5]);
   const double smag = sqrt(2.0 * ss);
-  const double dy = gd.y[k - 1] - gd.y[k - 2];
-  const double delta = cbrt(les.dx * dy * les.dz);
-  const double utau = sqrt(0.5 * (fabs(d_um_dy[0]) + fabs(d_um_dy[ny - 1])) / les.re);
-  const double yplus = (1.0 - fabs(gd.yh[k - 1])) * utau * les.re;
-  const double f = les.cs * delta * (1.0 - exp(-yplus / les.aplus));
   return f * f * smag;
 }
 
@@ -88,10 +104,11 @@ template <typename T>
 __global__ void __launch_bounds__(128) k_les_sgs(const T* __restrict__ P, T* __restrict__ S, float* __restrict__ F,
                                                  Geom g, GridDev gd, LesDev les, const double* __restrict__ d_um_dy) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x, z = blockIdx.y, k = 2 + blockIdx.z;
+  const double len = les_block_length(gd, les, d_um_dy, g.ny, k);
   if (x >= g.nx2) return;
   double G[9], Sd[6];
   les_gradient<T>(P, g, gd, les, k, z, x, G);
-  const double nut = les_strain_nut(G, gd, les, d_um_dy, g.ny, k, Sd);
+  const double nut = les_strain_nut(G, len, Sd);
   const size_t cs = (size_t)g.nz2 * g.nx2, o = (size_t)(k - 1) * 6 * cs + (size_t)z * g.nx2 + x;
 #pragma unroll
   for (int c = 0; c < 6; ++c) S[o + c * cs] = (T)(-2.0 * nut * Sd[c]);
@@ -102,7 +119,7 @@ __global__ void __launch_bounds__(128) k_les_sgs(const T* __restrict__ P, T* __r
                           1.0 - fabs(gd.yh[k - 1])};
     float* out = F + (((size_t)(k - 2) * g.nz2 + z) * g.nx2 + x) * 10;
 #pragma unroll
-    for (int i = 0; i < 10; ++i) out[i] = (float)((f[i] - les.in_shift[i]) / les.in_scale[i]);
+    for (int i = 0; i < 10; ++i) out[i] = (float)((f[i] - les.in_shift[i]) * les.in_iscale[i]);
   }
 }
 
@@ -117,6 +134,7 @@ __global__ void __launch_bounds__(128) k_les_blend(const float* __restrict__ F, 
                                                    const double* __restrict__ d_um_dy,
                                                    unsigned long long* __restrict__ nfall) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x, z = blockIdx.y, k = 2 + blockIdx.z;
+  const double len = les_block_length(gd, les, d_um_dy, g.ny, k);
   bool fall = false;
   if (x < g.nx2) {
     const size_t pt = ((size_t)(k - 2) * g.nz2 + z) * g.nx2 + x;
@@ -129,7 +147,7 @@ __global__ void __launch_bounds__(128) k_les_blend(const float* __restrict__ F, 
     G[3] *= sgn;
     G[5] *= sgn;
     G[7] *= sgn;
-    const double nut = les_strain_nut(G, gd, les, d_um_dy, g.ny, k, Sd);
+    const double nut = les_strain_nut(G, len, Sd);
     const float* y = Y + pt * 6;
     double t[6];
 #pragma unroll
