@@ -29,6 +29,7 @@
 #include "io.cuh"
 #include "jet.cuh"
 #include "les.cuh"
+#include "mlp_les.h"
 #include "pass2v2.h"
 #include "planes.cuh"
 #include "restart.h"
@@ -240,7 +241,7 @@ struct cfg_ctx {
   cfg_mlp* les_mlp = nullptr;
   void* les_S = nullptr;
   float* les_F = nullptr;
-  float* les_Y = nullptr;
+  double* les_len = nullptr;   // the eddy viscosity's length per plane (model 2)
   unsigned long long* les_nfall = nullptr;
   unsigned long long les_points = 0;
 };
@@ -618,15 +619,17 @@ struct Impl {
     k_les_sgs<T><<<gr, 128, 0, c->st>>>((const T*)c->P, (T*)c->les_S, F, g, c->gd, c->les, c->d_um_dy);
     CKL();
     if (c->les.model == 2 && F == c->les_F) {
+      // the planes' eddy-viscosity lengths, then the network with the checks
+      // and the blend in its output layer's epilogue (the outputs never go
+      // to memory)
+      k_les_lengths<<<1, 128, 0, c->st>>>(c->les_len, c->gd, c->les, c->d_um_dy, g.ny);
+      CKL();
       prof_begin(c, "k_mlp_fwd");
-      if (cfg_mlp_forward(c->les_mlp, c->les_F, c->les_Y, (long long)c->les_points, c->st) != CFG_OK)
+      const LesBlend<T> b{(T*)c->les_S, c->les_F, c->les_len, c->gd, c->les, g.nx2, g.nz2, c->les_nfall};
+      if (mlp_forward_blend<T>(c->les_mlp, (long long)c->les_points, b, c->st) != CFG_OK)
         return fail(c, CFG_E_CUDA, "closure network launch");
       c->launches++;
       prof_end(c);
-      prof_begin(c, "k_les_blend");
-      k_les_blend<T><<<gr, 128, 0, c->st>>>(c->les_F, (T*)c->les_S, c->les_Y, g, c->gd, c->les, c->d_um_dy,
-                                            c->les_nfall);
-      CKL();
     }
     return CFG_OK;
   }
@@ -1139,7 +1142,7 @@ void cfg_destroy(cfg_ctx* c) {
                   c->rhs2_tbl, c->rhs2_tbl64, c->jst, c->pp_wy, c->pp_sy, c->pp_acc, c->cbc,
                   c->sc, c->d_um_dy, c->cflp, c->cflbits, c->l2acc, c->divbits, c->plist, c->pw_H,
                   c->pw_phys, c->pw_phys2, c->pw_in, c->stage, c->twx, c->twz, c->twxs, c->twzs,
-                  c->wl_fast, c->wl_prec, c->scat_tab, c->cfl_peers, c->les_S, c->les_F, c->les_Y,
+                  c->wl_fast, c->wl_prec, c->scat_tab, c->cfl_peers, c->les_S, c->les_F, c->les_len,
                   c->les_nfall, c->mean_base};
   for (void* b : bufs)
     if (b) cudaFree(b);
@@ -1537,7 +1540,7 @@ int cfg_set_les(cfg_ctx* c, const cfg_les* l) {
   }
   if (l->model == 2 && !c->les_F) {
     if (cudaMalloc(&c->les_F, sizeof(float) * 10 * c->les_points) != cudaSuccess ||
-        cudaMalloc(&c->les_Y, sizeof(float) * 6 * c->les_points) != cudaSuccess)
+        cudaMalloc(&c->les_len, sizeof(double) * (g.ny + 1)) != cudaSuccess)
       return fail(c, CFG_E_NOMEM, "LES closure buffers");
   }
   CK(cudaMemsetAsync(c->les_nfall, 0, 8, c->st));

@@ -123,62 +123,87 @@ __global__ void __launch_bounds__(128) k_les_sgs(const T* __restrict__ P, T* __r
   }
 }
 
-// model 2: the network's stresses Y[(k-2) nz2 nx2 + z nx2 + x][6] where they
-// pass the checks, the eddy viscosity's (already in S) elsewhere; counts the
-// fallbacks into *nfall.  The gradient comes back from the features F (the
-// normalisation and the mirroring undone), not from the planes.  Same grid
-// as k_les_sgs.
+// model 2 at one point: the network's (normalised) stresses y[6] where they
+// pass the checks, the eddy viscosity's (already in S) elsewhere; f[10]: the
+// point's normalised features, len: its plane's eddy-viscosity length, o:
+// the point's offset in S (components cs apart).  The gradient comes back
+// from the features (the normalisation and the mirroring undone), not from
+// the planes.  Returns whether the point falls back.
 template <typename T>
-__global__ void __launch_bounds__(128) k_les_blend(const float* __restrict__ F, T* __restrict__ S,
-                                                   const float* __restrict__ Y, Geom g, GridDev gd, LesDev les,
-                                                   const double* __restrict__ d_um_dy,
-                                                   unsigned long long* __restrict__ nfall) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x, z = blockIdx.y, k = 2 + blockIdx.z;
-  const double len = les_block_length(gd, les, d_um_dy, g.ny, k);
-  bool fall = false;
-  if (x < g.nx2) {
-    const size_t pt = ((size_t)(k - 2) * g.nz2 + z) * g.nx2 + x;
-    const float* f = F + pt * 10;
-    const double sgn = gd.yh[k - 1] > 0.0 ? -1.0 : 1.0;
-    double G[9], Sd[6];
+__device__ __forceinline__ bool les_blend_point(const float* f, const float* y, double len, const GridDev& gd,
+                                                const LesDev& les, int k, T* __restrict__ S, size_t o, size_t cs) {
+  const double sgn = gd.yh[k - 1] > 0.0 ? -1.0 : 1.0;
+  double G[9], Sd[6];
 #pragma unroll
-    for (int i = 0; i < 9; ++i) G[i] = (double)f[i] * les.in_scale[i] + les.in_shift[i];
-    G[1] *= sgn;
-    G[3] *= sgn;
-    G[5] *= sgn;
-    G[7] *= sgn;
-    const double nut = les_strain_nut(G, len, Sd);
-    const float* y = Y + pt * 6;
-    double t[6];
+  for (int i = 0; i < 9; ++i) G[i] = (double)f[i] * les.in_scale[i] + les.in_shift[i];
+  G[1] *= sgn;
+  G[3] *= sgn;
+  G[5] *= sgn;
+  G[7] *= sgn;
+  const double nut = les_strain_nut(G, len, Sd);
+  double t[6];
 #pragma unroll
-    for (int c = 0; c < 6; ++c) t[c] = les.out_shift[c] + les.out_scale[c] * (double)y[c];
-    if (gd.yh[k - 1] > 0.0) {   // back from the mirrored frame: 12 and 23 flip
-      t[3] = -t[3];
-      t[5] = -t[5];
-    }
-    bool ok = true;
-#pragma unroll
-    for (int c = 0; c < 6; ++c) ok = ok && isfinite(t[c]);
-    // realizability of the stress tensor (positive semi-definite)
-    ok = ok && t[0] >= 0.0 && t[1] >= 0.0 && t[2] >= 0.0 && t[3] * t[3] <= t[0] * t[1] &&
-         t[4] * t[4] <= t[0] * t[2] && t[5] * t[5] <= t[1] * t[2];
-    const double det = t[0] * (t[1] * t[2] - t[5] * t[5]) - t[3] * (t[3] * t[2] - t[5] * t[4]) +
-                       t[4] * (t[3] * t[5] - t[1] * t[4]);
-    ok = ok && det >= 0.0;
-    // backscatter: the transfer -tau:S against the eddy viscosity's
-    const double eps_nn = -(t[0] * Sd[0] + t[1] * Sd[1] + t[2] * Sd[2] + 2.0 * (t[3] * Sd[3] + t[4] * Sd[4] + t[5] * Sd[5]));
-    const double eps_ev = 2.0 * nut *
-                          (Sd[0] * Sd[0] + Sd[1] * Sd[1] + Sd[2] * Sd[2] + 2.0 * (Sd[3] * Sd[3] + Sd[4] * Sd[4] + Sd[5] * Sd[5]));
-    ok = ok && eps_nn >= -les.beta * eps_ev;
-    if (ok) {
-      const size_t cs = (size_t)g.nz2 * g.nx2, o = (size_t)(k - 1) * 6 * cs + (size_t)z * g.nx2 + x;
-#pragma unroll
-      for (int c = 0; c < 6; ++c) S[o + c * cs] = (T)t[c];
-    }
-    fall = !ok;
+  for (int c = 0; c < 6; ++c) t[c] = les.out_shift[c] + les.out_scale[c] * (double)y[c];
+  if (gd.yh[k - 1] > 0.0) {   // back from the mirrored frame: 12 and 23 flip
+    t[3] = -t[3];
+    t[5] = -t[5];
   }
-  const unsigned m = __ballot_sync(0xffffffffu, fall);
-  if ((threadIdx.x & 31) == 0 && m) atomicAdd(nfall, (unsigned long long)__popc(m));
+  bool ok = true;
+#pragma unroll
+  for (int c = 0; c < 6; ++c) ok = ok && isfinite(t[c]);
+  // realizability of the stress tensor (positive semi-definite)
+  ok = ok && t[0] >= 0.0 && t[1] >= 0.0 && t[2] >= 0.0 && t[3] * t[3] <= t[0] * t[1] &&
+       t[4] * t[4] <= t[0] * t[2] && t[5] * t[5] <= t[1] * t[2];
+  const double det = t[0] * (t[1] * t[2] - t[5] * t[5]) - t[3] * (t[3] * t[2] - t[5] * t[4]) +
+                     t[4] * (t[3] * t[5] - t[1] * t[4]);
+  ok = ok && det >= 0.0;
+  // backscatter: the transfer -tau:S against the eddy viscosity's
+  const double eps_nn = -(t[0] * Sd[0] + t[1] * Sd[1] + t[2] * Sd[2] + 2.0 * (t[3] * Sd[3] + t[4] * Sd[4] + t[5] * Sd[5]));
+  const double eps_ev = 2.0 * nut *
+                        (Sd[0] * Sd[0] + Sd[1] * Sd[1] + Sd[2] * Sd[2] + 2.0 * (Sd[3] * Sd[3] + Sd[4] * Sd[4] + Sd[5] * Sd[5]));
+  ok = ok && eps_nn >= -les.beta * eps_ev;
+  if (ok) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) S[o + c * cs] = (T)t[c];
+  }
+  return !ok;
 }
+
+// the eddy-viscosity length of every interior plane: len[k] for k = 2 .. ny
+// (one block)
+static __global__ void k_les_lengths(double* __restrict__ len, GridDev gd, LesDev les,
+                                     const double* __restrict__ d_um_dy, int ny) {
+  for (int k = 2 + threadIdx.x; k <= ny; k += blockDim.x) len[k] = les_nut_length(gd, les, d_um_dy, ny, k);
+}
+
+// the blend of the points of the network's outputs, run by the output layer
+// of the network's forward kernel (mlp_les.h): the outputs never go to memory
+template <typename T>
+struct LesBlend {
+  T* S;                       // S[pl][6][nz2][nx2]
+  const float* F;             // features F[pt][10]
+  const double* len;          // len[k], k_les_lengths
+  GridDev gd;
+  LesDev les;
+  int nx2, nz2;
+  unsigned long long* nfall;
+  // point pt = (k - 2) nz2 nx2 + z nx2 + x with its network outputs y[6];
+  // every lane of the warp calls it (valid false past the last point)
+  __device__ __forceinline__ void operator()(long long pt, bool valid, const float* y) const {
+    bool fall = false;
+    if (valid) {
+      const long long plane = (long long)nz2 * nx2;
+      const int k = 2 + (int)(pt / plane);
+      const long long rem = pt - (long long)(k - 2) * plane;
+      const size_t cs = (size_t)plane, o = (size_t)(k - 1) * 6 * cs + (size_t)rem;
+      float f[10];
+#pragma unroll
+      for (int i = 0; i < 10; ++i) f[i] = __ldg(F + pt * 10 + i);
+      fall = les_blend_point<T>(f, y, len[k], gd, les, k, S, o, cs);
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, fall);
+    if ((threadIdx.x & 31) == 0 && m) atomicAdd(nfall, (unsigned long long)__popc(m));
+  }
+};
 
 }  // namespace cfd

@@ -12,6 +12,7 @@
 
 #include "chanflow.h"
 #include "mlp.cuh"
+#include "mlp_les.h"
 
 using namespace cfd::mlp;
 
@@ -113,9 +114,23 @@ __device__ __forceinline__ void sync_for_mma() {
 }
 
 // ------------------------------------------------------------- kernels
-// Inference: y[n][6] = MLP(x[n][10]), persistent over tiles of 128 points.
+// the outputs of a point: stored as y[row][6]
+struct PlainOut {
+  float* y;
+  __device__ __forceinline__ void operator()(long long row, bool valid, const float* v) const {
+    if (valid) {
+#pragma unroll
+      for (int c = 0; c < OUT; ++c) y[row * OUT + c] = v[c];
+    }
+  }
+};
+
+// Inference: MLP(x[n][10]) of every point handed to out (PlainOut, or the
+// LES blend), persistent over tiles of 128 points.  out is called by every
+// lane (valid false past n).
+template <class Out>
 __global__ void __launch_bounds__(128) k_mlp_fwd(const uint4* __restrict__ img, const float* __restrict__ bias,
-                                                 const float* __restrict__ x, float* __restrict__ y, long long n,
+                                                 const float* __restrict__ x, Out out, long long n,
                                                  int* __restrict__ err) {
   extern __shared__ __align__(128) uint4 sm[];
   __shared__ __align__(8) uint64_t bar;
@@ -157,10 +172,9 @@ __global__ void __launch_bounds__(128) k_mlp_fwd(const uint4* __restrict__ img, 
       } else {
         float z[16];
         tmem_ld16(tlane, z);
-        if (row < n) {
 #pragma unroll
-          for (int c = 0; c < OUT; ++c) y[row * OUT + c] = z[c] + sb[bias_base(3) + c];
-        }
+        for (int c = 0; c < OUT; ++c) z[c] += sb[bias_base(3) + c];
+        out(row, row < n, z);
       }
     }
     fence_before_sync();
@@ -394,7 +408,12 @@ int cfg_mlp_create(int device, cfg_mlp** out) {
   cudaMemset(m->loss, 0, sizeof(float) + sizeof(int));
   cudaMemset(m->img, 0, IMG_UNITS * sizeof(uint4));   // the padding stays zero
   cudaMemset(m->bias, 0, NBIAS * sizeof(float));
-  if (cudaFuncSetAttribute(k_mlp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_FWD) != cudaSuccess ||
+  if (cudaFuncSetAttribute(k_mlp_fwd<PlainOut>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_FWD) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(k_mlp_fwd<cfd::LesBlend<float>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)SMEM_FWD) != cudaSuccess ||
+      cudaFuncSetAttribute(k_mlp_fwd<cfd::LesBlend<double>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)SMEM_FWD) != cudaSuccess ||
       cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_TRAIN) != cudaSuccess ||
       cudaDeviceSynchronize() != cudaSuccess) {
     cfg_mlp_destroy(m);
@@ -440,7 +459,7 @@ int cfg_mlp_forward(cfg_mlp* m, const float* x, float* y, long long n, void* str
   // would hold eight); a grid past what is resident leaves a second,
   // partial wave (measured 2.5x slower)
   const int grid = (int)(ntiles < 5LL * m->nsm ? ntiles : 5LL * m->nsm);
-  k_mlp_fwd<<<grid, 128, SMEM_FWD, (cudaStream_t)stream>>>(m->img, m->bias, x, y, n, m->err);
+  k_mlp_fwd<PlainOut><<<grid, 128, SMEM_FWD, (cudaStream_t)stream>>>(m->img, m->bias, x, PlainOut{y}, n, m->err);
   return cudaGetLastError() == cudaSuccess ? CFG_OK : CFG_E_CUDA;
 }
 
@@ -490,3 +509,18 @@ int cfg_mlp_status(cfg_mlp* m) {
 }
 
 }  // extern "C"
+
+namespace cfd {
+template <typename T>
+int mlp_forward_blend(cfg_mlp* m, long long n, const LesBlend<T>& b, void* stream) {
+  if (!m || n < 0 || (n > 0 && (!b.F || !b.S || !b.len || !b.nfall))) return CFG_E_ARG;
+  if (n == 0) return CFG_OK;
+  cudaSetDevice(m->dev);
+  const long long ntiles = (n + TILE - 1) / TILE;
+  const int grid = (int)(ntiles < 5LL * m->nsm ? ntiles : 5LL * m->nsm);
+  k_mlp_fwd<LesBlend<T>><<<grid, 128, SMEM_FWD, (cudaStream_t)stream>>>(m->img, m->bias, b.F, b, n, m->err);
+  return cudaGetLastError() == cudaSuccess ? CFG_OK : CFG_E_CUDA;
+}
+template int mlp_forward_blend<float>(cfg_mlp*, long long, const LesBlend<float>&, void*);
+template int mlp_forward_blend<double>(cfg_mlp*, long long, const LesBlend<double>&, void*);
+}  // namespace cfd
