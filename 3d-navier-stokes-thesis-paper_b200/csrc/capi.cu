@@ -3143,11 +3143,11 @@ static int ens_batched_enqueue(cfg_ensemble* e) {
   return CFG_OK;
 }
 
-// The launch tiles of a batched ensemble, tuned per class on the class's
-// own batched step: coordinate descent over warps per rhs block, z rows per
-// flux block and planes per z-transform block, every member's state,
-// scalars, wall values and jet walk restored before each trial and at the
-// end.  A setting whose launch fails or that sets a device error flag is
+// The launch tiles of a batched ensemble, tuned per class on the batched
+// step of the whole ensemble: coordinate descent over warps per rhs block,
+// z rows per flux block, planes per z-transform block and z rows per
+// inverse-x block, one class at a time, every member's state, scalars, wall
+// values and jet walk restored before each trial and at the end.  A setting whose launch fails or that sets a device error flag is
 // skipped.
 static int ens_tune_batched(cfg_ensemble* e, int trial_steps) {
   const int n = (int)e->m.size();
@@ -3167,8 +3167,12 @@ static int ens_tune_batched(cfg_ensemble* e, int trial_steps) {
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (!r && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)) r = CFG_E_CUDA;
   if (!r && cudaDeviceSynchronize() != cudaSuccess) r = CFG_E_CUDA;
+  // one trial of class q's current tiles: the whole batched step, every
+  // class at once as the graph runs them, so that a class's tiles are judged
+  // by what they cost beside the others (alone, a small class favours many
+  // small blocks that only fill an otherwise idle GPU)
   auto trial = [&](int q) -> float {
-    for (int i : groups[q]) {
+    for (int i = 0; i < n; ++i) {
       snap_restore(e->m[i], snaps[i]);
       e->m[i]->step = step0[i];
     }
@@ -3176,20 +3180,19 @@ static int ens_tune_batched(cfg_ensemble* e, int trial_steps) {
       cudaGetLastError();
       return -1.f;
     }
-    EnsClass* k = nullptr;
-    for (EnsClass& x : e->cls)
-      if (x.mem == groups[q]) k = &x;
-    if (!k) return -1.f;
-    bool ok = ens_class_enqueue(e, *k) == CFG_OK && cudaEventRecord(e0, k->st) == cudaSuccess;
-    for (int s = 0; s < trial_steps && ok; ++s) ok = ens_class_enqueue(e, *k) == CFG_OK;
-    ok = ok && cudaEventRecord(e1, k->st) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess;
+    bool found = false;
+    for (const EnsClass& x : e->cls) found = found || x.mem == groups[q];
+    if (!found) return -1.f;
+    bool ok = ens_batched_enqueue(e) == CFG_OK && cudaEventRecord(e0, e->st) == cudaSuccess;
+    for (int s = 0; s < trial_steps && ok; ++s) ok = ens_batched_enqueue(e) == CFG_OK;
+    ok = ok && cudaEventRecord(e1, e->st) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess;
     if (!ok) {
       cudaGetLastError();
       cudaDeviceSynchronize();
       cudaGetLastError();
       return -1.f;
     }
-    for (int i : groups[q]) {
+    for (int i = 0; i < n; ++i) {
       DevScalars h;
       if (cudaMemcpy(&h, e->m[i]->sc, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess || h.status != 0) return -1.f;
     }
@@ -3255,9 +3258,9 @@ int cfg_ensemble_create(int n, cfg_ctx* const* members, int autotune, cfg_ensemb
   bool tune_batched = e->batched && autotune;
   for (int i = 0; i < n; ++i) tune_batched = tune_batched && members[i]->mean64_valid;
   if (tune_batched) {
-    // one class per grid first (each grid's default tiles), then per class
-    // on its batched step
-    const int r = ens_tune_batched(e, 2);
+    // one class per grid first (each grid's default tiles), tuned one class
+    // at a time on the whole batched step
+    const int r = ens_tune_batched(e, 3);
     if (r) { cfg_ensemble_destroy(e); return r; }
   } else if (autotune) {
     // one trial run per distinct grid and precision; the others take its tiles

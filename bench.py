@@ -410,7 +410,7 @@ def run_ensemble(args):
     big = make_flow(cf, NX, NY, NZ, cf.MIXED, 0)
     big.autotune(3)   # as the headline run does
     big.timestep(3)
-    ms_big = timed_steps(torch, big, 20)[0] / 20
+    ms_big = timed_steps(torch, big, 50)[0] / 50
     big.close()
     big_rate = mpts(NX, NY, NZ) / (ms_big / 1e3)
     rate = pts / (ms_b / 1e3)
