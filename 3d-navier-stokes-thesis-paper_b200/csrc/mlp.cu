@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(128) k_mlp_fwd(const uint4* __restrict__ img, 
   fence_after_sync();
   const uint32_t tm = tslot, tlane = tm + ((uint32_t)(32 * warp) << 16);
   const uint32_t sbase = smem_u32(sm);
-  const uint32_t sW = sbase + Smem::W * 16, sX0 = sbase + Smem::X0 * 16, sX1 = sbase + Smem::X1 * 16;
+  const uint32_t sW = sbase + Smem::W * 16, sX = sbase + Smem::FWD_ACT * 16;
   uint32_t phase = 0;
   bool ok = true;
   const long long ntiles = (n + TILE - 1) / TILE;
@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(128) k_mlp_fwd(const uint4* __restrict__ img, 
       sync_for_mma();
       if (p == 0) {
         fence_after_sync();
-        issue_forward(tm, l == 0 ? sX0 : sX1, sW, l);
+        issue_forward(tm, sX, sW, l);
         mma_commit(&bar);
       }
       ok = __syncthreads_and(mbar_wait(&bar, phase));   // uniform across the block
@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(128) k_mlp_fwd(const uint4* __restrict__ img, 
       fence_after_sync();
       if (!ok) break;
       if (l < 3) {
-        gelu_to_tile(tlane, sb + bias_base(l), sm + Smem::X1, p);
+        gelu_to_tile(tlane, sb + bias_base(l), sm + Smem::FWD_ACT, p);
       } else {
         float z[16];
         tmem_ld16(tlane, z);
@@ -415,6 +415,14 @@ int cfg_mlp_create(int device, cfg_mlp** out) {
       cudaFuncSetAttribute(k_mlp_fwd<cfd::LesBlend<double>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)SMEM_FWD) != cudaSuccess ||
       cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_TRAIN) != cudaSuccess ||
+      // the whole of the SM's on-chip memory as shared memory: six forward
+      // CTAs per SM
+      cudaFuncSetAttribute(k_mlp_fwd<PlainOut>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           (int)cudaSharedmemCarveoutMaxShared) != cudaSuccess ||
+      cudaFuncSetAttribute(k_mlp_fwd<cfd::LesBlend<float>>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           (int)cudaSharedmemCarveoutMaxShared) != cudaSuccess ||
+      cudaFuncSetAttribute(k_mlp_fwd<cfd::LesBlend<double>>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           (int)cudaSharedmemCarveoutMaxShared) != cudaSuccess ||
       cudaDeviceSynchronize() != cudaSuccess) {
     cfg_mlp_destroy(m);
     return CFG_E_CUDA;
@@ -455,10 +463,10 @@ int cfg_mlp_forward(cfg_mlp* m, const float* x, float* y, long long n, void* str
   if (n == 0) return CFG_OK;
   cudaSetDevice(m->dev);
   const long long ntiles = (n + TILE - 1) / TILE;
-  // persistent: five CTAs per SM, as many as the shared memory holds (TMEM
+  // persistent: six CTAs per SM, as many as the shared memory holds (TMEM
   // would hold eight); a grid past what is resident leaves a second,
   // partial wave (measured 2.5x slower)
-  const int grid = (int)(ntiles < 5LL * m->nsm ? ntiles : 5LL * m->nsm);
+  const int grid = (int)(ntiles < 6LL * m->nsm ? ntiles : 6LL * m->nsm);
   k_mlp_fwd<PlainOut><<<grid, 128, SMEM_FWD, (cudaStream_t)stream>>>(m->img, m->bias, x, PlainOut{y}, n, m->err);
   return cudaGetLastError() == cudaSuccess ? CFG_OK : CFG_E_CUDA;
 }
@@ -517,7 +525,7 @@ int mlp_forward_blend(cfg_mlp* m, long long n, const LesBlend<T>& b, void* strea
   if (n == 0) return CFG_OK;
   cudaSetDevice(m->dev);
   const long long ntiles = (n + TILE - 1) / TILE;
-  const int grid = (int)(ntiles < 5LL * m->nsm ? ntiles : 5LL * m->nsm);
+  const int grid = (int)(ntiles < 6LL * m->nsm ? ntiles : 6LL * m->nsm);
   k_mlp_fwd<LesBlend<T>><<<grid, 128, SMEM_FWD, (cudaStream_t)stream>>>(m->img, m->bias, b.F, b, n, m->err);
   return cudaGetLastError() == cudaSuccess ? CFG_OK : CFG_E_CUDA;
 }

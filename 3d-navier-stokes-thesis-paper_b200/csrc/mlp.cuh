@@ -210,7 +210,11 @@ struct Smem {
   static constexpr int X2 = X1 + TILE * H / 8;
   static constexpr int X3 = X2 + TILE * H / 8;
   static constexpr int DZ = X3 + TILE * H / 8;              // 128 x 128 gradient tile (upper half zero)
-  static constexpr int END_FWD = X1 + TILE * H / 8;         // inference: X0 and one activation tile
+  // inference: the input tile and the activation tile share one buffer at
+  // X0 (a layer's product has completed before its epilogue overwrites its
+  // input), so that six CTAs fit on an SM
+  static constexpr int FWD_ACT = X0;
+  static constexpr int END_FWD = FWD_ACT + TILE * H / 8;
   static constexpr int END_TRAIN = DZ + TILE * 128 / 8;
 };
 
