@@ -100,11 +100,12 @@ __device__ __forceinline__ void gelu_to_tile(uint32_t taddr, const float* sb, ui
   }
 }
 
-// the warp's sum over its 32 points of v, added to *dst by lane 0
-__device__ __forceinline__ void warp_sum_add(float v, float* dst) {
+// the warp's sum over its 32 points of v (a fixed shuffle tree), stored to
+// *dst by lane 0
+__device__ __forceinline__ void warp_sum_to(float v, float* dst) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  if ((threadIdx.x & 31) == 0) atomicAdd(dst, v);
+  if ((threadIdx.x & 31) == 0) *dst = v;
 }
 
 __device__ __forceinline__ void sync_for_mma() {
@@ -189,17 +190,20 @@ __global__ void __launch_bounds__(128) k_mlp_fwd(const uint4* __restrict__ img, 
 
 // Training: one tile of the batch per CTA.  Forward with the pre-activations
 // kept in TMEM, mean-square loss against t over the 6 outputs, backward, and
-// the tile's weight and bias gradients added to grad (FP32, flat parameter
-// layout) and its loss to *loss.
+// the tile's weight and bias gradients (FP32, flat parameter layout) and its
+// loss (at NPARAM) stored to its own slice part[blockIdx.x][PART_STRIDE]:
+// every weight gradient by the one thread that holds it, every bias gradient
+// and the loss as the sum of the four warps' sums in warp order, so that the
+// slice does not depend on the order in which warps or tiles finish.
 __global__ void __launch_bounds__(128, 1) k_mlp_train(const uint4* __restrict__ img, const float* __restrict__ bias,
                                                       const float* __restrict__ x, const float* __restrict__ t,
                                                       const int* __restrict__ idx, int batch,
-                                                      float* __restrict__ grad, float* __restrict__ loss,
-                                                      int* __restrict__ err) {
+                                                      float* __restrict__ part, int* __restrict__ err) {
   extern __shared__ __align__(128) uint4 sm[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t tslot;
   __shared__ float sb[NBIAS];
+  __shared__ float sg[4][H + 1];   // per-warp sums: bias gradients, the loss at H
   const int p = threadIdx.x, warp = p >> 5, lane = p & 31;
   for (int i = p; i < IMG_UNITS; i += 128) sm[Smem::W + i] = img[i];
   for (int i = p; i < NBIAS; i += 128) sb[i] = bias[i];
@@ -209,6 +213,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_train(const uint4* __restrict__ 
     mbar_init(&bar, 1);
     fence_mbar_init();
   }
+  float* const grad = part + (size_t)blockIdx.x * PART_STRIDE;
   const int r = blockIdx.x * TILE + p;
   const bool valid = r < batch;
   const long long row = valid ? (long long)idx[r] : 0;
@@ -257,9 +262,11 @@ __global__ void __launch_bounds__(128, 1) k_mlp_train(const uint4* __restrict__ 
     sm[Smem::DZ + unit_of(p, 0, TILE)] = pack8(dz);
     sm[Smem::DZ + unit_of(p, 8, TILE)] = pack8(dz + 8);
 #pragma unroll
-    for (int c = 0; c < OUT; ++c) warp_sum_add(dz[c], grad + OFF_B3 + c);
-    warp_sum_add(lsum / (6.0f * (float)batch), loss);
+    for (int c = 0; c < OUT; ++c) warp_sum_to(dz[c], &sg[warp][c]);
+    warp_sum_to(lsum / (6.0f * (float)batch), &sg[warp][H]);
     sync_for_mma();
+    if (p < OUT) grad[OFF_B3 + p] = sg[0][p] + sg[1][p] + sg[2][p] + sg[3][p];
+    if (p == TILE - 1) grad[NPARAM] = sg[0][H] + sg[1][H] + sg[2][H] + sg[3][H];
   }
   // backward through layers 3, 2, 1 (weight and input gradients), then the
   // weight gradient of layer 0
@@ -282,7 +289,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_train(const uint4* __restrict__ 
         float v[16];
         tmem_ld16(tlane + TM_DW, v);
         if (n < L.nreal)
-          for (int k = 0; k < L.kreal; ++k) atomicAdd(grad + L.woff + n * L.kreal + k, v[k]);
+          for (int k = 0; k < L.kreal; ++k) grad[L.woff + n * L.kreal + k] = v[k];
       } else {
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
@@ -290,7 +297,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_train(const uint4* __restrict__ 
           tmem_ld32(tlane + TM_DW + 32 * h, v);
           if (n < L.nreal)
 #pragma unroll
-            for (int k = 0; k < 32; ++k) atomicAdd(grad + L.woff + n * L.kreal + 32 * h + k, v[k]);
+            for (int k = 0; k < 32; ++k) grad[L.woff + n * L.kreal + 32 * h + k] = v[k];
         }
       }
     }
@@ -307,16 +314,31 @@ __global__ void __launch_bounds__(128, 1) k_mlp_train(const uint4* __restrict__ 
 #pragma unroll
         for (int q = 0; q < 4; ++q) sm[Smem::DZ + unit_of(p, 32 * h + 8 * q, TILE)] = pack8(dx + 8 * q);
 #pragma unroll
-        for (int i = 0; i < 32; ++i) warp_sum_add(dx[i], grad + layer(lp).boff + 32 * h + i);
+        for (int i = 0; i < 32; ++i) warp_sum_to(dx[i], &sg[warp][32 * h + i]);
       }
     }
     sync_for_mma();
+    // the bias gradient of layer l - 1 (sg is next written after the next
+    // product's barrier)
+    if (l > 0 && p < H) grad[layer(l - 1).boff + p] = sg[0][p] + sg[1][p] + sg[2][p] + sg[3][p];
   }
   if (!ok && p == 0) atomicExch(err, 1);
   fence_before_sync();
   __syncthreads();
   fence_after_sync();
   if (warp == 0) tmem_dealloc(tm, TM_TRAIN_COLS);
+}
+
+// the batch's tile slices summed in tile order into the gradient and the loss
+// accumulators (the same sums, bit for bit, on every run)
+__global__ void k_mlp_reduce(const float* __restrict__ part, int ntiles, float* __restrict__ G,
+                             float* __restrict__ loss) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > NPARAM) return;
+  float s = 0.f;
+  for (int b = 0; b < ntiles; ++b) s += part[(size_t)b * PART_STRIDE + i];
+  if (i < NPARAM) G[i] += s;
+  else *loss += s;
 }
 
 // weight images and padded biases from the FP32 parameter vector
@@ -368,6 +390,8 @@ struct cfg_mlp {
   int* err = nullptr;
   uint4* img = nullptr;   // [IMG_UNITS] BF16 weight images
   float* bias = nullptr;  // [NBIAS]
+  float* part = nullptr;  // [part_tiles][PART_STRIDE] per-tile gradients of a batch
+  int part_tiles = 0;
   long long step = 0;
   int nsm = 148;
 };
@@ -375,6 +399,7 @@ struct cfg_mlp {
 namespace {
 constexpr size_t SMEM_FWD = (size_t)Smem::END_FWD * 16;
 constexpr size_t SMEM_TRAIN = 120 * 1024;   // >= END_TRAIN*16; one CTA per SM (512 TMEM columns)
+constexpr int PART_TILES0 = 512;             // per-tile gradient slices held from creation (batch 65536)
 static_assert((size_t)Smem::END_TRAIN * 16 <= SMEM_TRAIN, "training tile plan exceeds its shared memory");
 }
 
@@ -395,7 +420,9 @@ int cfg_mlp_create(int device, cfg_mlp** out) {
   bool ok = cudaMalloc(&m->P, 4 * NPARAM * sizeof(float)) == cudaSuccess &&
             cudaMalloc(&m->loss, sizeof(float) + sizeof(int)) == cudaSuccess &&
             cudaMalloc(&m->img, IMG_UNITS * sizeof(uint4)) == cudaSuccess &&
-            cudaMalloc(&m->bias, NBIAS * sizeof(float)) == cudaSuccess;
+            cudaMalloc(&m->bias, NBIAS * sizeof(float)) == cudaSuccess &&
+            cudaMalloc(&m->part, (size_t)PART_TILES0 * PART_STRIDE * sizeof(float)) == cudaSuccess;
+  if (ok) m->part_tiles = PART_TILES0;
   if (!ok) {
     cfg_mlp_destroy(m);
     return CFG_E_NOMEM;
@@ -438,6 +465,7 @@ void cfg_mlp_destroy(cfg_mlp* m) {
   cudaFree(m->loss);
   cudaFree(m->img);
   cudaFree(m->bias);
+  cudaFree(m->part);
   delete m;
 }
 
@@ -474,8 +502,18 @@ int cfg_mlp_forward(cfg_mlp* m, const float* x, float* y, long long n, void* str
 int cfg_mlp_accumulate_grad(cfg_mlp* m, const float* x, const float* t, const int* idx, int batch, void* stream) {
   if (!m || !x || !t || !idx || batch <= 0) return CFG_E_ARG;
   cudaSetDevice(m->dev);
-  k_mlp_train<<<(batch + TILE - 1) / TILE, 128, SMEM_TRAIN, (cudaStream_t)stream>>>(m->img, m->bias, x, t, idx, batch,
-                                                                                  m->G, m->loss, m->err);
+  const int ntiles = (batch + TILE - 1) / TILE;
+  if (ntiles > m->part_tiles) {
+    // a larger batch than any before: the slices grow (cudaFree waits for
+    // the kernels still reading the old ones)
+    cudaFree(m->part);
+    m->part = nullptr;
+    m->part_tiles = 0;
+    if (cudaMalloc(&m->part, (size_t)ntiles * PART_STRIDE * sizeof(float)) != cudaSuccess) return CFG_E_NOMEM;
+    m->part_tiles = ntiles;
+  }
+  k_mlp_train<<<ntiles, 128, SMEM_TRAIN, (cudaStream_t)stream>>>(m->img, m->bias, x, t, idx, batch, m->part, m->err);
+  k_mlp_reduce<<<(NPARAM + 1 + 255) / 256, 256, 0, (cudaStream_t)stream>>>(m->part, ntiles, m->G, m->loss);
   return cudaGetLastError() == cudaSuccess ? CFG_OK : CFG_E_CUDA;
 }
 

@@ -36,6 +36,9 @@ constexpr int TILE = 128;  // points per CTA tile (MMA M)
 constexpr int OFF_W0 = 0, OFF_B0 = OFF_W0 + H * IN, OFF_W1 = OFF_B0 + H, OFF_B1 = OFF_W1 + H * H,
               OFF_W2 = OFF_B1 + H, OFF_B2 = OFF_W2 + H * H, OFF_W3 = OFF_B2 + H, OFF_B3 = OFF_W3 + OUT * H,
               NPARAM = OFF_B3 + OUT;
+// one training tile's gradient slice: the NPARAM gradients and the loss,
+// padded to 16 bytes
+constexpr int PART_STRIDE = (NPARAM + 1 + 3) / 4 * 4;
 // BF16 operand images of the weights (units of 16 B, the layout above with
 // rows = output features): W0 64x16, W1 64x64, W2 64x64, W3 16x64
 constexpr int IMG_W0 = 0, IMG_W1 = IMG_W0 + H * KIN / 8, IMG_W2 = IMG_W1 + H * H / 8,

@@ -411,7 +411,10 @@ void cfg_ensemble_destroy(cfg_ensemble *e);
  * cfg_mlp_accumulate_grad: one batch of training samples, rows idx[0..batch)
  *   of x [.][10] and targets t [.][6] (device): adds the gradient of the
  *   mean-square loss (mean over batch x 6) and the loss itself to the
- *   network's accumulators.  cfg_mlp_get_grads copies them to the host
+ *   network's accumulators, summed in a fixed order (the same bits on every
+ *   run); calls on one network run in stream order, since they share its
+ *   per-tile gradient buffer, which grows (cudaFree, cudaMalloc) the first
+ *   time a batch exceeds 65536 rows.  cfg_mlp_get_grads copies them to the host
  *   (synchronises); cfg_mlp_adam_step applies one Adam update (bias
  *   corrected) from them and clears them; cfg_mlp_zero_grads clears them.
  * cfg_mlp_status: CFG_E_STATE if a kernel gave up waiting for the tensor

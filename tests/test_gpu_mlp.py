@@ -8,7 +8,10 @@ the CPU restatement (oracle/mlp_oracle.py, BF16 operands emulated):
   L2 <= 1e-2 per weight and bias tensor, the loss to 1e-4;
 - the Adam update from the GPU's own gradient: parameters to 1e-6;
 - training: a student network fitted to a fixed teacher network's outputs
-  lowers its loss more than 10x in 300 Adam steps.
+  lowers its loss more than 10x in 300 Adam steps;
+- reproducibility: two trainings from the same start on the same batches
+  (one of them larger than the per-tile gradient slices held from creation)
+  end with the same parameters and losses, bit for bit.
 """
 import numpy as np
 import pytest
@@ -101,3 +104,33 @@ def test_training_fits_a_teacher(cf):
     print("mlp training losses", losses)
     assert losses[-1] < 0.1 * losses[0], losses
     m.close()
+
+
+def test_training_is_reproducible(cf):
+    import torch
+    rng = np.random.default_rng(9)
+    x = rng.standard_normal((8192, 10)).astype(np.float32)
+    t = rng.standard_normal((8192, 6)).astype(np.float32)
+    xd, td = torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda()
+
+    def run():
+        m = cf.Mlp(0, params(10))
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(11)
+        losses = []
+        for it in range(20):
+            for b in (1000, 70000 if it == 5 else 3000):
+                idx = torch.randint(0, 8192, (b,), device="cuda", dtype=torch.int32, generator=gen)
+                m.accumulate_grad(xd.data_ptr(), td.data_ptr(), idx.data_ptr(), b)
+            losses.append(m.grads()[1])
+            m.adam_step(1e-3)
+        torch.cuda.synchronize()
+        assert m.status() == 0
+        p = m.get_params()
+        m.close()
+        return p, losses
+
+    p1, l1 = run()
+    p2, l2 = run()
+    assert l1 == l2, (l1, l2)
+    assert np.array_equal(p1.view(np.uint32), p2.view(np.uint32))
